@@ -1,0 +1,241 @@
+/*
+ * nrg_b200.h -- C ABI of the B200 NRG hot path.
+ *
+ * The reference (eminamitani/nrg-mpi, Fortran 90 + MPI + OpenMP + LAPACK/BLAS) keeps all
+ * state in module globals and calls its hot routines without arguments.  Each entry point
+ * below replaces one of those routines; its arguments are exactly the module arrays the
+ * routine reads and writes (raw pointers, sizes, 1-based integer values inside the
+ * packed records, Fortran column-major real arrays), so a Fortran caller binds them with
+ * ISO_C_BINDING (see INTEGRATION.md for the interface block and the wrapper subroutines
+ * that keep the reference's names).
+ *
+ * Pointers may be host or device memory (CUDA unified addressing tells them apart).
+ * Host arrays are copied to the device inside the call and results copied back before
+ * the call returns, so the call is a drop-in for the synchronous Fortran routine.
+ *
+ * Packed integer records (module.F90):
+ *   Basis_type            [basis(1:nVar), reference, variation, operation]   (:440-466)
+ *   SubspaceInfo_type     [basis(1:nVar), dimension, count_eigenvector, start_input] (:167-194)
+ *   FullSubspaceInfo_type [basis(1:nVar), dimension_before, dimension_after,
+ *                          start_eigen, start_input, start_output, start_matrix] (:294-327)
+ *
+ * Every call returns an NRG_* status; nrg_last_error() describes the last failure.
+ * There is no CPU fallback: without a usable CUDA device every compute call fails with
+ * NRG_ERR_DEVICE.
+ */
+#ifndef NRG_B200_H
+#define NRG_B200_H
+
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define NRG_API __attribute__((visibility("default")))
+#else
+#define NRG_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum {
+    NRG_OK = 0,
+    NRG_ERR_INVALID = 1,      /* an argument is inconsistent (sizes, indices, NULL)   */
+    NRG_ERR_CUDA = 2,         /* a CUDA runtime call failed                          */
+    NRG_ERR_NOMEM = 3,        /* device allocation failed                            */
+    NRG_ERR_TOO_LARGE = 4,    /* a block exceeds a kernel's size plan                */
+    NRG_ERR_DEVICE = 5,       /* no usable CUDA device                                */
+    NRG_ERR_UNSUPPORTED = 6,  /* input outside what the kernels implement            */
+    NRG_ERR_STATE = 7,        /* call sequence error (e.g. no model set)             */
+    NRG_ERR_NUMERIC = 8,      /* a kernel flagged a numerical failure                */
+    NRG_ERR_TIMEOUT = 9       /* a bounded device wait expired                       */
+};
+
+typedef struct nrg_context nrg_context;
+
+/* Model-wide inputs: what setupHamiltonian, read_parameter and read_initial_basis fill
+ * (module.F90:612-626, 722-760, 826-944; read_initial_basis.F90:27-204).  Chains are
+ * passed already rescaled (read_initial_basis.F90:103-142). */
+typedef struct nrg_model {
+    int32_t numberOfIteration;
+    int32_t numberOfChain;
+    int32_t numberOfVariation;
+    int32_t conservationBlock[4];            /* Fortran conservationBlock(2,2), col-major */
+    int32_t numberOfMatrix;
+    int32_t numberOfConductionMatrix;
+    int32_t numberOfCoefficient;
+    int32_t numberOfOperation;
+    int32_t numberOfBCSCoefficient;
+    int32_t indexOfFirstIteration;
+    int32_t flag_spectrum;
+    int32_t flag_BCS;
+    double bandWidth;
+    double ztrick;
+    double Lambda;
+    int32_t scalingType;
+    int32_t truncation;
+    const int32_t* operation;                         /* (nOps, nVar+nChain)          */
+    const int32_t* coefficient_invariant_matrix_type; /* (nCoef, 3)                    */
+    const double* coefficient_invariant_matrix;       /* (nCoef)                       */
+    const int32_t* coefficient_diagonalization_type;  /* (nCoef, 4)                    */
+    const double* coefficient_diagonalization;        /* (nCoef)                       */
+    const double* chain_diagonal;                     /* (0:nIter+1, nChain)           */
+    const double* chain_nondiagonal;                  /* (first:nIter+1, nChain)       */
+    const double* chain_BCS;                          /* (0:nIter+1, nChain) or NULL   */
+    const int32_t* coefficient_BCS;                   /* (nBCS, 3) or NULL             */
+    const double* coefficient_invariant_matrix_spectrum; /* (nMat, nOps)               */
+    const int32_t* conservation_difference_spectrum;  /* (nMat, nVar)                  */
+    const int32_t* positiveSpectrumOperation;         /* (nMat, nVar)                  */
+    const int32_t* negativeSpectrumOperation;         /* (nMat, nVar)                  */
+} nrg_model;
+
+/* ---- context ------------------------------------------------------------------------ */
+NRG_API int nrg_context_create(nrg_context** ctx, int device);
+NRG_API int nrg_context_destroy(nrg_context* ctx);
+/* CUDA stream (cudaStream_t) the kernels are launched on; NULL = the default stream. */
+NRG_API int nrg_context_set_stream(nrg_context* ctx, void* stream);
+/* Copies the model tables into the context (setupHamiltonian + read_initial_basis). */
+NRG_API int nrg_context_set_model(nrg_context* ctx, const nrg_model* model);
+/* Number of kernels this library launched on the context since creation. */
+NRG_API int64_t nrg_context_launch_count(const nrg_context* ctx);
+NRG_API const char* nrg_last_error(void);
+NRG_API const char* nrg_status_string(int status);
+NRG_API int nrg_version(void);
+
+/* ---- diagonalization(iteration, ismysubspace)  (diagonalization.F90:1-529) ----------
+ * Replaces the routine called from nrgIteration.F90:23.  Per symmetry sector: assemble
+ * the block Hamiltonian (diagonalization.F90:272-381), diagonalise it (dsyev 'V','U',
+ * :386), chop |V| < 1e-14 (:392-399); then shift the eigenvalues by their minimum and
+ * zero those <= 1e-12 (:469-475) and rebuild basis_output (:513-526).  ismysubspace of
+ * the reference is not needed: one device owns all sectors. */
+typedef struct nrg_diagonalization_io {
+    int32_t numberOfSubspace;          /* in                                             */
+    const int32_t* subspaceInfo;       /* in  [nsub*(nVar+3)]                            */
+    int32_t numberOfBasis;             /* in  nb = numberOfBasis_old * nOps              */
+    const int32_t* basis_input;        /* in  [nb*(nVar+3)]                              */
+    int32_t numberOfBasis_old;         /* in                                             */
+    const double* eigenvalue_old;      /* in  [nb_old]  eigenvalue of the last iteration */
+    const double* invariant_matrix;    /* in  (nb_old, nb_old, nCM)                      */
+    double* eigenvalue;                /* out [nb]                                       */
+    double* eigenvector;               /* out [sizeOfEigenvector] column-major blocks    */
+    int64_t sizeOfEigenvector;         /* in  capacity = sum over sectors of dimension^2 */
+    int32_t* basis_output;             /* out [nb*(nVar+3)]                              */
+    double* groundStateEnergy;         /* out eigenvalue(1) before the shift (:470)      */
+} nrg_diagonalization_io;
+NRG_API int nrg_diagonalization(nrg_context* ctx, int32_t iteration, const nrg_diagonalization_io* io);
+
+/* ---- invariantMatrixDGEMM(iteration) and invariantMatrixForSpectrumDGEMM(iteration) ---
+ * (invariantMatrixDGEMM.F90:1-394, invariantMatrixForSpectrumDGEMM.F90:1-392), called
+ * from postprocess.F90:194,197 after truncation.  basis_output holds the kept states
+ * first (numberOfBasis of them, postprocess.F90:143-160). */
+typedef struct nrg_invariant_matrix_io {
+    int32_t numberOfSubspace;          /* in                                             */
+    const int32_t* subspaceInfo;       /* in  [nsub*(nVar+3)]                            */
+    int32_t numberOfBasisFull;         /* in  states before truncation                   */
+    const int32_t* basis_input;        /* in  [nb_full*(nVar+3)]                         */
+    int32_t numberOfBasis;             /* in  kept states                                */
+    const int32_t* basis_output;       /* in  [>= nb*(nVar+3)], kept prefix used         */
+    const double* eigenvector;         /* in  [sizeOfEigenvector]                        */
+    int64_t sizeOfEigenvector;         /* in                                             */
+    int32_t numberOfBasis_old;         /* in  (spectrum variant) rows of the old matrix  */
+    const double* invariant_matrix_spectrum_old; /* in (nb_old, nb_old, nMat) (spectrum) */
+    double* invariant_matrix;          /* out (nb, nb, nCM) or (nb, nb, nMat)            */
+} nrg_invariant_matrix_io;
+NRG_API int nrg_invariant_matrix_dgemm(nrg_context* ctx, int32_t iteration,
+                               const nrg_invariant_matrix_io* io);
+NRG_API int nrg_invariant_matrix_for_spectrum_dgemm(nrg_context* ctx, int32_t iteration,
+                                            const nrg_invariant_matrix_io* io);
+
+/* ---- reducedDensityMatrixCalculation()  (reducedDensityMatrixDGEMM.F90:2-377) --------
+ * Backward recursion rho_N = A rho_{N+1} A^T for N = numberOfIteration-1 .. startTrancation,
+ * called from main.F90:200 after initializeReducedDensity.  mapFullSubspaceInfo is
+ * indexed from iteration -1 (element 0 is mapFullSubspaceInfo(-1)). */
+typedef struct nrg_reduced_density_io {
+    int32_t numberOfIteration;
+    int32_t startTrancation;
+    const int32_t* mapFullSubspaceInfo;   /* in  (-1:numberOfIteration)                  */
+    int32_t elementNumFullSubspace;       /* in                                          */
+    int32_t* fullSubspaceInfo;            /* inout [n*(nVar+6)], start_matrix filled     */
+    const int32_t* fullBasisInput;        /* in  [numFullBasisInput*(nVar+3)]            */
+    int64_t numFullBasisInput;
+    const int32_t* fullBasisOutput;       /* in  [numFullBasisOutput*(nVar+3)]           */
+    int64_t numFullBasisOutput;
+    const double* fullEigenvector;        /* in                                          */
+    int64_t numFullEigenvector;
+    double* reducedDensityMatrix;         /* inout [sizeOfReducedDensity]                */
+    int64_t sizeOfReducedDensity;
+    int32_t* pointReducedDensity;         /* inout                                       */
+    double* trace;                        /* out, optional [numberOfIteration - startTrancation] */
+} nrg_reduced_density_io;
+NRG_API int nrg_reduced_density_matrix(nrg_context* ctx, const nrg_reduced_density_io* io);
+
+/* ---- spikeZeroTemperature(iteration) / spikeCFS(iteration, numberOfBasisFull) --------
+ * (calculateSpectrumDGEMM.F90:1-215 and :217-646), called from cfsSpectrumCalculation
+ * (module.F90:1700,1702) after getRestore.  Spikes are binned onto the logarithmic grid
+ * of binningSpike (module.F90:1210-1254) and added to the weight column of the bins. */
+typedef struct nrg_spike_io {
+    int32_t numberOfSubspace;
+    const int32_t* subspaceInfo;          /* [nsub*(nVar+3)] of this iteration           */
+    int32_t numberOfBasis;                /* kept states (hami%numberOfBasis)            */
+    int32_t numberOfBasisFull;            /* all states of this iteration                */
+    const int32_t* basis_input;           /* [nb_full*(nVar+3)]                          */
+    const int32_t* basis_output;          /* [nb_full*(nVar+3)]                          */
+    const double* eigenvalue;             /* [nb_full]                                   */
+    const double* eigenvector;            /* [sizeOfEigenvector]                         */
+    int64_t sizeOfEigenvector;
+    int32_t numberOfBasis_old;
+    const double* invariant_matrix_spectrum; /* (nb_old, nb_old, nMat) of iteration-1   */
+    const int32_t* fullSubspaceInfo;      /* spikeCFS only                               */
+    const int32_t* mapFullSubspaceInfo;   /* spikeCFS only, from iteration -1            */
+    int32_t elementNumFullSubspace;       /* spikeCFS only                               */
+    const double* reducedDensityMatrix;   /* spikeCFS only                               */
+    int64_t sizeOfReducedDensity;
+    int32_t numberOfBin;
+    double* binnedSpikePositive;          /* inout (numberOfBin*nMat, 2)                 */
+    double* binnedSpikeNegative;          /* inout (numberOfBin*nMat, 2)                 */
+    double* total_sum;                    /* out, optional [4*nMat]: raw negative, raw
+                                             positive, binned negative, binned positive
+                                             (spikeCFS check, :559-596)                  */
+} nrg_spike_io;
+NRG_API int nrg_spike_zero_temperature(nrg_context* ctx, int32_t iteration, const nrg_spike_io* io);
+NRG_API int nrg_spike_cfs(nrg_context* ctx, int32_t iteration, const nrg_spike_io* io);
+
+/* ---- whole run: main.F90:142-252 with everything device resident ---------------------
+ * Replays the reference's driver (forward NRG sweep, backward reduced density matrices,
+ * CFS spectrum at T = 0) on one device.  Initial state as read from initial.dat. */
+typedef struct nrg_run_input {
+    int32_t numberOfBasis;                /* impurity basis size                        */
+    const int32_t* basis_output;          /* [nb*(nVar+3)]                              */
+    const double* eigenvalue;             /* [nb]                                       */
+    const double* invariant_matrix;       /* (nb, nb, nCM)                              */
+    const double* invariant_matrix_spectrum; /* (nb, nb, nMat)                          */
+    int32_t spectrum;                     /* 0: forward sweep only                     */
+    int32_t host_drop_in;                 /* 1: every routine goes through the drop-in
+                                             entry points with host arrays (the
+                                             Fortran caller's data flow)               */
+} nrg_run_input;
+
+typedef struct nrg_run_output {
+    int32_t numberOfBin;                  /* out                                        */
+    double* binnedSpikePositive;          /* out, capacity numberOfBin*nMat*2 (may be NULL) */
+    double* binnedSpikeNegative;          /* out                                        */
+    int64_t binCapacity;                  /* in  doubles available in each bin array    */
+    int32_t startTrancation;              /* out                                        */
+    int32_t* kept;                        /* out, optional [nIter-first+1]              */
+    int32_t* numberOfBasisFull;           /* out, optional [nIter-first+1]              */
+    double* groundStateEnergy;            /* out, optional [nIter-first+1]              */
+    double* rdmTrace;                     /* out, optional [nIter+1]: trace at N         */
+    double* flow;                         /* out, optional [nIter-first+1]*flowStride:
+                                             lowest kept energies per iteration         */
+    int32_t flowStride;
+    double* finalEigenvalue;              /* out, optional [finalCapacity]              */
+    int32_t finalCapacity;
+    double* phaseSeconds;                 /* out, optional [4]: nrg sweep, rdm, cfs, total
+                                             (device events)                            */
+} nrg_run_output;
+NRG_API int nrg_run(nrg_context* ctx, const nrg_run_input* in, nrg_run_output* out);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* NRG_B200_H */

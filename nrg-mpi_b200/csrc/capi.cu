@@ -1,0 +1,657 @@
+// C ABI entry points (include/nrg_b200.h): context, model, and the drop-in replacements
+// of the reference routines.  Host arrays are staged through device buffers; device
+// arrays are used in place.
+#include "internal.hpp"
+
+#include <algorithm>
+#include <cstdarg>
+#include <cstring>
+#include <vector>
+
+namespace {
+thread_local char g_err[1024] = "";
+}
+
+void nrg_set_error_message(const char* fmt, ...) {
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(g_err, sizeof(g_err), fmt, ap);
+    va_end(ap);
+}
+
+nrg_context::~nrg_context() {
+    for (auto& b : store) b.release();
+    for (auto& b : scratch.b) b.release();
+    for (auto& s : iter_sectors) { s.d_bi.release(); s.d_lst.release(); s.d_lstOff.release(); }
+    d_status.release();
+    nrg::Model& M = model;
+    for (nrg::DevBuf* b : {&M.d_operation, &M.d_dflag, &M.d_dtype, &M.d_dch, &M.d_dswp, &M.d_bflag,
+                           &M.d_bch, &M.d_dcoef, &M.d_imflag, &M.d_imcoef})
+        b->release();
+}
+
+using namespace nrg;
+
+namespace {
+
+bool is_device_ptr(const void* p) {
+    if (!p) return false;
+    cudaPointerAttributes a;
+    if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
+}
+
+template <class T>
+int stage_in(nrg_context* ctx, const T* p, size_t n, size_t slot, const T** out) {
+    if (n == 0) { *out = nullptr; return NRG_OK; }
+    if (!p) { nrg_set_error_message("NULL input array"); return NRG_ERR_INVALID; }
+    if (is_device_ptr(p)) { *out = p; return NRG_OK; }
+    DevBuf& b = ctx->slot(slot);
+    NRG_TRY(b.ensure(sizeof(T) * n));
+    NRG_CUDA_TRY(cudaMemcpyAsync(b.p, p, sizeof(T) * n, cudaMemcpyHostToDevice, ctx->stream));
+    *out = b.as<T>();
+    return NRG_OK;
+}
+
+template <class T>
+int stage_out(nrg_context* ctx, T* p, size_t n, size_t slot, T** dev) {
+    if (!p) { nrg_set_error_message("NULL output array"); return NRG_ERR_INVALID; }
+    if (is_device_ptr(p)) { *dev = p; return NRG_OK; }
+    DevBuf& b = ctx->slot(slot);
+    NRG_TRY(b.ensure(sizeof(T) * std::max<size_t>(n, 1)));
+    *dev = b.as<T>();
+    return NRG_OK;
+}
+
+template <class T>
+int finish_out(nrg_context* ctx, T* p, const T* dev, size_t n) {
+    if (p == dev || n == 0) return NRG_OK;
+    NRG_CUDA_TRY(cudaMemcpyAsync(p, dev, sizeof(T) * n, cudaMemcpyDeviceToHost, ctx->stream));
+    return NRG_OK;
+}
+
+template <class T>
+std::vector<T> to_host(nrg_context* ctx, const T* p, size_t n, int* status) {
+    std::vector<T> v(n);
+    *status = NRG_OK;
+    if (n == 0) return v;
+    if (is_device_ptr(p)) {
+        cudaError_t e = cudaMemcpyAsync(v.data(), p, sizeof(T) * n, cudaMemcpyDeviceToHost, ctx->stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+        if (e != cudaSuccess) { *status = NRG_ERR_CUDA; nrg_set_error_message("%s", cudaGetErrorString(e)); }
+    } else {
+        std::memcpy(v.data(), p, sizeof(T) * n);
+    }
+    return v;
+}
+
+int need_model(nrg_context* ctx) {
+    if (!ctx) { nrg_set_error_message("NULL context"); return NRG_ERR_INVALID; }
+    if (!ctx->model.set) { nrg_set_error_message("nrg_context_set_model has not been called"); return NRG_ERR_STATE; }
+    return NRG_OK;
+}
+
+template <class T>
+int up(DevBuf& b, const std::vector<T>& v, cudaStream_t st) {
+    NRG_TRY(b.ensure(sizeof(T) * std::max<size_t>(v.size(), 1)));
+    if (!v.empty()) NRG_CUDA_TRY(cudaMemcpyAsync(b.p, v.data(), sizeof(T) * v.size(), cudaMemcpyHostToDevice, st));
+    return NRG_OK;
+}
+
+constexpr size_t kSlotIO = 100000;   // drop-in staging slots
+
+}  // namespace
+
+extern "C" {
+
+const char* nrg_last_error(void) { return g_err; }
+
+const char* nrg_status_string(int s) {
+    switch (s) {
+        case NRG_OK: return "ok";
+        case NRG_ERR_INVALID: return "invalid argument";
+        case NRG_ERR_CUDA: return "CUDA error";
+        case NRG_ERR_NOMEM: return "out of device memory";
+        case NRG_ERR_TOO_LARGE: return "block too large";
+        case NRG_ERR_DEVICE: return "no usable CUDA device";
+        case NRG_ERR_UNSUPPORTED: return "unsupported input";
+        case NRG_ERR_STATE: return "call sequence error";
+        case NRG_ERR_NUMERIC: return "numerical failure";
+        case NRG_ERR_TIMEOUT: return "device wait timed out";
+        default: return "unknown status";
+    }
+}
+
+int nrg_version(void) { return 1; }
+
+int nrg_context_create(nrg_context** out, int device) {
+    if (!out) return NRG_ERR_INVALID;
+    *out = nullptr;
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess || n <= device || device < 0) {
+        cudaGetLastError();
+        nrg_set_error_message("no CUDA device %d (count %d)", device, n);
+        return NRG_ERR_DEVICE;
+    }
+    NRG_CUDA_TRY(cudaSetDevice(device));
+    cudaDeviceProp prop;
+    NRG_CUDA_TRY(cudaGetDeviceProperties(&prop, device));
+    if (prop.major < 10) {
+        nrg_set_error_message("device %d is sm_%d%d; this library is built for sm_100a", device, prop.major, prop.minor);
+        return NRG_ERR_DEVICE;
+    }
+    nrg_context* c = new nrg_context();
+    c->device = device;
+    int st = c->d_status.ensure(sizeof(int) * 4);
+    if (st != NRG_OK) { delete c; return st; }
+    if (cudaMemset(c->d_status.p, 0, sizeof(int) * 4) != cudaSuccess) { delete c; return NRG_ERR_CUDA; }
+    *out = c;
+    return NRG_OK;
+}
+
+int nrg_context_destroy(nrg_context* ctx) {
+    if (!ctx) return NRG_OK;
+    cudaSetDevice(ctx->device);
+    cudaStreamSynchronize(ctx->stream);
+    delete ctx;
+    return NRG_OK;
+}
+
+int nrg_context_set_stream(nrg_context* ctx, void* stream) {
+    if (!ctx) return NRG_ERR_INVALID;
+    ctx->stream = (cudaStream_t)stream;
+    return NRG_OK;
+}
+
+int64_t nrg_context_launch_count(const nrg_context* ctx) { return ctx ? ctx->launches : 0; }
+
+int nrg_context_set_model(nrg_context* ctx, const nrg_model* m) {
+    if (!ctx || !m) return NRG_ERR_INVALID;
+    NRG_CUDA_TRY(cudaSetDevice(ctx->device));
+    Model& M = ctx->model;
+    M.set = false;
+    M.nIter = m->numberOfIteration; M.nChain = m->numberOfChain; M.nVar = m->numberOfVariation;
+    for (int i = 0; i < 4; ++i) M.cb[i] = m->conservationBlock[i];
+    M.nMat = m->flag_spectrum ? m->numberOfMatrix : 0;
+    M.nCM = m->numberOfConductionMatrix; M.nCoef = m->numberOfCoefficient;
+    M.nOps = m->numberOfOperation; M.nBCS = m->numberOfBCSCoefficient;
+    M.first = m->indexOfFirstIteration; M.flag_spectrum = m->flag_spectrum; M.flag_BCS = m->flag_BCS;
+    M.D = m->bandWidth; M.z = m->ztrick; M.Lambda = m->Lambda;
+    M.scalingType = m->scalingType; M.truncation = m->truncation;
+    if (M.nVar < 1 || M.nOps < 1 || M.nChain < 1 || M.nCM < 1 || M.nIter < M.first || M.nCoef < 0) {
+        nrg_set_error_message("inconsistent model sizes");
+        return NRG_ERR_INVALID;
+    }
+    if (!m->operation || (M.nCoef > 0 && (!m->coefficient_invariant_matrix_type ||
+        !m->coefficient_invariant_matrix || !m->coefficient_diagonalization_type ||
+        !m->coefficient_diagonalization)) || !m->chain_diagonal || !m->chain_nondiagonal) {
+        nrg_set_error_message("missing model table");
+        return NRG_ERR_INVALID;
+    }
+    const int nOps = M.nOps, nVar = M.nVar, nChain = M.nChain;
+    M.operation.assign(m->operation, m->operation + (size_t)nOps * (nVar + nChain));
+    const size_t nd = (size_t)(M.nIter + 2) * nChain, nn = (size_t)(M.nIter + 2 - M.first) * nChain;
+    M.chain_diag.assign(m->chain_diagonal, m->chain_diagonal + nd);
+    M.chain_nond.assign(m->chain_nondiagonal, m->chain_nondiagonal + nn);
+    M.chain_bcs.clear();
+    if (M.flag_BCS && m->chain_BCS) M.chain_bcs.assign(m->chain_BCS, m->chain_BCS + nd);
+    if (M.nMat > 0) {
+        if (!m->coefficient_invariant_matrix_spectrum || !m->conservation_difference_spectrum ||
+            !m->positiveSpectrumOperation || !m->negativeSpectrumOperation) {
+            nrg_set_error_message("missing spectrum table");
+            return NRG_ERR_INVALID;
+        }
+        M.cspec.assign(m->coefficient_invariant_matrix_spectrum, m->coefficient_invariant_matrix_spectrum + (size_t)M.nMat * nOps);
+        M.cons_diff.assign(m->conservation_difference_spectrum, m->conservation_difference_spectrum + (size_t)M.nMat * nVar);
+        M.pos_op.assign(m->positiveSpectrumOperation, m->positiveSpectrumOperation + (size_t)M.nMat * nVar);
+        M.neg_op.assign(m->negativeSpectrumOperation, m->negativeSpectrumOperation + (size_t)M.nMat * nVar);
+    }
+    // coefficient scans of diagonalization.F90:195-224 and invariantMatrixDGEMM.F90:248-254
+    const int nC = M.nCoef;
+    auto cdt = [&](int ic, int col) { return m->coefficient_diagonalization_type[(size_t)ic + (size_t)col * nC]; };
+    auto cit = [&](int ic, int col) { return m->coefficient_invariant_matrix_type[(size_t)ic + (size_t)col * nC]; };
+    const size_t nn2 = (size_t)nOps * nOps;
+    M.dflag.assign(nn2, 0); M.dtype.assign(nn2, 0); M.dch.assign(nn2, 0); M.dswp.assign(nn2, 0);
+    M.dcoef.assign(nn2, 0.0); M.bflag.assign(nn2, 0); M.bch.assign(nn2, 0);
+    for (int a = 1; a <= nOps; ++a)
+        for (int b = 1; b <= nOps; ++b) {
+            const size_t x = (size_t)(a - 1) * nOps + (b - 1);
+            for (int ic = 0; ic < nC; ++ic) {
+                if (a == cdt(ic, 0) && b == cdt(ic, 1)) {
+                    M.dflag[x] = 1; M.dtype[x] = cdt(ic, 2); M.dch[x] = cdt(ic, 3);
+                    M.dcoef[x] = m->coefficient_diagonalization[ic];
+                } else if (a == cdt(ic, 1) && b == cdt(ic, 0)) {
+                    M.dflag[x] = 1; M.dtype[x] = cdt(ic, 2); M.dch[x] = cdt(ic, 3);
+                    M.dcoef[x] = m->coefficient_diagonalization[ic];
+                    M.dswp[x] = 1;
+                }
+            }
+            if (M.dflag[x] && (M.dtype[x] < 1 || M.dtype[x] > M.nCM || M.dch[x] < 1 || M.dch[x] > nChain)) {
+                nrg_set_error_message("coefficient_diagonalization_type row out of range");
+                return NRG_ERR_INVALID;
+            }
+        }
+    if (M.flag_BCS && m->coefficient_BCS) {
+        for (int ic = 0; ic < M.nBCS; ++ic) {
+            const int a = m->coefficient_BCS[ic], b = m->coefficient_BCS[ic + M.nBCS], ch = m->coefficient_BCS[ic + 2 * M.nBCS];
+            if (a < 1 || a > nOps || b < 1 || b > nOps) return NRG_ERR_INVALID;
+            const size_t x = (size_t)(a - 1) * nOps + (b - 1);
+            M.bflag[x] = 1; M.bch[x] = ch;
+        }
+    }
+    M.imflag.assign(nn2 * M.nCM, 0);
+    M.imcoef.assign(nn2 * M.nCM, 0.0);
+    for (int ic = 0; ic < nC; ++ic) {
+        const int a = cit(ic, 0), b = cit(ic, 1), t = cit(ic, 2);
+        if (a < 1 || a > nOps || b < 1 || b > nOps || t < 1 || t > M.nCM) {
+            nrg_set_error_message("coefficient_invariant_matrix_type row out of range");
+            return NRG_ERR_INVALID;
+        }
+        const size_t x = ((size_t)(a - 1) * nOps + (b - 1)) * M.nCM + (t - 1);
+        M.imflag[x] = 1;
+        M.imcoef[x] = m->coefficient_invariant_matrix[ic];
+    }
+    cudaStream_t st = ctx->stream;
+    NRG_TRY(up(M.d_operation, M.operation, st));
+    NRG_TRY(up(M.d_dflag, M.dflag, st)); NRG_TRY(up(M.d_dtype, M.dtype, st));
+    NRG_TRY(up(M.d_dch, M.dch, st)); NRG_TRY(up(M.d_dswp, M.dswp, st));
+    NRG_TRY(up(M.d_dcoef, M.dcoef, st)); NRG_TRY(up(M.d_bflag, M.bflag, st));
+    NRG_TRY(up(M.d_bch, M.bch, st)); NRG_TRY(up(M.d_imflag, M.imflag, st));
+    NRG_TRY(up(M.d_imcoef, M.imcoef, st));
+    NRG_CUDA_TRY(cudaStreamSynchronize(st));
+    M.set = true;
+    return NRG_OK;
+}
+
+// ------------------------------------------------------------------------------------
+int nrg_diagonalization(nrg_context* ctx, int32_t iteration, const nrg_diagonalization_io* io) {
+    NRG_TRY(need_model(ctx));
+    if (!io) return NRG_ERR_INVALID;
+    NRG_CUDA_TRY(cudaSetDevice(ctx->device));
+    const Model& M = ctx->model;
+    if (iteration < M.first || iteration > M.nIter) {
+        nrg_set_error_message("iteration %d outside [%d, %d]", iteration, M.first, M.nIter);
+        return NRG_ERR_INVALID;
+    }
+    const int rs = M.nVar + 3;
+    int st = NRG_OK;
+    auto si = to_host(ctx, io->subspaceInfo, (size_t)io->numberOfSubspace * rs, &st);
+    NRG_TRY(st);
+    auto bi = to_host(ctx, io->basis_input, (size_t)io->numberOfBasis * rs, &st);
+    NRG_TRY(st);
+    Sectors S;
+    int rc = S.build(io->numberOfSubspace, si.data(), io->numberOfBasis, bi.data(), M.nVar, M.nOps);
+    if (rc == NRG_OK) rc = S.upload(ctx->stream);
+    if (rc != NRG_OK) { S.d_bi.release(); S.d_lst.release(); S.d_lstOff.release(); return rc; }
+    const int nbo = io->numberOfBasis_old;
+    if (io->sizeOfEigenvector < S.sizeV || nbo < 1) {
+        nrg_set_error_message("eigenvector capacity %lld < %lld", (long long)io->sizeOfEigenvector, S.sizeV);
+        rc = NRG_ERR_INVALID;
+    }
+    const double *dEo = nullptr, *dIM = nullptr;
+    double *dV = nullptr, *dE = nullptr;
+    if (rc == NRG_OK) rc = stage_in(ctx, io->eigenvalue_old, (size_t)nbo, kSlotIO + 0, &dEo);
+    if (rc == NRG_OK) rc = stage_in(ctx, io->invariant_matrix, (size_t)nbo * nbo * M.nCM, kSlotIO + 1, &dIM);
+    if (rc == NRG_OK) rc = stage_out(ctx, io->eigenvector, (size_t)S.sizeV, kSlotIO + 2, &dV);
+    if (rc == NRG_OK) rc = stage_out(ctx, io->eigenvalue, (size_t)S.nb, kSlotIO + 3, &dE);
+    DiagOut out;
+    if (rc == NRG_OK) rc = diag_device(ctx, iteration, S, dEo, nbo, dIM, dV, dE, &out);
+    if (rc == NRG_OK) rc = finish_out(ctx, io->eigenvector, dV, (size_t)S.sizeV);
+    if (rc == NRG_OK) rc = finish_out(ctx, io->eigenvalue, dE, (size_t)S.nb);
+    if (rc == NRG_OK && io->basis_output) {
+        std::vector<int> bo((size_t)S.nb * rs, 0);
+        for (int s = 0; s < S.nsub; ++s)
+            for (int j = 0; j < S.dim[s]; ++j) {
+                int* r = &bo[(size_t)(S.start[s] + j) * rs];
+                for (int v = 0; v < M.nVar; ++v) r[v] = S.qn[(size_t)s * M.nVar + v];
+                r[M.nVar] = j + 1;
+            }
+        if (is_device_ptr(io->basis_output))
+            rc = cudaMemcpyAsync(io->basis_output, bo.data(), sizeof(int) * bo.size(), cudaMemcpyHostToDevice, ctx->stream) == cudaSuccess ? NRG_OK : NRG_ERR_CUDA;
+        else
+            std::memcpy(io->basis_output, bo.data(), sizeof(int) * bo.size());
+    }
+    if (rc == NRG_OK && io->groundStateEnergy) *io->groundStateEnergy = out.groundStateEnergy;
+    if (cudaStreamSynchronize(ctx->stream) != cudaSuccess && rc == NRG_OK) rc = NRG_ERR_CUDA;
+    S.d_bi.release(); S.d_lst.release(); S.d_lstOff.release();
+    return rc;
+}
+
+static int invmat_common(nrg_context* ctx, int32_t iteration, const nrg_invariant_matrix_io* io, bool spec) {
+    NRG_TRY(need_model(ctx));
+    if (!io) return NRG_ERR_INVALID;
+    NRG_CUDA_TRY(cudaSetDevice(ctx->device));
+    const Model& M = ctx->model;
+    (void)iteration;
+    if (spec && M.nMat == 0) { nrg_set_error_message("model has no spectrum tables"); return NRG_ERR_STATE; }
+    const int rs = M.nVar + 3;
+    int st = NRG_OK;
+    auto si = to_host(ctx, io->subspaceInfo, (size_t)io->numberOfSubspace * rs, &st);
+    NRG_TRY(st);
+    auto bi = to_host(ctx, io->basis_input, (size_t)io->numberOfBasisFull * rs, &st);
+    NRG_TRY(st);
+    auto bo = to_host(ctx, io->basis_output, (size_t)io->numberOfBasis * rs, &st);
+    NRG_TRY(st);
+    Sectors S;
+    int rc = S.build(io->numberOfSubspace, si.data(), io->numberOfBasisFull, bi.data(), M.nVar, M.nOps);
+    if (rc == NRG_OK) rc = S.upload(ctx->stream);
+    std::vector<int> kept;
+    if (rc == NRG_OK) {
+        kept = kept_per_sector(S, io->numberOfBasis, bo.data());
+        long long tot = 0;
+        for (int s = 0; s < S.nsub; ++s) { tot += kept[s]; if (kept[s] > S.dim[s]) rc = NRG_ERR_INVALID; }
+        if (tot != io->numberOfBasis) rc = NRG_ERR_INVALID;
+        if (rc != NRG_OK) nrg_set_error_message("kept states do not match the sectors");
+    }
+    if (rc == NRG_OK && io->sizeOfEigenvector < S.sizeV) rc = NRG_ERR_INVALID;
+    const double* dV = nullptr;
+    const double* dIMSo = nullptr;
+    double* dOut = nullptr;
+    const int nbk = io->numberOfBasis;
+    const size_t nout = (size_t)nbk * nbk * (spec ? M.nMat : M.nCM);
+    if (rc == NRG_OK) rc = stage_in(ctx, io->eigenvector, (size_t)S.sizeV, kSlotIO + 4, &dV);
+    if (rc == NRG_OK && spec)
+        rc = stage_in(ctx, io->invariant_matrix_spectrum_old,
+                      (size_t)io->numberOfBasis_old * io->numberOfBasis_old * M.nMat, kSlotIO + 5, &dIMSo);
+    if (rc == NRG_OK) rc = stage_out(ctx, io->invariant_matrix, nout, kSlotIO + 6, &dOut);
+    if (rc == NRG_OK) {
+        if (spec) rc = invmat_spec_device(ctx, S, kept, dV, io->numberOfBasis_old, dIMSo, dOut);
+        else rc = invmat_device(ctx, S, kept, dV, dOut);
+    }
+    if (rc == NRG_OK) rc = finish_out(ctx, io->invariant_matrix, dOut, nout);
+    if (cudaStreamSynchronize(ctx->stream) != cudaSuccess && rc == NRG_OK) rc = NRG_ERR_CUDA;
+    if (rc == NRG_OK) rc = check_device_status(ctx);
+    S.d_bi.release(); S.d_lst.release(); S.d_lstOff.release();
+    return rc;
+}
+
+int nrg_invariant_matrix_dgemm(nrg_context* ctx, int32_t iteration, const nrg_invariant_matrix_io* io) {
+    return invmat_common(ctx, iteration, io, false);
+}
+int nrg_invariant_matrix_for_spectrum_dgemm(nrg_context* ctx, int32_t iteration,
+                                            const nrg_invariant_matrix_io* io) {
+    return invmat_common(ctx, iteration, io, true);
+}
+
+}  // extern "C"
+
+// ------------------------------------------------------------------------------------
+// the full stock (fullSubspaceInfo & co.) as per-iteration sector tables
+// ------------------------------------------------------------------------------------
+namespace {
+
+struct FullIter {
+    Sectors S;
+    std::vector<int> kept;
+    std::vector<long long> rdm_off;
+    std::vector<int> rows;      // fullSubspaceInfo row index per sector
+};
+
+void release(FullIter& f) { f.S.d_bi.release(); f.S.d_lst.release(); f.S.d_lstOff.release(); }
+
+// builds the sectors of one iteration from rows [r0, r1) of fullSubspaceInfo
+int build_full_iter(nrg_context* ctx, const int* fsi, int r0, int r1, const int* fbi, long long nfbi,
+                    FullIter* out) {
+    const Model& M = ctx->model;
+    const int nVar = M.nVar, rsf = nVar + 6, rs = nVar + 3;
+    const int nsub = r1 - r0;
+    std::vector<int> si((size_t)nsub * rs), bi;
+    int rowpos = 0;
+    out->kept.assign(nsub, 0);
+    out->rdm_off.assign(nsub, -1);
+    out->rows.resize(nsub);
+    std::vector<long long> ce(nsub);
+    for (int s = 0; s < nsub; ++s) {
+        const int* f = fsi + (size_t)(r0 + s) * rsf;
+        const int d = f[nVar], k = f[nVar + 1];
+        const long long sin0 = (long long)f[nVar + 3] - 1;
+        if (sin0 < 0 || sin0 + d > nfbi) { nrg_set_error_message("fullSubspaceInfo start_input out of range"); return NRG_ERR_INVALID; }
+        for (int v = 0; v < nVar; ++v) si[(size_t)s * rs + v] = f[v];
+        si[(size_t)s * rs + nVar] = d;
+        si[(size_t)s * rs + nVar + 1] = 0;   // replaced below
+        si[(size_t)s * rs + nVar + 2] = rowpos + 1;
+        bi.insert(bi.end(), fbi + sin0 * rs, fbi + (sin0 + d) * rs);
+        rowpos += d;
+        out->kept[s] = k;
+        out->rdm_off[s] = (long long)f[nVar + 5] - 1;
+        out->rows[s] = r0 + s;
+        ce[s] = (long long)f[nVar + 2] - 1;
+    }
+    // count_eigenvector as the running square sums (checked by build), then the stock's
+    // start_eigen replaces it: the stock keeps only the kept columns of each block
+    long long acc = 0;
+    for (int s = 0; s < nsub; ++s) {
+        si[(size_t)s * rs + nVar + 1] = (int)std::min(acc + 1, 0x7fffffffLL);
+        acc += (long long)si[(size_t)s * rs + nVar] * si[(size_t)s * rs + nVar];
+    }
+    NRG_TRY(out->S.build(nsub, si.data(), rowpos, bi.data(), nVar, M.nOps));
+    out->S.ce = ce;
+    return out->S.upload(ctx->stream);
+}
+
+int full_range(const int* map, int nIter, int first, int elementNum, int N, int* r0, int* r1) {
+    // mapFullSubspaceInfo(-1:nIter), element 0 = iteration -1
+    (void)first;
+    *r0 = map[N + 1] - 1;
+    *r1 = (N == nIter) ? elementNum : map[N + 2] - 1;
+    if (*r0 < 0 || *r1 < *r0 || *r1 > elementNum) {
+        nrg_set_error_message("mapFullSubspaceInfo inconsistent at iteration %d", N);
+        return NRG_ERR_INVALID;
+    }
+    return NRG_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int nrg_reduced_density_matrix(nrg_context* ctx, const nrg_reduced_density_io* io) {
+    NRG_TRY(need_model(ctx));
+    if (!io) return NRG_ERR_INVALID;
+    NRG_CUDA_TRY(cudaSetDevice(ctx->device));
+    const Model& M = ctx->model;
+    const int nVar = M.nVar, rsf = nVar + 6, rs = nVar + 3;
+    const int nIter = io->numberOfIteration, start = io->startTrancation;
+    if (nIter - start <= 0) return NRG_OK;   // reducedDensityMatrixDGEMM.F90:62 loop is empty
+    int st = NRG_OK;
+    auto map = to_host(ctx, io->mapFullSubspaceInfo, (size_t)(nIter + 2), &st);
+    NRG_TRY(st);
+    auto fsi = to_host(ctx, (const int*)io->fullSubspaceInfo, (size_t)io->elementNumFullSubspace * rsf, &st);
+    NRG_TRY(st);
+    auto fbi = to_host(ctx, io->fullBasisInput, (size_t)io->numFullBasisInput * rs, &st);
+    NRG_TRY(st);
+    const double *dV = nullptr;
+    double* dR = nullptr;
+    NRG_TRY(stage_in(ctx, io->fullEigenvector, (size_t)io->numFullEigenvector, kSlotIO + 7, &dV));
+    NRG_TRY(stage_out(ctx, io->reducedDensityMatrix, (size_t)io->sizeOfReducedDensity, kSlotIO + 8, &dR));
+    if (dR != io->reducedDensityMatrix)
+        NRG_CUDA_TRY(cudaMemcpyAsync(dR, io->reducedDensityMatrix, sizeof(double) * io->sizeOfReducedDensity,
+                                     cudaMemcpyHostToDevice, ctx->stream));
+    int point = *io->pointReducedDensity;
+    DevBuf& tr = ctx->scratch.b[21];
+    NRG_TRY(tr.ensure(sizeof(double) * (size_t)(nIter - start + 1)));
+    FullIter child, present;
+    int rc = NRG_OK;
+    int r0, r1;
+    rc = full_range(map.data(), nIter, M.first, io->elementNumFullSubspace, nIter, &r0, &r1);
+    if (rc == NRG_OK) rc = build_full_iter(ctx, fsi.data(), r0, r1, fbi.data(), io->numFullBasisInput, &child);
+    for (int i = 1; rc == NRG_OK && i <= nIter - start; ++i) {
+        const int N = nIter - i;
+        rc = full_range(map.data(), nIter, M.first, io->elementNumFullSubspace, N, &r0, &r1);
+        if (rc != NRG_OK) break;
+        // start_matrix of the present iteration (:94-100)
+        for (int j = r0; j < r1; ++j) {
+            fsi[(size_t)j * rsf + nVar + 5] = point;
+            point += fsi[(size_t)j * rsf + nVar + 1] * fsi[(size_t)j * rsf + nVar + 1];
+        }
+        if (point - 1 > io->sizeOfReducedDensity) { rc = NRG_ERR_INVALID; nrg_set_error_message("reducedDensityMatrix too small"); break; }
+        rc = build_full_iter(ctx, fsi.data(), r0, r1, fbi.data(), io->numFullBasisInput, &present);
+        if (rc != NRG_OK) break;
+        IterView P, C;
+        P.S = &present.S; P.kept = present.kept; P.d_V = dV; P.d_rdm = dR; P.rdm_off = present.rdm_off;
+        C.S = &child.S; C.kept = child.kept; C.d_V = dV; C.d_rdm = dR; C.rdm_off = child.rdm_off;
+        rc = rdm_step_device(ctx, P, C, dR, tr.as<double>() + (i - 1));
+        release(child);
+        child = present;
+        present = FullIter();
+    }
+    release(child);
+    release(present);
+    if (rc == NRG_OK) rc = finish_out(ctx, io->reducedDensityMatrix, dR, (size_t)io->sizeOfReducedDensity);
+    if (rc == NRG_OK && io->trace) {
+        std::vector<double> t(nIter - start);
+        NRG_CUDA_TRY(cudaMemcpyAsync(t.data(), tr.p, sizeof(double) * t.size(), cudaMemcpyDeviceToHost, ctx->stream));
+        NRG_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+        std::memcpy(io->trace, t.data(), sizeof(double) * t.size());
+    }
+    if (cudaStreamSynchronize(ctx->stream) != cudaSuccess && rc == NRG_OK) rc = NRG_ERR_CUDA;
+    if (rc == NRG_OK) {
+        if (is_device_ptr(io->fullSubspaceInfo))
+            NRG_CUDA_TRY(cudaMemcpy(io->fullSubspaceInfo, fsi.data(), sizeof(int) * fsi.size(), cudaMemcpyHostToDevice));
+        else
+            std::memcpy(io->fullSubspaceInfo, fsi.data(), sizeof(int) * fsi.size());
+        *io->pointReducedDensity = point;
+        rc = check_device_status(ctx);
+    }
+    return rc;
+}
+
+static int spike_common(nrg_context* ctx, int32_t iteration, const nrg_spike_io* io, bool cfs) {
+    NRG_TRY(need_model(ctx));
+    if (!io) return NRG_ERR_INVALID;
+    NRG_CUDA_TRY(cudaSetDevice(ctx->device));
+    const Model& M = ctx->model;
+    if (M.nMat == 0) { nrg_set_error_message("model has no spectrum tables"); return NRG_ERR_STATE; }
+    const int nVar = M.nVar, rs = nVar + 3, rsf = nVar + 6;
+    const int nbin = M.numberOfBin();
+    if (io->numberOfBin != nbin) {
+        nrg_set_error_message("numberOfBin %d, expected %d", io->numberOfBin, nbin);
+        return NRG_ERR_INVALID;
+    }
+    int st = NRG_OK;
+    const int nbf = io->numberOfBasisFull;
+    auto si = to_host(ctx, io->subspaceInfo, (size_t)io->numberOfSubspace * rs, &st); NRG_TRY(st);
+    auto bi = to_host(ctx, io->basis_input, (size_t)nbf * rs, &st); NRG_TRY(st);
+    auto bo = to_host(ctx, io->basis_output, (size_t)nbf * rs, &st); NRG_TRY(st);
+    auto E = to_host(ctx, io->eigenvalue, (size_t)nbf, &st); NRG_TRY(st);
+    Sectors S;
+    int rc = S.build(io->numberOfSubspace, si.data(), nbf, bi.data(), nVar, M.nOps);
+    if (rc == NRG_OK) rc = S.upload(ctx->stream);
+    if (rc != NRG_OK) { S.d_bi.release(); S.d_lst.release(); S.d_lstOff.release(); return rc; }
+    // eigenvalues back in sector order (the caller's array is in the truncation order)
+    std::vector<double> Esec(nbf, 0.0);
+    for (int i = 0; i < nbf; ++i) {
+        const int s = S.find(&bo[(size_t)i * rs]);
+        const int col = bo[(size_t)i * rs + nVar] - 1;
+        if (s < 0 || col < 0 || col >= S.dim[s]) { rc = NRG_ERR_INVALID; nrg_set_error_message("basis_output(%d) not in a sector", i + 1); break; }
+        Esec[S.start[s] + col] = E[i];
+    }
+    IterView it;
+    it.S = &S;
+    it.kept = kept_per_sector(S, io->numberOfBasis, bo.data());
+    it.rdm_off.assign(S.nsub, -1);
+    std::vector<int> gs;
+    if (rc == NRG_OK && cfs) {
+        auto map = to_host(ctx, io->mapFullSubspaceInfo, (size_t)(M.nIter + 2), &st); NRG_TRY(st);
+        auto fsi = to_host(ctx, io->fullSubspaceInfo, (size_t)io->elementNumFullSubspace * rsf, &st); NRG_TRY(st);
+        int r0, r1;
+        rc = full_range(map.data(), M.nIter, M.first, io->elementNumFullSubspace, iteration, &r0, &r1);
+        for (int j = r0; rc == NRG_OK && j < r1; ++j) {
+            const int* f = &fsi[(size_t)j * rsf];
+            const int s = S.find(f);
+            if (s < 0) continue;
+            if (f[nVar] != S.dim[s]) {   // calculateSpectrumDGEMM.F90:418-423
+                nrg_set_error_message("variation in fullSubspaceInfo and subspaceInfo is different");
+                rc = NRG_ERR_INVALID;
+                break;
+            }
+            it.kept[s] = f[nVar + 1];
+            it.rdm_off[s] = (long long)f[nVar + 5] - 1;
+        }
+    } else if (rc == NRG_OK) {
+        for (int i = 0; i < io->numberOfBasis; ++i)
+            if (E[i] < 1.0e-8) gs.push_back(S.find(&bo[(size_t)i * rs]));   // :56-75
+    }
+    const double *dV = nullptr, *dIMS = nullptr, *dR = nullptr;
+    double *dEs = nullptr;
+    if (rc == NRG_OK) rc = stage_in(ctx, io->eigenvector, (size_t)S.sizeV, kSlotIO + 9, &dV);
+    if (rc == NRG_OK) rc = stage_in(ctx, io->invariant_matrix_spectrum,
+                                    (size_t)io->numberOfBasis_old * io->numberOfBasis_old * M.nMat, kSlotIO + 10, &dIMS);
+    if (rc == NRG_OK && cfs) rc = stage_in(ctx, io->reducedDensityMatrix, (size_t)io->sizeOfReducedDensity, kSlotIO + 11, &dR);
+    DevBuf& bE = ctx->slot(kSlotIO + 12);
+    if (rc == NRG_OK) rc = bE.ensure(sizeof(double) * std::max(nbf, 1));
+    if (rc == NRG_OK && cudaMemcpyAsync(bE.p, Esec.data(), sizeof(double) * nbf, cudaMemcpyHostToDevice, ctx->stream) != cudaSuccess) rc = NRG_ERR_CUDA;
+    dEs = bE.as<double>();
+    it.d_V = dV; it.d_Esec = dEs; it.d_rdm = dR; it.nb_kept = io->numberOfBasis;
+    // per-iteration bins (tmpBinnedSpike*, :304-325), zeroed
+    const size_t nw = (size_t)nbin * M.nMat;
+    DevBuf& tb = ctx->slot(kSlotIO + 13);
+    DevBuf& tt = ctx->slot(kSlotIO + 14);
+    if (rc == NRG_OK) rc = tb.ensure(sizeof(double) * 2 * nw);
+    if (rc == NRG_OK) rc = tt.ensure(sizeof(double) * 4 * M.nMat);
+    double* tPos = tb.as<double>();
+    double* tNeg = tPos + nw;
+    double* tot = tt.as<double>();
+    if (rc == NRG_OK) rc = run_fill(ctx, tPos, (long long)(2 * nw), 0.0);
+    if (rc == NRG_OK) rc = run_fill(ctx, tot, 4LL * M.nMat, 0.0);
+    if (rc == NRG_OK) {
+        if (cfs) rc = spike_cfs_device(ctx, iteration, it, io->numberOfBasis_old, dIMS, dR, tPos, tNeg, tot);
+        else rc = spike_t0_device(ctx, iteration, it, gs, io->numberOfBasis_old, dIMS, tPos, tNeg);
+    }
+    // add into the caller's bins (weight column = second column)
+    std::vector<double> hp(nw), hn(nw);
+    if (rc == NRG_OK && cudaMemcpyAsync(hp.data(), tPos, sizeof(double) * nw, cudaMemcpyDeviceToHost, ctx->stream) != cudaSuccess) rc = NRG_ERR_CUDA;
+    if (rc == NRG_OK && cudaMemcpyAsync(hn.data(), tNeg, sizeof(double) * nw, cudaMemcpyDeviceToHost, ctx->stream) != cudaSuccess) rc = NRG_ERR_CUDA;
+    std::vector<double> htot(4 * M.nMat, 0.0);
+    if (rc == NRG_OK && cudaMemcpyAsync(htot.data(), tot, sizeof(double) * 2 * M.nMat, cudaMemcpyDeviceToHost, ctx->stream) != cudaSuccess) rc = NRG_ERR_CUDA;
+    if (cudaStreamSynchronize(ctx->stream) != cudaSuccess && rc == NRG_OK) rc = NRG_ERR_CUDA;
+    if (rc == NRG_OK) rc = check_device_status(ctx);
+    if (rc == NRG_OK) {
+        const bool dev_bins = is_device_ptr(io->binnedSpikePositive);
+        std::vector<double> bp, bn;
+        double *wp, *wn;
+        if (dev_bins) {
+            bp.resize(nw); bn.resize(nw);
+            cudaMemcpy(bp.data(), io->binnedSpikePositive + nw, sizeof(double) * nw, cudaMemcpyDeviceToHost);
+            cudaMemcpy(bn.data(), io->binnedSpikeNegative + nw, sizeof(double) * nw, cudaMemcpyDeviceToHost);
+            wp = bp.data(); wn = bn.data();
+        } else {
+            wp = io->binnedSpikePositive + nw;
+            wn = io->binnedSpikeNegative + nw;
+        }
+        for (int m = 0; m < M.nMat; ++m) {
+            double sp = 0.0, sn = 0.0;
+            for (int i = 0; i < nbin; ++i) { sp += hp[(size_t)m * nbin + i]; sn += hn[(size_t)m * nbin + i]; }
+            htot[2 * M.nMat + 2 * m] = sn;
+            htot[2 * M.nMat + 2 * m + 1] = sp;
+        }
+        for (size_t i = 0; i < nw; ++i) { wp[i] += hp[i]; wn[i] += hn[i]; }
+        if (dev_bins) {
+            cudaMemcpy(io->binnedSpikePositive + nw, bp.data(), sizeof(double) * nw, cudaMemcpyHostToDevice);
+            cudaMemcpy(io->binnedSpikeNegative + nw, bn.data(), sizeof(double) * nw, cudaMemcpyHostToDevice);
+        }
+        if (io->total_sum) {
+            // [raw negative, raw positive, binned negative, binned positive] per matrix
+            for (int m = 0; m < M.nMat; ++m) {
+                io->total_sum[4 * m + 0] = htot[2 * m + 0];
+                io->total_sum[4 * m + 1] = htot[2 * m + 1];
+                io->total_sum[4 * m + 2] = htot[2 * M.nMat + 2 * m];
+                io->total_sum[4 * m + 3] = htot[2 * M.nMat + 2 * m + 1];
+            }
+        }
+    }
+    S.d_bi.release(); S.d_lst.release(); S.d_lstOff.release();
+    return rc;
+}
+
+int nrg_spike_zero_temperature(nrg_context* ctx, int32_t iteration, const nrg_spike_io* io) {
+    return spike_common(ctx, iteration, io, false);
+}
+int nrg_spike_cfs(nrg_context* ctx, int32_t iteration, const nrg_spike_io* io) {
+    return spike_common(ctx, iteration, io, true);
+}
+
+}  // extern "C"

@@ -1,0 +1,148 @@
+// Grouped FP64 GEMM with gathered operands: one launch runs every (sector pair, matrix
+// type, local operation) product of a phase.  It replaces the per-pair dgemm calls of
+// invariantMatrixDGEMM.F90:300,316, invariantMatrixForSpectrumDGEMM.F90:296,312,
+// reducedDensityMatrixDGEMM.F90:280,296 and module.F90:1100,1113, without building the
+// reference's dense coefficient matrices: rows of the eigenvector blocks are gathered
+// through index lists instead.
+//
+//   C(i,j) = alpha * sum_k A(i,k) B(k,j) + beta * C(i,j)
+//   A(i,k) = A[ri(i)*a_si + k*a_sk]              ri = a_ri ? a_ri[i] : i
+//   B(k,j) = B[ki(k)*b_sk + ji(j)*b_sj]          ki = b_ki ? b_ki[k] : k, ji likewise
+//   C(i,j) = C[ci(i)*c_si + j*c_sj]              ci = c_ri ? c_ri[i] : i
+//
+// 64x64 output tiles, 256 threads with 4x4 register tiles, k slabs of 16 staged in
+// shared memory, double buffered.  Loads are coalesced along whichever index of each
+// operand has unit stride.
+#include "internal.hpp"
+
+namespace nrg {
+namespace {
+
+constexpr int TM = 64, TN = 64, TK = 16, NT = 256;
+constexpr int LDS = TM + 1;
+
+__device__ __forceinline__ void load_slab(const GemmProblem& P, int i0, int j0, int k0, double* As,
+                                          double* Bs, bool a_kfast, bool b_kfast) {
+    const int tid = threadIdx.x;
+#pragma unroll
+    for (int r = 0; r < (TM * TK) / NT; ++r) {
+        const int e = tid + r * NT;
+        int ii, kk;
+        if (a_kfast) { kk = e % TK; ii = e / TK; } else { ii = e % TM; kk = e / TM; }
+        const int gi = i0 + ii, gk = k0 + kk;
+        double v = 0.0;
+        if (gi < P.M && gk < P.K) {
+            const long long ri = P.a_ri ? P.a_ri[gi] : gi;
+            v = P.A[ri * P.a_si + (long long)gk * P.a_sk];
+        }
+        As[kk * LDS + ii] = v;
+    }
+#pragma unroll
+    for (int r = 0; r < (TN * TK) / NT; ++r) {
+        const int e = tid + r * NT;
+        int jj, kk;
+        if (b_kfast) { kk = e % TK; jj = e / TK; } else { jj = e % TN; kk = e / TN; }
+        const int gj = j0 + jj, gk = k0 + kk;
+        double v = 0.0;
+        if (gj < P.N && gk < P.K) {
+            const long long ki = P.b_ki ? P.b_ki[gk] : gk;
+            const long long ji = P.b_ji ? P.b_ji[gj] : gj;
+            v = P.B[ki * P.b_sk + ji * P.b_sj];
+        }
+        Bs[kk * LDS + jj] = v;
+    }
+}
+
+__global__ void __launch_bounds__(NT) k_ggemm(const GemmProblem* __restrict__ probs,
+                                              const int* __restrict__ tilePrefix, int nprob) {
+    __shared__ double As[2][TK * LDS];
+    __shared__ double Bs[2][TK * LDS];
+    const int bid = blockIdx.x;
+    int lo = 0, hi = nprob - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (tilePrefix[mid] <= bid) lo = mid; else hi = mid - 1;
+    }
+    const GemmProblem P = probs[lo];
+    const int t = bid - tilePrefix[lo];
+    const int tilesN = (P.N + TN - 1) / TN;
+    const int i0 = (t / tilesN) * TM, j0 = (t % tilesN) * TN;
+    const bool a_kfast = (P.a_sk == 1 && P.a_si != 1);
+    const bool b_kfast = (P.b_sk == 1 && P.b_sj != 1);
+    const int tx = threadIdx.x % 16, ty = threadIdx.x / 16;
+    double acc[4][4];
+#pragma unroll
+    for (int r = 0; r < 4; ++r)
+#pragma unroll
+        for (int c = 0; c < 4; ++c) acc[r][c] = 0.0;
+    const int nslab = (P.K + TK - 1) / TK;
+    if (nslab > 0) load_slab(P, i0, j0, 0, As[0], Bs[0], a_kfast, b_kfast);
+    __syncthreads();
+    for (int s = 0; s < nslab; ++s) {
+        const int cur = s & 1;
+        if (s + 1 < nslab) load_slab(P, i0, j0, (s + 1) * TK, As[cur ^ 1], Bs[cur ^ 1], a_kfast, b_kfast);
+        const double* as = As[cur];
+        const double* bs = Bs[cur];
+#pragma unroll
+        for (int kk = 0; kk < TK; ++kk) {
+            double a[4], b[4];
+#pragma unroll
+            for (int r = 0; r < 4; ++r) a[r] = as[kk * LDS + ty * 4 + r];
+#pragma unroll
+            for (int c = 0; c < 4; ++c) b[c] = bs[kk * LDS + tx + 16 * c];
+#pragma unroll
+            for (int r = 0; r < 4; ++r)
+#pragma unroll
+                for (int c = 0; c < 4; ++c) acc[r][c] = fma(a[r], b[c], acc[r][c]);
+        }
+        __syncthreads();
+    }
+#pragma unroll
+    for (int r = 0; r < 4; ++r) {
+        const int gi = i0 + ty * 4 + r;
+        if (gi >= P.M) continue;
+        const long long ci = P.c_ri ? P.c_ri[gi] : gi;
+#pragma unroll
+        for (int c = 0; c < 4; ++c) {
+            const int gj = j0 + tx + 16 * c;
+            if (gj >= P.N) continue;
+            double* out = P.C + ci * P.c_si + (long long)gj * P.c_sj;
+            const double v = P.alpha * acc[r][c];
+            *out = (P.beta == 0.0) ? v : P.beta * *out + v;
+        }
+    }
+}
+
+}  // namespace
+
+int launch_ggemm(nrg_context* ctx, std::vector<GemmProblem>& probs, int scratch_slot) {
+    // drop empty problems
+    std::vector<GemmProblem> live;
+    live.reserve(probs.size());
+    for (auto& p : probs)
+        if (p.M > 0 && p.N > 0 && p.K > 0) live.push_back(p);
+    const int np = (int)live.size();
+    if (np == 0) return NRG_OK;
+    std::vector<int> prefix(np);
+    long long total = 0;
+    for (int i = 0; i < np; ++i) {
+        live[i].tiles = ((live[i].M + TM - 1) / TM) * ((live[i].N + TN - 1) / TN);
+        prefix[i] = (int)total;
+        total += live[i].tiles;
+    }
+    if (total > 0x7fffffffLL) return NRG_ERR_TOO_LARGE;
+    DevBuf& dp = ctx->scratch.b[scratch_slot];
+    DevBuf& dq = ctx->scratch.b[scratch_slot + 1];
+    NRG_TRY(dp.ensure(sizeof(GemmProblem) * np));
+    NRG_TRY(dq.ensure(sizeof(int) * np));
+    NRG_CUDA_TRY(cudaMemcpyAsync(dp.p, live.data(), sizeof(GemmProblem) * np, cudaMemcpyHostToDevice, ctx->stream));
+    NRG_CUDA_TRY(cudaMemcpyAsync(dq.p, prefix.data(), sizeof(int) * np, cudaMemcpyHostToDevice, ctx->stream));
+    k_ggemm<<<(unsigned)total, NT, 0, ctx->stream>>>(dp.as<GemmProblem>(), dq.as<int>(), np);
+    ctx->launches++;
+    NRG_CUDA_TRY(cudaGetLastError());
+    // the problem table is host memory owned by this frame
+    NRG_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+    return NRG_OK;
+}
+
+}  // namespace nrg

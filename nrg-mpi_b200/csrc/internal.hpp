@@ -1,0 +1,186 @@
+// Internal structures shared by the C ABI (capi.cu), the device-resident driver
+// (driver.cu) and the kernels.
+#pragma once
+#include "common.cuh"
+
+#include <string>
+#include <vector>
+#include <map>
+#include <deque>
+
+namespace nrg {
+
+// ------------------------------------------------------------------------------------
+// grow-only device buffer
+// ------------------------------------------------------------------------------------
+struct DevBuf {
+    void* p = nullptr;
+    size_t bytes = 0;
+    int ensure(size_t want);
+    void release();
+    template <class T> T* as() const { return static_cast<T*>(p); }
+};
+
+// ------------------------------------------------------------------------------------
+// model tables (host copies + device copies + derived lookup tables)
+// ------------------------------------------------------------------------------------
+struct Model {
+    bool set = false;
+    int nIter = 0, nChain = 0, nVar = 0, cb[4] = {0, 0, 0, 0}, nMat = 0, nCM = 0, nCoef = 0,
+        nOps = 0, nBCS = 0, first = 0, flag_spectrum = 0, flag_BCS = 0;
+    double D = 1, z = 1, Lambda = 2;
+    int scalingType = 1, truncation = 0;
+    std::vector<int> operation;          // (nOps, nVar+nChain) col-major
+    std::vector<double> chain_diag;      // (nIter+2, nChain)
+    std::vector<double> chain_nond;      // (nIter+2-first, nChain)
+    std::vector<double> chain_bcs;       // (nIter+2, nChain)
+    std::vector<double> cspec;           // (nMat, nOps)
+    std::vector<int> cons_diff, pos_op, neg_op;  // (nMat, nVar)
+    // outcome of the coefficient scans, per (op_i, op_j) (diagonalization.F90:195-224)
+    std::vector<int> dflag, dtype, dch, dswp, bflag, bch;
+    std::vector<double> dcoef;
+    // invariantMatrixDGEMM.F90:248-254, per (op_l, op_r, type)
+    std::vector<int> imflag;
+    std::vector<double> imcoef;
+    // device copies
+    DevBuf d_operation, d_dflag, d_dtype, d_dch, d_dswp, d_bflag, d_bch, d_dcoef, d_imflag, d_imcoef;
+
+    double scale(int N) const;
+    double cd(int N, int c) const { return chain_diag[(size_t)N + (size_t)c * (nIter + 2)]; }
+    double cn(int N, int c) const { return chain_nond[(size_t)(N - first) + (size_t)c * (nIter + 2 - first)]; }
+    double cbcs(int N, int c) const { return chain_bcs.empty() ? 0.0 : chain_bcs[(size_t)N + (size_t)c * (nIter + 2)]; }
+    int op(int j, int col) const { return operation[(size_t)j + (size_t)col * nOps]; }
+    int numberOfBin() const;
+};
+
+// ------------------------------------------------------------------------------------
+// per-iteration sector tables built from subspaceInfo + basis_input
+// ------------------------------------------------------------------------------------
+struct Sectors {
+    int nsub = 0, nb = 0, nVar = 0, nOps = 0;
+    std::vector<int> qn;        // nsub*nVar
+    std::vector<int> dim, start;        // start: 0-based row of basis_input
+    std::vector<long long> ce;          // 0-based offset of the eigenvector block
+    long long sizeV = 0;
+    std::vector<int> rowOp, rowRef, rowVar;   // per row (0-based op / ref, 1-based var)
+    // rows of sector s with local operation a, ordered by variation: local row indices
+    std::vector<int> lst, lstOff;       // lstOff: nsub*nOps + 1
+    std::vector<int> refBase;           // nsub*nOps: 0-based reference of the first listed row
+    // device copies
+    DevBuf d_bi, d_lst, d_lstOff;
+    int build(int nsub, const int* si, int nb, const int* bi, int nVar, int nOps);
+    int upload(cudaStream_t st);
+    int find(const int* q) const;       // findSubspace: first sector with these qn, or -1
+    int cnt(int s, int a) const { return lstOff[s * nOps + a + 1] - lstOff[s * nOps + a]; }
+};
+
+// ------------------------------------------------------------------------------------
+// the context
+// ------------------------------------------------------------------------------------
+struct Scratch {
+    DevBuf b[24];
+};
+
+}  // namespace nrg
+
+struct nrg_context {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    nrg::Model model;
+    nrg::Scratch scratch;
+    nrg::DevBuf d_status;
+    long long launches = 0;
+    // driver-owned persistent storage, reused across runs
+    std::deque<nrg::DevBuf> store;
+    std::vector<nrg::Sectors> iter_sectors;
+    nrg::DevBuf& slot(size_t i) {
+        if (store.size() <= i) store.resize(i + 1);
+        return store[i];
+    }
+    ~nrg_context();
+};
+
+namespace nrg {
+
+// ---- grouped gather GEMM -------------------------------------------------------------
+struct GemmProblem {
+    int M, N, K;
+    int tiles;              // filled by the launcher
+    double alpha, beta;
+    const double* A; long long a_si, a_sk; const int* a_ri;   // A(i,k) = A[ri(i)*a_si + k*a_sk]
+    const double* B; long long b_sk, b_sj; const int* b_ki; const int* b_ji;
+    double* C; long long c_si, c_sj; const int* c_ri;
+};
+int launch_ggemm(nrg_context* ctx, std::vector<GemmProblem>& probs, int scratch_slot);
+
+// ---- kernels (kernels.cu) ------------------------------------------------------------
+int run_assemble(nrg_context* ctx, int iteration, const Sectors& S, const SyevSector* d_secs,
+                 const long long* d_colPrefix, const int* d_secStart, int nsec, long long ncols,
+                 const double* d_Eold, int nb_old, const double* d_IMold, double* d_V);
+int run_eig_finalize(nrg_context* ctx, double* d_E, int nb, long long sizeV, double* d_V,
+                     double* d_min_and_gs);
+
+struct ImGatherProb {
+    long long t_off;    // T (dL x kR) col-major
+    long long vR_off;   // V_R block
+    int L, R, t, dL, dR, kR, startL;
+};
+int run_im_gather(nrg_context* ctx, const Sectors& S, std::vector<ImGatherProb>& probs,
+                  const double* d_V, double* d_T);
+
+struct SpikeProb {
+    long long s_off, y_off;   // S, Y (kk x nl) col-major in the workspace (y_off < 0: T=0)
+    long long ek_off, el_off; // offsets into the energy array (k states, l states)
+    int kk, nl, m, toPos, lstride;  // lstride: 1 for consecutive l energies, 0 for a fixed one
+    double sgn, cE, scale, invpf;
+};
+int run_spikes(nrg_context* ctx, std::vector<SpikeProb>& probs, const double* d_work,
+               const double* d_E, int nbin, int nMat, double* d_binPos, double* d_binNeg,
+               double* d_tot);
+int run_fill(nrg_context* ctx, double* p, long long n, double v);
+int run_add(nrg_context* ctx, double* dst, const double* src, long long n);
+int run_sum_bins(nrg_context* ctx, const double* bins, int nbin, int nMat, double* out);
+int run_trace(nrg_context* ctx, const double* rdm, const long long* d_offs, const int* d_dims,
+              int nblk, double* out);
+int run_gather_rows(nrg_context* ctx, double* dst, long long dst_ld, const double* src,
+                    long long src_ld, const int* d_rows, int nrows, int ncols);
+
+// ---- internal routines shared by the ABI and the driver (routines.cu) ------------------
+struct DiagOut {
+    double groundStateEnergy = 0.0;
+};
+// diagonalization for one iteration; d_Eold/d_IMold/d_V/d_E are device pointers.
+int diag_device(nrg_context* ctx, int iteration, Sectors& S, const double* d_Eold, int nb_old,
+                const double* d_IMold, double* d_V, double* d_E, DiagOut* out);
+
+// kept counts per sector from the kept prefix of basis_output (invariantMatrixDGEMM.F90:84-100)
+std::vector<int> kept_per_sector(const Sectors& S, int nb_kept, const int* basis_output_kept);
+
+int invmat_device(nrg_context* ctx, const Sectors& S, const std::vector<int>& kept,
+                  const double* d_V, double* d_IM);
+int invmat_spec_device(nrg_context* ctx, const Sectors& S, const std::vector<int>& kept,
+                       const double* d_V, int nb_old, const double* d_IMSold, double* d_IMS);
+
+// rdm / spectrum inputs for one iteration (device resident)
+struct IterView {
+    const Sectors* S = nullptr;
+    std::vector<int> kept;            // kept per sector
+    const double* d_V = nullptr;      // all eigenvector blocks
+    const double* d_Esec = nullptr;   // eigenvalues in sector order
+    int nb_kept = 0;
+    // reduced density blocks of the kept sectors (row-major k x k), device offsets
+    const double* d_rdm = nullptr;
+    std::vector<long long> rdm_off;   // per sector, -1 when the sector has no kept state
+};
+int rdm_step_device(nrg_context* ctx, const IterView& present, const IterView& child,
+                    double* d_rdm, double* d_trace_out);
+int spike_cfs_device(nrg_context* ctx, int iteration, const IterView& it, int nb_old,
+                     const double* d_IMSold, const double* d_rdm, double* d_binPos,
+                     double* d_binNeg, double* d_tot);
+int spike_t0_device(nrg_context* ctx, int iteration, const IterView& it,
+                    const std::vector<int>& gs_sectors, int nb_old, const double* d_IMSold,
+                    double* d_binPos, double* d_binNeg);
+
+int check_device_status(nrg_context* ctx);
+
+}  // namespace nrg

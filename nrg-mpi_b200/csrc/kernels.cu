@@ -1,0 +1,370 @@
+// Element kernels of the NRG hot path: sector Hamiltonian assembly, the post-eigensolver
+// shift and chop, the sparse f^dagger gather, spike weights with log-grid binning, and
+// small helpers.  All arithmetic is FP64.
+#include "internal.hpp"
+
+#include <math.h>
+
+namespace nrg {
+namespace {
+
+constexpr int kMaxChain = 8;
+
+struct AsmParams {
+    int nb_old, nVar, nOps, nChain, nCM, flag_BCS, nsec, rec;
+    double sqrtL;
+    double cdiag[kMaxChain];   // chain_diagonal(iteration+1, c)
+    double cnond[kMaxChain];   // chain_nondiagonal(iteration, c)
+    double cbcs[kMaxChain];    // chain_BCS(iteration+1, c)
+};
+
+// Block Hamiltonian of diagonalization.F90:272-381.  One block per column of one sector.
+// Products are rounded one at a time (no fused multiply-add) in the reference's order.
+__global__ void k_assemble(const SyevSector* __restrict__ secs, const long long* __restrict__ colPrefix,
+                           const int* __restrict__ secStart, const int* __restrict__ bi,
+                           const double* __restrict__ Eold, const double* __restrict__ IMold,
+                           const int* __restrict__ operation, const int* __restrict__ dflag,
+                           const int* __restrict__ dtype, const int* __restrict__ dch,
+                           const int* __restrict__ dswp, const double* __restrict__ dcoef,
+                           const int* __restrict__ bflag, const int* __restrict__ bch,
+                           double* __restrict__ V, AsmParams P, int* status) {
+    const long long col = blockIdx.x;
+    int lo = 0, hi = P.nsec - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (colPrefix[mid] <= col) lo = mid; else hi = mid - 1;
+    }
+    const int s = lo;
+    const SyevSector sec = secs[s];
+    const int d = sec.n;
+    const int j = (int)(col - colPrefix[s]);
+    const int row0 = secStart[s];
+    const int R = P.rec;
+    const size_t nbo = (size_t)P.nb_old;
+    for (int i = threadIdx.x; i < d; i += blockDim.x) {
+        double v;
+        if (i == j) {
+            const int* r = bi + (size_t)(row0 + i) * R;
+            const int op = r[P.nVar + 2] - 1, ref = r[P.nVar] - 1;
+            if (ref < 0 || ref >= P.nb_old || op < 0 || op >= P.nOps) { atomicOr(status, NRG_DEV_BAD_INDEX); continue; }
+            v = __dmul_rn(Eold[ref], P.sqrtL);
+            for (int c = 0; c < P.nChain; ++c)
+                v = __dadd_rn(v, __dmul_rn((double)operation[op + (size_t)(P.nVar + c) * P.nOps], P.cdiag[c]));
+        } else {
+            const int p = i < j ? i : j, q = i < j ? j : i;
+            const int* rp = bi + (size_t)(row0 + p) * R;
+            const int* rq = bi + (size_t)(row0 + q) * R;
+            const int a = rp[P.nVar + 2] - 1, b = rq[P.nVar + 2] - 1;
+            const int refp = rp[P.nVar] - 1, refq = rq[P.nVar] - 1;
+            if (a < 0 || a >= P.nOps || b < 0 || b >= P.nOps) { atomicOr(status, NRG_DEV_BAD_INDEX); continue; }
+            const int idx = a * P.nOps + b;
+            const bool sw = dswp[idx] != 0;
+            const int ir = sw ? refq : refp, jr = sw ? refp : refq;
+            v = 0.0;
+            if (dflag[idx]) {
+                const int t = dtype[idx] - 1, ch = dch[idx] - 1;
+                if (ir < 0 || jr < 0 || ir >= P.nb_old || jr >= P.nb_old || t < 0 || t >= P.nCM ||
+                    ch < 0 || ch >= P.nChain) {
+                    atomicOr(status, NRG_DEV_BAD_INDEX);
+                    continue;
+                }
+                v = __dmul_rn(__dmul_rn(P.cnond[ch], dcoef[idx]),
+                              IMold[(size_t)jr + (size_t)ir * nbo + (size_t)t * nbo * nbo]);
+            }
+            if (P.flag_BCS && bflag[idx] && ir == jr) {
+                const int ch = bch[idx] - 1;
+                if (ch >= 0 && ch < P.nChain) v = P.cbcs[ch];
+            }
+        }
+        V[sec.a_off + (size_t)i + (size_t)j * d] = v;
+    }
+}
+
+// minimum of E and the ground-state energy eigenvalue(1) before the shift
+__global__ void k_min(const double* __restrict__ E, int n, double* out) {
+    __shared__ double red[32];
+    double m = INFINITY;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) m = fmin(m, E[i]);
+    for (int o = 16; o > 0; o >>= 1) m = fmin(m, __shfl_xor_sync(0xffffffffu, m, o));
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = m;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double r = INFINITY;
+        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) r = fmin(r, red[w]);
+        out[0] = r;
+        out[1] = E[0];
+    }
+}
+
+// diagonalization.F90:472-475
+__global__ void k_shift(double* __restrict__ E, int n, const double* __restrict__ mn) {
+    const double m = mn[0];
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        double e = E[i] - m;
+        if (e <= 1.0e-12) e = 0.0;
+        E[i] = e;
+    }
+}
+
+// diagonalization.F90:392-399
+__global__ void k_chop(double* __restrict__ V, long long n) {
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        if (fabs(V[i]) < 1.0e-14) V[i] = 0.0;
+    }
+}
+
+// T(i, j) = sum_b coef(a_i, b, t) V_R(rowOf(R, b, var_i), j), the sparse C_t of
+// invariantMatrixDGEMM.F90:236-256 applied to V_R(:, 1:k_R)
+__global__ void k_im_gather(const ImGatherProb* __restrict__ probs, const long long* __restrict__ prefix,
+                            int nprob, const int* __restrict__ bi, int rec, int nVar, int nOps, int nCM,
+                            const int* __restrict__ lst, const int* __restrict__ lstOff,
+                            const int* __restrict__ imflag, const double* __restrict__ imcoef,
+                            const double* __restrict__ V, double* __restrict__ T, long long total) {
+    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < total;
+         e += (long long)gridDim.x * blockDim.x) {
+        int lo = 0, hi = nprob - 1;
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (prefix[mid] <= e) lo = mid; else hi = mid - 1;
+        }
+        const ImGatherProb pr = probs[lo];
+        const long long loc = e - prefix[lo];
+        const int i = (int)(loc % pr.dL), j = (int)(loc / pr.dL);
+        const int* r = bi + (size_t)(pr.startL + i) * rec;
+        const int a = r[nVar + 2] - 1, var = r[nVar + 1];
+        double s = 0.0;
+        for (int b = 0; b < nOps; ++b) {
+            const int idx = (a * nOps + b) * nCM + pr.t;
+            if (!imflag[idx]) continue;
+            const int o0 = lstOff[pr.R * nOps + b], o1 = lstOff[pr.R * nOps + b + 1];
+            if (var < 1 || var > o1 - o0) continue;
+            const int row = lst[o0 + var - 1];
+            s = fma(imcoef[idx], V[pr.vR_off + (size_t)row + (size_t)j * pr.dR], s);
+        }
+        T[pr.t_off + loc] = s;
+    }
+}
+
+// spike weights w = S * Y (or S^2/pf at T=0) at energies sgn*(E_k - cE*E_l)*scale,
+// binned like binningSpike (module.F90:1210-1254); raw sums per (matrix, sign)
+__global__ void k_spikes(const SpikeProb* __restrict__ probs, const long long* __restrict__ prefix, int nprob,
+                         const double* __restrict__ W, const double* __restrict__ E, int nbin,
+                         double* __restrict__ binPos, double* __restrict__ binNeg,
+                         double* __restrict__ tot, long long total) {
+    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < total;
+         e += (long long)gridDim.x * blockDim.x) {
+        int lo = 0, hi = nprob - 1;
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (prefix[mid] <= e) lo = mid; else hi = mid - 1;
+        }
+        const SpikeProb pr = probs[lo];
+        const long long loc = e - prefix[lo];
+        const int k1 = (int)(loc % pr.kk), l = (int)(loc / pr.kk);
+        const double s = W[pr.s_off + loc];
+        double w;
+        if (pr.y_off >= 0) w = s * W[pr.y_off + loc];
+        else w = s * s * pr.invpf;
+        const double ek = E[pr.ek_off + k1];
+        const double el = E[pr.el_off + (long long)l * pr.lstride];
+        const double en = pr.sgn * ((ek - pr.cE * el) * pr.scale);
+        double* cont = pr.toPos ? binPos : binNeg;
+        atomicAdd(&tot[2 * pr.m + (pr.toPos ? 1 : 0)], w);
+        // binningSpike
+        const double position = (log10(fabs(en)) - (-15.0)) * 1000.0 + 1.0;
+        long long pref = (long long)position;   // int(): truncation toward zero
+        int i1 = 0;
+        if (position <= 0.0) i1 = 1;
+        else if (position >= (double)nbin) i1 = nbin;
+        if (pref <= 0) pref = 1;
+        const size_t base = (size_t)pr.m * nbin - 1;
+        if (i1 > 0) {
+            atomicAdd(&cont[base + i1], w);
+        } else {
+            const double wb = position - (double)pref;
+            atomicAdd(&cont[base + pref], w * (1.0 - wb));
+            atomicAdd(&cont[base + pref + 1], w * wb);
+        }
+    }
+}
+
+__global__ void k_fill(double* p, long long n, double v) {
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) p[i] = v;
+}
+__global__ void k_add(double* dst, const double* src, long long n) {
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) dst[i] += src[i];
+}
+// per matrix type: sum of the bins (sequential per type, deterministic)
+__global__ void k_sum_bins(const double* bins, int nbin, double* out) {
+    __shared__ double red[32];
+    const int m = blockIdx.x;
+    double s = 0.0;
+    for (int i = threadIdx.x; i < nbin; i += blockDim.x) s += bins[(size_t)m * nbin + i];
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double r = 0.0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) r += red[w];
+        out[m] = r;
+    }
+}
+// sum of the diagonals of row-major square blocks
+__global__ void k_trace(const double* rdm, const long long* offs, const int* dims, int nblk, double* out) {
+    __shared__ double red[32];
+    double s = 0.0;
+    for (int b = 0; b < nblk; ++b) {
+        const int n = dims[b];
+        for (int i = threadIdx.x; i < n; i += blockDim.x) s += rdm[offs[b] + (long long)i * n + i];
+    }
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double r = 0.0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) r += red[w];
+        out[0] = r;
+    }
+}
+__global__ void k_gather_rows(double* dst, long long dst_ld, const double* src, long long src_ld,
+                              const int* rows, int nrows, int ncols) {
+    const long long total = (long long)nrows * ncols;
+    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < total; e += (long long)gridDim.x * blockDim.x) {
+        const int i = (int)(e % nrows), j = (int)(e / nrows);
+        dst[(size_t)i + (size_t)j * dst_ld] = src[(size_t)rows[i] + (size_t)j * src_ld];
+    }
+}
+
+int grid_for(long long n, int threads) {
+    long long g = (n + threads - 1) / threads;
+    if (g < 1) g = 1;
+    if (g > 148 * 32) g = 148 * 32;
+    return (int)g;
+}
+
+}  // namespace
+
+int run_assemble(nrg_context* ctx, int iteration, const Sectors& S, const SyevSector* d_secs,
+                 const long long* d_colPrefix, const int* d_secStart, int nsec, long long ncols,
+                 const double* d_Eold, int nb_old, const double* d_IMold, double* d_V) {
+    const Model& M = ctx->model;
+    if (M.nChain > kMaxChain) return NRG_ERR_UNSUPPORTED;
+    AsmParams P;
+    P.nb_old = nb_old; P.nVar = M.nVar; P.nOps = M.nOps; P.nChain = M.nChain; P.nCM = M.nCM;
+    P.flag_BCS = M.flag_BCS; P.nsec = nsec; P.rec = M.nVar + 3;
+    P.sqrtL = sqrt(M.Lambda);
+    for (int c = 0; c < kMaxChain; ++c) {
+        P.cdiag[c] = c < M.nChain ? M.cd(iteration + 1, c) : 0.0;
+        P.cnond[c] = c < M.nChain ? M.cn(iteration, c) : 0.0;
+        P.cbcs[c] = (c < M.nChain && M.flag_BCS) ? M.cbcs(iteration + 1, c) : 0.0;
+    }
+    if (ncols == 0) return NRG_OK;
+    k_assemble<<<(unsigned)ncols, 128, 0, ctx->stream>>>(
+        d_secs, d_colPrefix, d_secStart, S.d_bi.as<int>(),
+        d_Eold, d_IMold, M.d_operation.as<int>(), M.d_dflag.as<int>(), M.d_dtype.as<int>(),
+        M.d_dch.as<int>(), M.d_dswp.as<int>(), M.d_dcoef.as<double>(), M.d_bflag.as<int>(),
+        M.d_bch.as<int>(), d_V, P, ctx->d_status.as<int>());
+    ctx->launches++;
+    NRG_CUDA_TRY(cudaGetLastError());
+    return NRG_OK;
+}
+
+int run_eig_finalize(nrg_context* ctx, double* d_E, int nb, long long sizeV, double* d_V,
+                     double* d_min_and_gs) {
+    k_min<<<1, 1024, 0, ctx->stream>>>(d_E, nb, d_min_and_gs);
+    k_shift<<<grid_for(nb, 256), 256, 0, ctx->stream>>>(d_E, nb, d_min_and_gs);
+    k_chop<<<grid_for(sizeV, 256), 256, 0, ctx->stream>>>(d_V, sizeV);
+    ctx->launches += 3;
+    NRG_CUDA_TRY(cudaGetLastError());
+    return NRG_OK;
+}
+
+int run_im_gather(nrg_context* ctx, const Sectors& S, std::vector<ImGatherProb>& probs,
+                  const double* d_V, double* d_T) {
+    const Model& M = ctx->model;
+    const int np = (int)probs.size();
+    if (np == 0) return NRG_OK;
+    std::vector<long long> prefix(np);
+    long long total = 0;
+    for (int p = 0; p < np; ++p) { prefix[p] = total; total += (long long)probs[p].dL * probs[p].kR; }
+    if (total == 0) return NRG_OK;
+    DevBuf& dp = ctx->scratch.b[16];
+    DevBuf& dq = ctx->scratch.b[17];
+    NRG_TRY(dp.ensure(sizeof(ImGatherProb) * np));
+    NRG_TRY(dq.ensure(sizeof(long long) * np));
+    NRG_CUDA_TRY(cudaMemcpyAsync(dp.p, probs.data(), sizeof(ImGatherProb) * np, cudaMemcpyHostToDevice, ctx->stream));
+    NRG_CUDA_TRY(cudaMemcpyAsync(dq.p, prefix.data(), sizeof(long long) * np, cudaMemcpyHostToDevice, ctx->stream));
+    k_im_gather<<<grid_for(total, 256), 256, 0, ctx->stream>>>(
+        dp.as<ImGatherProb>(), dq.as<long long>(), np, S.d_bi.as<int>(), M.nVar + 3, M.nVar, M.nOps,
+        M.nCM, S.d_lst.as<int>(), S.d_lstOff.as<int>(), M.d_imflag.as<int>(), M.d_imcoef.as<double>(),
+        d_V, d_T, total);
+    ctx->launches++;
+    NRG_CUDA_TRY(cudaGetLastError());
+    // the host vectors must stay alive until the copies ran
+    NRG_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+    return NRG_OK;
+}
+
+int run_spikes(nrg_context* ctx, std::vector<SpikeProb>& probs, const double* d_work,
+               const double* d_E, int nbin, int nMat, double* d_binPos, double* d_binNeg,
+               double* d_tot) {
+    (void)nMat;
+    const int np = (int)probs.size();
+    if (np == 0) return NRG_OK;
+    std::vector<long long> prefix(np);
+    long long total = 0;
+    for (int p = 0; p < np; ++p) { prefix[p] = total; total += (long long)probs[p].kk * probs[p].nl; }
+    if (total == 0) return NRG_OK;
+    DevBuf& dp = ctx->scratch.b[18];
+    DevBuf& dq = ctx->scratch.b[19];
+    NRG_TRY(dp.ensure(sizeof(SpikeProb) * np));
+    NRG_TRY(dq.ensure(sizeof(long long) * np));
+    NRG_CUDA_TRY(cudaMemcpyAsync(dp.p, probs.data(), sizeof(SpikeProb) * np, cudaMemcpyHostToDevice, ctx->stream));
+    NRG_CUDA_TRY(cudaMemcpyAsync(dq.p, prefix.data(), sizeof(long long) * np, cudaMemcpyHostToDevice, ctx->stream));
+    k_spikes<<<grid_for(total, 256), 256, 0, ctx->stream>>>(dp.as<SpikeProb>(), dq.as<long long>(), np, d_work,
+                                                          d_E, nbin, d_binPos, d_binNeg, d_tot, total);
+    ctx->launches++;
+    NRG_CUDA_TRY(cudaGetLastError());
+    NRG_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+    return NRG_OK;
+}
+
+int run_fill(nrg_context* ctx, double* p, long long n, double v) {
+    if (n <= 0) return NRG_OK;
+    k_fill<<<grid_for(n, 256), 256, 0, ctx->stream>>>(p, n, v);
+    ctx->launches++;
+    NRG_CUDA_TRY(cudaGetLastError());
+    return NRG_OK;
+}
+int run_add(nrg_context* ctx, double* dst, const double* src, long long n) {
+    if (n <= 0) return NRG_OK;
+    k_add<<<grid_for(n, 256), 256, 0, ctx->stream>>>(dst, src, n);
+    ctx->launches++;
+    NRG_CUDA_TRY(cudaGetLastError());
+    return NRG_OK;
+}
+int run_sum_bins(nrg_context* ctx, const double* bins, int nbin, int nMat, double* out) {
+    if (nMat <= 0) return NRG_OK;
+    k_sum_bins<<<nMat, 1024, 0, ctx->stream>>>(bins, nbin, out);
+    ctx->launches++;
+    NRG_CUDA_TRY(cudaGetLastError());
+    return NRG_OK;
+}
+int run_trace(nrg_context* ctx, const double* rdm, const long long* d_offs, const int* d_dims,
+              int nblk, double* out) {
+    k_trace<<<1, 1024, 0, ctx->stream>>>(rdm, d_offs, d_dims, nblk, out);
+    ctx->launches++;
+    NRG_CUDA_TRY(cudaGetLastError());
+    return NRG_OK;
+}
+int run_gather_rows(nrg_context* ctx, double* dst, long long dst_ld, const double* src,
+                    long long src_ld, const int* d_rows, int nrows, int ncols) {
+    const long long n = (long long)nrows * ncols;
+    if (n <= 0) return NRG_OK;
+    k_gather_rows<<<grid_for(n, 256), 256, 0, ctx->stream>>>(dst, dst_ld, src, src_ld, d_rows, nrows, ncols);
+    ctx->launches++;
+    NRG_CUDA_TRY(cudaGetLastError());
+    return NRG_OK;
+}
+
+}  // namespace nrg

@@ -1,0 +1,603 @@
+// Device-side implementations of the reference routines, shared by the C ABI (capi.cu)
+// and the device-resident driver (driver.cu).
+#include "internal.hpp"
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <numeric>
+
+namespace nrg {
+
+// ------------------------------------------------------------------------------------
+// DevBuf
+// ------------------------------------------------------------------------------------
+int DevBuf::ensure(size_t want) {
+    if (want <= bytes && p) return NRG_OK;
+    if (p) cudaFree(p);
+    p = nullptr;
+    bytes = 0;
+    size_t sz = want < 256 ? 256 : want;
+    sz = (sz + 255) & ~size_t(255);
+    cudaError_t e = cudaMalloc(&p, sz);
+    if (e != cudaSuccess) {
+        p = nullptr;
+        nrg_set_error_message("cudaMalloc(%zu) failed: %s", sz, cudaGetErrorString(e));
+        return NRG_ERR_NOMEM;
+    }
+    bytes = sz;
+    return NRG_OK;
+}
+void DevBuf::release() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    bytes = 0;
+}
+
+// ------------------------------------------------------------------------------------
+// Model
+// ------------------------------------------------------------------------------------
+double Model::scale(int N) const {
+    // module.F90:690-711
+    if (scalingType == 0) return std::pow(Lambda, -double(N) * 0.5);
+    if (scalingType == 1)
+        return D * 0.5 * (1.0 + 1.0 / Lambda) * std::pow(Lambda, -double(N) * 0.5 - z + 1.0);
+    return std::pow(Lambda, -double(N) * 0.5 - z) * D * (Lambda - 1.0) / std::log(Lambda);
+}
+int Model::numberOfBin() const {
+    // main.F90:142-144
+    const double Emax = scale(-1);
+    const double log10Emax = double((int)std::log10(Emax)) + 1.0;
+    return (int)(log10Emax - (-15.0)) * 1000 + 1;
+}
+
+// ------------------------------------------------------------------------------------
+// Sectors
+// ------------------------------------------------------------------------------------
+int Sectors::build(int nsub_, const int* si, int nb_, const int* bi, int nVar_, int nOps_) {
+    nsub = nsub_; nb = nb_; nVar = nVar_; nOps = nOps_;
+    const int rs = nVar + 3;
+    qn.assign((size_t)nsub * nVar, 0);
+    dim.assign(nsub, 0);
+    start.assign(nsub, 0);
+    ce.assign(nsub, 0);
+    long long acc = 0;
+    for (int s = 0; s < nsub; ++s) {
+        for (int v = 0; v < nVar; ++v) qn[(size_t)s * nVar + v] = si[(size_t)s * rs + v];
+        dim[s] = si[(size_t)s * rs + nVar];
+        start[s] = si[(size_t)s * rs + nVar + 2] - 1;
+        ce[s] = acc;
+        const long long ref_ce = (long long)si[(size_t)s * rs + nVar + 1] - 1;
+        if (acc < 0x7fffffffLL && ref_ce != acc) {
+            nrg_set_error_message("subspaceInfo(%d)%%count_eigenvector=%lld, expected %lld", s + 1,
+                                  ref_ce + 1, acc + 1);
+            return NRG_ERR_INVALID;
+        }
+        if (dim[s] < 1 || start[s] < 0 || start[s] + dim[s] > nb) {
+            nrg_set_error_message("subspaceInfo(%d) out of range", s + 1);
+            return NRG_ERR_INVALID;
+        }
+        acc += (long long)dim[s] * dim[s];
+    }
+    sizeV = acc;
+    rowOp.resize(nb); rowRef.resize(nb); rowVar.resize(nb);
+    for (int i = 0; i < nb; ++i) {
+        rowRef[i] = bi[(size_t)i * rs + nVar] - 1;
+        rowVar[i] = bi[(size_t)i * rs + nVar + 1];
+        rowOp[i] = bi[(size_t)i * rs + nVar + 2] - 1;
+        if (rowOp[i] < 0 || rowOp[i] >= nOps) {
+            nrg_set_error_message("basis_input(%d)%%operation out of range", i + 1);
+            return NRG_ERR_INVALID;
+        }
+    }
+    // rows per (sector, operation), in row order
+    lstOff.assign((size_t)nsub * nOps + 1, 0);
+    for (int s = 0; s < nsub; ++s)
+        for (int i = start[s]; i < start[s] + dim[s]; ++i) lstOff[(size_t)s * nOps + rowOp[i] + 1]++;
+    for (size_t x = 1; x < lstOff.size(); ++x) lstOff[x] += lstOff[x - 1];
+    lst.assign(lstOff.back(), 0);
+    std::vector<int> fill(lstOff.begin(), lstOff.end() - 1);
+    for (int s = 0; s < nsub; ++s)
+        for (int i = start[s]; i < start[s] + dim[s]; ++i)
+            lst[fill[(size_t)s * nOps + rowOp[i]]++] = i - start[s];
+    // the rows of one (sector, operation) descend from one previous sector: they must list
+    // its states by column 1, 2, ... with consecutive references
+    refBase.assign((size_t)nsub * nOps, -1);
+    for (int s = 0; s < nsub; ++s) {
+        for (int a = 0; a < nOps; ++a) {
+            const int o0 = lstOff[(size_t)s * nOps + a], o1 = lstOff[(size_t)s * nOps + a + 1];
+            if (o1 == o0) continue;
+            const int r0 = rowRef[start[s] + lst[o0]];
+            refBase[(size_t)s * nOps + a] = r0;
+            for (int q = o0; q < o1; ++q) {
+                const int row = start[s] + lst[q];
+                if (rowVar[row] != q - o0 + 1 || rowRef[row] != r0 + (q - o0)) {
+                    nrg_set_error_message(
+                        "sector %d operation %d: rows are not the previous sector's states in "
+                        "column order (variation %d, reference %d)", s + 1, a + 1, rowVar[row],
+                        rowRef[row] + 1);
+                    return NRG_ERR_UNSUPPORTED;
+                }
+            }
+        }
+    }
+    return NRG_OK;
+}
+
+int Sectors::upload(cudaStream_t st) {
+    const int rs = nVar + 3;
+    std::vector<int> bi((size_t)nb * rs, 0);
+    for (int i = 0; i < nb; ++i) {
+        bi[(size_t)i * rs + nVar] = rowRef[i] + 1;
+        bi[(size_t)i * rs + nVar + 1] = rowVar[i];
+        bi[(size_t)i * rs + nVar + 2] = rowOp[i] + 1;
+    }
+    NRG_TRY(d_bi.ensure(sizeof(int) * bi.size()));
+    NRG_TRY(d_lst.ensure(sizeof(int) * (lst.size() + 1)));
+    NRG_TRY(d_lstOff.ensure(sizeof(int) * lstOff.size()));
+    NRG_CUDA_TRY(cudaMemcpyAsync(d_bi.p, bi.data(), sizeof(int) * bi.size(), cudaMemcpyHostToDevice, st));
+    if (!lst.empty())
+        NRG_CUDA_TRY(cudaMemcpyAsync(d_lst.p, lst.data(), sizeof(int) * lst.size(), cudaMemcpyHostToDevice, st));
+    NRG_CUDA_TRY(cudaMemcpyAsync(d_lstOff.p, lstOff.data(), sizeof(int) * lstOff.size(), cudaMemcpyHostToDevice, st));
+    NRG_CUDA_TRY(cudaStreamSynchronize(st));
+    return NRG_OK;
+}
+
+int Sectors::find(const int* q) const {
+    for (int s = 0; s < nsub; ++s) {
+        bool eq = true;
+        for (int v = 0; v < nVar; ++v)
+            if (qn[(size_t)s * nVar + v] != q[v]) { eq = false; break; }
+        if (eq) return s;
+    }
+    return -1;
+}
+
+int check_device_status(nrg_context* ctx) {
+    int st = 0;
+    NRG_CUDA_TRY(cudaMemcpyAsync(&st, ctx->d_status.p, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+    NRG_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+    if (st != 0) {
+        NRG_CUDA_TRY(cudaMemsetAsync(ctx->d_status.p, 0, sizeof(int), ctx->stream));
+        nrg_set_error_message("device status flags 0x%x (1: index out of range, 4: secular root)", st);
+        return (st & NRG_DEV_SECULAR) ? NRG_ERR_NUMERIC : NRG_ERR_INVALID;
+    }
+    return NRG_OK;
+}
+
+// ------------------------------------------------------------------------------------
+// diagonalization (diagonalization.F90:185-528)
+// ------------------------------------------------------------------------------------
+int diag_device(nrg_context* ctx, int iteration, Sectors& S, const double* d_Eold, int nb_old,
+                const double* d_IMold, double* d_V, double* d_E, DiagOut* out) {
+    const int nsec = S.nsub;
+    std::vector<int> order(nsec);
+    std::iota(order.begin(), order.end(), 0);
+    std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return S.dim[a] > S.dim[b]; });
+    std::vector<SyevSector> secs(nsec);
+    std::vector<long long> colPrefix(nsec);
+    std::vector<int> secStart(nsec);
+    long long wsd = 0, wsi = 0, cols = 0;
+    int max_n = 1;
+    for (int x = 0; x < nsec; ++x) {
+        const int s = order[x];
+        SyevSector& q = secs[x];
+        q.n = S.dim[s];
+        q.a_off = S.ce[s];
+        q.e_off = S.start[s];
+        q.w_off = wsd;
+        q.i_off = wsi;
+        q.pad = 0;
+        wsd += syev_ws_doubles(q.n);
+        wsi += syev_ws_ints(q.n);
+        colPrefix[x] = cols;
+        cols += q.n;
+        secStart[x] = S.start[s];
+        max_n = std::max(max_n, q.n);
+    }
+    DevBuf& bsec = ctx->scratch.b[0];
+    DevBuf& bcol = ctx->scratch.b[1];
+    DevBuf& bstart = ctx->scratch.b[2];
+    DevBuf& bwd = ctx->scratch.b[3];
+    DevBuf& bwi = ctx->scratch.b[4];
+    DevBuf& bmin = ctx->scratch.b[5];
+    NRG_TRY(bsec.ensure(sizeof(SyevSector) * nsec));
+    NRG_TRY(bcol.ensure(sizeof(long long) * nsec));
+    NRG_TRY(bstart.ensure(sizeof(int) * nsec));
+    NRG_TRY(bwd.ensure(sizeof(double) * (size_t)wsd));
+    NRG_TRY(bwi.ensure(sizeof(int) * (size_t)wsi));
+    NRG_TRY(bmin.ensure(sizeof(double) * 2));
+    NRG_CUDA_TRY(cudaMemcpyAsync(bsec.p, secs.data(), sizeof(SyevSector) * nsec, cudaMemcpyHostToDevice, ctx->stream));
+    NRG_CUDA_TRY(cudaMemcpyAsync(bcol.p, colPrefix.data(), sizeof(long long) * nsec, cudaMemcpyHostToDevice, ctx->stream));
+    NRG_CUDA_TRY(cudaMemcpyAsync(bstart.p, secStart.data(), sizeof(int) * nsec, cudaMemcpyHostToDevice, ctx->stream));
+    NRG_TRY(run_assemble(ctx, iteration, S, bsec.as<SyevSector>(), bcol.as<long long>(), bstart.as<int>(),
+                         nsec, cols, d_Eold, nb_old, d_IMold, d_V));
+    NRG_TRY(launch_syev(bsec.as<SyevSector>(), nsec, max_n, d_V, d_E, bwd.as<double>(), bwi.as<int>(),
+                        ctx->d_status.as<int>(), ctx->stream));
+    ctx->launches++;
+    NRG_TRY(run_eig_finalize(ctx, d_E, S.nb, S.sizeV, d_V, bmin.as<double>()));
+    double mg[2];
+    NRG_CUDA_TRY(cudaMemcpyAsync(mg, bmin.p, sizeof(double) * 2, cudaMemcpyDeviceToHost, ctx->stream));
+    NRG_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+    if (out) out->groundStateEnergy = mg[1];
+    return check_device_status(ctx);
+}
+
+std::vector<int> kept_per_sector(const Sectors& S, int nb_kept, const int* bo) {
+    // invariantMatrixDGEMM.F90:84-100: count kept states whose quantum numbers match
+    std::vector<int> kept(S.nsub, 0);
+    const int rs = S.nVar + 3;
+    for (int i = 0; i < nb_kept; ++i) {
+        const int s = S.find(bo + (size_t)i * rs);
+        if (s >= 0) kept[s]++;
+    }
+    return kept;
+}
+
+// ------------------------------------------------------------------------------------
+// invariant matrices
+// ------------------------------------------------------------------------------------
+int invmat_device(nrg_context* ctx, const Sectors& S, const std::vector<int>& kept,
+                  const double* d_V, double* d_IM) {
+    // invariantMatrixDGEMM.F90:67-341
+    const Model& M = ctx->model;
+    const int nsub = S.nsub, nVar = S.nVar;
+    std::vector<long long> kst(nsub + 1, 0);
+    for (int s = 0; s < nsub; ++s) kst[s + 1] = kst[s] + kept[s];
+    const long long nbk = kst[nsub];
+    NRG_TRY(run_fill(ctx, d_IM, nbk * nbk * M.nCM, 0.0));
+    const int cs = M.cb[0], ce_ = M.cb[2], ss = M.cb[1], se = M.cb[3];
+    std::vector<ImGatherProb> gp;
+    long long toff = 0;
+    for (int L = 0; L < nsub; ++L) {
+        if (kept[L] == 0) continue;
+        for (int R = 0; R < nsub; ++R) {
+            if (kept[R] == 0) continue;
+            int dQ = 0, dS = 0;
+            for (int v = ss; v <= se; ++v) dS += S.qn[(size_t)L * nVar + v - 1] - S.qn[(size_t)R * nVar + v - 1];
+            if (cs == ce_ && cs == 0) {
+                if (std::abs(dS) != 1) continue;
+            } else {
+                for (int v = cs; v <= ce_; ++v) dQ += S.qn[(size_t)L * nVar + v - 1] - S.qn[(size_t)R * nVar + v - 1];
+                if (dQ != 1 || std::abs(dS) != 1) continue;
+            }
+            for (int t = 0; t < M.nCM; ++t) {
+                ImGatherProb p;
+                p.t_off = toff; p.vR_off = S.ce[R]; p.L = L; p.R = R; p.t = t;
+                p.dL = S.dim[L]; p.dR = S.dim[R]; p.kR = kept[R]; p.startL = S.start[L];
+                gp.push_back(p);
+                toff += (long long)p.dL * p.kR;
+            }
+        }
+    }
+    if (gp.empty()) return NRG_OK;
+    DevBuf& T = ctx->scratch.b[6];
+    NRG_TRY(T.ensure(sizeof(double) * (size_t)toff));
+    NRG_TRY(run_im_gather(ctx, S, gp, d_V, T.as<double>()));
+    std::vector<GemmProblem> probs;
+    for (const auto& g : gp) {
+        GemmProblem P;
+        std::memset(&P, 0, sizeof(P));
+        P.M = kept[g.L]; P.N = kept[g.R]; P.K = g.dL;
+        P.alpha = 1.0; P.beta = 0.0;
+        P.A = d_V + S.ce[g.L]; P.a_si = g.dL; P.a_sk = 1;
+        P.B = T.as<double>() + g.t_off; P.b_sk = 1; P.b_sj = g.dL;
+        P.C = d_IM + kst[g.R] + kst[g.L] * nbk + (long long)g.t * nbk * nbk;
+        P.c_si = nbk; P.c_sj = 1;
+        probs.push_back(P);
+    }
+    return launch_ggemm(ctx, probs, 8);
+}
+
+int invmat_spec_device(nrg_context* ctx, const Sectors& S, const std::vector<int>& kept,
+                       const double* d_V, int nb_old, const double* d_IMSold, double* d_IMS) {
+    // invariantMatrixForSpectrumDGEMM.F90:71-370
+    const Model& M = ctx->model;
+    const int nsub = S.nsub, nVar = S.nVar, nOps = S.nOps;
+    std::vector<long long> kst(nsub + 1, 0);
+    for (int s = 0; s < nsub; ++s) kst[s + 1] = kst[s] + kept[s];
+    const long long nbk = kst[nsub];
+    const long long nbo = nb_old;
+    NRG_TRY(run_fill(ctx, d_IMS, nbk * nbk * M.nMat, 0.0));
+    struct Pair { int L, R, m; long long t_off; };
+    std::vector<Pair> pairs;
+    long long toff = 0;
+    for (int L = 0; L < nsub; ++L) {
+        if (kept[L] == 0) continue;
+        for (int R = 0; R < nsub; ++R) {
+            if (kept[R] == 0) continue;
+            for (int m = 0; m < M.nMat; ++m) {
+                bool ok = true;
+                for (int v = 0; v < nVar; ++v)
+                    if (S.qn[(size_t)L * nVar + v] - S.qn[(size_t)R * nVar + v] !=
+                        M.cons_diff[(size_t)m + (size_t)v * M.nMat]) { ok = false; break; }
+                if (!ok) continue;
+                pairs.push_back({L, R, m, toff});
+                toff += (long long)S.dim[L] * kept[R];
+            }
+        }
+    }
+    if (pairs.empty()) return NRG_OK;
+    DevBuf& T = ctx->scratch.b[6];
+    NRG_TRY(T.ensure(sizeof(double) * (size_t)toff));
+    NRG_TRY(run_fill(ctx, T.as<double>(), toff, 0.0));
+    std::vector<GemmProblem> p1, p2;
+    const int* dl = S.d_lst.as<int>();
+    for (const auto& pr : pairs) {
+        const int L = pr.L, R = pr.R, m = pr.m;
+        for (int a = 0; a < nOps; ++a) {
+            const int cL = S.cnt(L, a), cR = S.cnt(R, a);
+            if (cL == 0 || cR == 0) continue;
+            GemmProblem P;
+            std::memset(&P, 0, sizeof(P));
+            P.M = cL; P.N = kept[R]; P.K = cR;
+            P.alpha = M.cspec[(size_t)m + (size_t)a * M.nMat]; P.beta = 0.0;
+            P.A = d_IMSold + S.refBase[(size_t)R * nOps + a] + (long long)S.refBase[(size_t)L * nOps + a] * nbo +
+                  (long long)m * nbo * nbo;
+            P.a_si = nbo; P.a_sk = 1;
+            P.B = d_V + S.ce[R]; P.b_ki = dl + S.lstOff[(size_t)R * nOps + a]; P.b_sk = 1; P.b_sj = S.dim[R];
+            P.C = T.as<double>() + pr.t_off; P.c_ri = dl + S.lstOff[(size_t)L * nOps + a];
+            P.c_si = 1; P.c_sj = S.dim[L];
+            p1.push_back(P);
+        }
+        GemmProblem Q;
+        std::memset(&Q, 0, sizeof(Q));
+        Q.M = kept[L]; Q.N = kept[R]; Q.K = S.dim[L];
+        Q.alpha = 1.0; Q.beta = 0.0;
+        Q.A = d_V + S.ce[L]; Q.a_si = S.dim[L]; Q.a_sk = 1;
+        Q.B = T.as<double>() + pr.t_off; Q.b_sk = 1; Q.b_sj = S.dim[L];
+        Q.C = d_IMS + kst[R] + kst[L] * nbk + (long long)m * nbk * nbk; Q.c_si = nbk; Q.c_sj = 1;
+        p2.push_back(Q);
+    }
+    NRG_TRY(launch_ggemm(ctx, p1, 8));
+    return launch_ggemm(ctx, p2, 10);
+}
+
+// ------------------------------------------------------------------------------------
+// backward reduced density matrix step (reducedDensityMatrixDGEMM.F90:115-321)
+// ------------------------------------------------------------------------------------
+int rdm_step_device(nrg_context* ctx, const IterView& P, const IterView& C, double* d_rdm,
+                    double* d_trace_out) {
+    const Model& M = ctx->model;
+    const Sectors& SP = *P.S;
+    const Sectors& SC = *C.S;
+    const int nVar = SP.nVar, nOps = SP.nOps;
+    struct Blk { int s; int n; long long off; };
+    std::vector<Blk> blocks;
+    std::vector<GemmProblem> p1;
+    std::vector<std::vector<GemmProblem>> p2(nOps);
+    std::vector<long long> toffs;
+    long long ttot = 0;
+    DevBuf& T = ctx->scratch.b[6];
+    // first pass: sizes
+    struct Link { int S, c, op; long long colOff; };
+    std::vector<Link> links;
+    std::vector<long long> tS(SP.nsub, -1);
+    std::vector<int> q(nVar);
+    for (int s = 0; s < SP.nsub; ++s) {
+        const int n = P.kept[s];
+        if (n == 0) continue;
+        long long colOff = 0;
+        for (int op = 0; op < nOps; ++op) {
+            for (int v = 0; v < nVar; ++v) q[v] = SP.qn[(size_t)s * nVar + v] - M.op(op, v);
+            const int c = SC.find(q.data());
+            if (c < 0 || C.kept[c] == 0) continue;
+            if (SC.cnt(c, op) != n) {
+                nrg_set_error_message("rdm: child sector rows (%d) differ from kept states (%d)",
+                                      SC.cnt(c, op), n);
+                return NRG_ERR_INVALID;
+            }
+            links.push_back({s, c, op, colOff});
+            colOff += C.kept[c];
+        }
+        tS[s] = ttot;
+        ttot += (long long)n * colOff;
+        blocks.push_back({s, n, P.rdm_off[s]});
+    }
+    NRG_TRY(T.ensure(sizeof(double) * (size_t)std::max(ttot, 1LL)));
+    const int* dl = SC.d_lst.as<int>();
+    for (const auto& lk : links) {
+        const int n = P.kept[lk.S], c = lk.c, kc = C.kept[c], dc = SC.dim[c];
+        const int* rows = dl + SC.lstOff[(size_t)c * nOps + lk.op];
+        // T_op = A_op rho_c, A_op(i, k) = V_c(rows[i], k); rho_c row-major
+        GemmProblem A;
+        std::memset(&A, 0, sizeof(A));
+        A.M = n; A.N = kc; A.K = kc; A.alpha = 1.0; A.beta = 0.0;
+        A.A = C.d_V + SC.ce[c]; A.a_ri = rows; A.a_si = 1; A.a_sk = dc;
+        A.B = d_rdm + C.rdm_off[c]; A.b_sk = kc; A.b_sj = 1;
+        A.C = T.as<double>() + tS[lk.S] + lk.colOff * n; A.c_si = 1; A.c_sj = n;
+        p1.push_back(A);
+        // rho_S += T_op A_op^T (row-major store)
+        GemmProblem B;
+        std::memset(&B, 0, sizeof(B));
+        B.M = n; B.N = n; B.K = kc; B.alpha = 1.0; B.beta = 1.0;
+        B.A = T.as<double>() + tS[lk.S] + lk.colOff * n; B.a_si = 1; B.a_sk = n;
+        B.B = C.d_V + SC.ce[c]; B.b_sk = dc; B.b_ji = rows; B.b_sj = 1;
+        B.C = d_rdm + P.rdm_off[lk.S]; B.c_si = n; B.c_sj = 1;
+        p2[lk.op].push_back(B);
+    }
+    for (const auto& b : blocks) NRG_TRY(run_fill(ctx, d_rdm + b.off, (long long)b.n * b.n, 0.0));
+    NRG_TRY(launch_ggemm(ctx, p1, 8));
+    for (int op = 0; op < nOps; ++op) NRG_TRY(launch_ggemm(ctx, p2[op], 10));
+    if (d_trace_out && !blocks.empty()) {
+        std::vector<long long> offs;
+        std::vector<int> dims;
+        for (const auto& b : blocks) { offs.push_back(b.off); dims.push_back(b.n); }
+        DevBuf& bo = ctx->scratch.b[12];
+        DevBuf& bd = ctx->scratch.b[13];
+        NRG_TRY(bo.ensure(sizeof(long long) * offs.size()));
+        NRG_TRY(bd.ensure(sizeof(int) * dims.size()));
+        NRG_CUDA_TRY(cudaMemcpyAsync(bo.p, offs.data(), sizeof(long long) * offs.size(), cudaMemcpyHostToDevice, ctx->stream));
+        NRG_CUDA_TRY(cudaMemcpyAsync(bd.p, dims.data(), sizeof(int) * dims.size(), cudaMemcpyHostToDevice, ctx->stream));
+        NRG_TRY(run_trace(ctx, d_rdm, bo.as<long long>(), bd.as<int>(), (int)blocks.size(), d_trace_out));
+        NRG_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+    }
+    return NRG_OK;
+}
+
+// ------------------------------------------------------------------------------------
+// spectrum: spikeCFS (calculateSpectrumDGEMM.F90:217-646) and spikeZeroTemperature (:1-215)
+// ------------------------------------------------------------------------------------
+namespace {
+
+struct SpecJob {
+    int k, l;          // k sector (kept columns / all columns at T=0), l sector
+    int kk, c0, nl;    // columns of k used, first l column, number of l columns
+    int m, part;       // part 0: <k|d^dag|l>, part 1: <l|d^dag|k>
+    double sgn, cE, invpf;
+    int toPos;
+    long long rdm_off; // -1: T=0 weights
+    long long t_off, s_off, y_off;
+};
+
+int run_spec_jobs(nrg_context* ctx, const IterView& it, std::vector<SpecJob>& jobs, int nb_old,
+                  const double* d_IMSold, double sc, int nbin, double* d_binPos, double* d_binNeg,
+                  double* d_tot) {
+    const Model& M = ctx->model;
+    const Sectors& S = *it.S;
+    const int nOps = S.nOps;
+    const long long nbo = nb_old;
+    long long ttot = 0, stot = 0;
+    for (auto& j : jobs) {
+        j.t_off = ttot;
+        ttot += (long long)S.dim[j.k] * j.nl;
+        j.s_off = stot;
+        stot += (long long)j.kk * j.nl;
+        if (j.rdm_off >= 0) { j.y_off = stot; stot += (long long)j.kk * j.nl; } else j.y_off = -1;
+    }
+    if (jobs.empty()) return NRG_OK;
+    DevBuf& T = ctx->scratch.b[6];
+    DevBuf& W = ctx->scratch.b[7];
+    NRG_TRY(T.ensure(sizeof(double) * (size_t)std::max(ttot, 1LL)));
+    NRG_TRY(W.ensure(sizeof(double) * (size_t)std::max(stot, 1LL)));
+    NRG_TRY(run_fill(ctx, T.as<double>(), ttot, 0.0));
+    const int* dl = S.d_lst.as<int>();
+    std::vector<GemmProblem> p1, p2, p3;
+    for (const auto& j : jobs) {
+        const int k = j.k, l = j.l, m = j.m;
+        for (int a = 0; a < nOps; ++a) {
+            const int ck = S.cnt(k, a), cl = S.cnt(l, a);
+            if (ck == 0 || cl == 0) continue;
+            GemmProblem P;
+            std::memset(&P, 0, sizeof(P));
+            P.M = ck; P.N = j.nl; P.K = cl;
+            P.alpha = M.cspec[(size_t)m + (size_t)a * M.nMat]; P.beta = 0.0;
+            const long long rk = S.refBase[(size_t)k * nOps + a], rl = S.refBase[(size_t)l * nOps + a];
+            if (j.part == 0) {
+                // C(i in k, j in l) = cspec(m, a) IMS(ref_j, ref_i, m)
+                P.A = d_IMSold + rl + rk * nbo + (long long)m * nbo * nbo; P.a_si = nbo; P.a_sk = 1;
+            } else {
+                // C'(j in k, i in l)^T: IMS(ref_j(k), ref_i(l), m)
+                P.A = d_IMSold + rk + rl * nbo + (long long)m * nbo * nbo; P.a_si = 1; P.a_sk = nbo;
+            }
+            P.B = it.d_V + S.ce[l] + (long long)j.c0 * S.dim[l];
+            P.b_ki = dl + S.lstOff[(size_t)l * nOps + a]; P.b_sk = 1; P.b_sj = S.dim[l];
+            P.C = T.as<double>() + j.t_off; P.c_ri = dl + S.lstOff[(size_t)k * nOps + a];
+            P.c_si = 1; P.c_sj = S.dim[k];
+            p1.push_back(P);
+        }
+        GemmProblem Q;
+        std::memset(&Q, 0, sizeof(Q));
+        Q.M = j.kk; Q.N = j.nl; Q.K = S.dim[k]; Q.alpha = 1.0; Q.beta = 0.0;
+        Q.A = it.d_V + S.ce[k]; Q.a_si = S.dim[k]; Q.a_sk = 1;
+        Q.B = T.as<double>() + j.t_off; Q.b_sk = 1; Q.b_sj = S.dim[k];
+        Q.C = W.as<double>() + j.s_off; Q.c_si = 1; Q.c_sj = j.kk;
+        p2.push_back(Q);
+        if (j.rdm_off >= 0) {
+            // Y(k1, l) = sum_k2 rho(k2, k1) S(k2, l); rho row-major -> X(k1,k2) = rdm[k1 + kk*k2]
+            GemmProblem Y;
+            std::memset(&Y, 0, sizeof(Y));
+            Y.M = j.kk; Y.N = j.nl; Y.K = j.kk; Y.alpha = 1.0; Y.beta = 0.0;
+            Y.A = it.d_rdm + j.rdm_off; Y.a_si = 1; Y.a_sk = j.kk;
+            Y.B = W.as<double>() + j.s_off; Y.b_sk = 1; Y.b_sj = j.kk;
+            Y.C = W.as<double>() + j.y_off; Y.c_si = 1; Y.c_sj = j.kk;
+            p3.push_back(Y);
+        }
+    }
+    NRG_TRY(launch_ggemm(ctx, p1, 8));
+    NRG_TRY(launch_ggemm(ctx, p2, 10));
+    NRG_TRY(launch_ggemm(ctx, p3, 14));
+    std::vector<SpikeProb> sp;
+    for (const auto& j : jobs) {
+        SpikeProb s;
+        s.s_off = j.s_off; s.y_off = j.y_off;
+        s.ek_off = S.start[j.k];
+        s.el_off = S.start[j.l] + j.c0;
+        s.kk = j.kk; s.nl = j.nl; s.m = j.m; s.toPos = j.toPos; s.lstride = 1;
+        s.sgn = j.sgn; s.cE = j.cE; s.scale = sc; s.invpf = j.invpf;
+        sp.push_back(s);
+    }
+    return run_spikes(ctx, sp, W.as<double>(), it.d_Esec, nbin, M.nMat, d_binPos, d_binNeg, d_tot);
+}
+
+}  // namespace
+
+int spike_cfs_device(nrg_context* ctx, int iteration, const IterView& it, int nb_old,
+                     const double* d_IMSold, const double* d_rdm, double* d_binPos,
+                     double* d_binNeg, double* d_tot) {
+    const Model& M = ctx->model;
+    const Sectors& S = *it.S;
+    const int nVar = S.nVar;
+    (void)d_rdm;
+    std::vector<SpecJob> jobs;
+    std::vector<int> q(nVar);
+    for (int l = 0; l < S.nsub; ++l) {
+        const int nl = S.dim[l] - it.kept[l];
+        if (nl <= 0) continue;
+        for (int part = 0; part < 2; ++part) {
+            const std::vector<int>& ops = part == 0 ? M.pos_op : M.neg_op;
+            for (int m = 0; m < M.nMat; ++m) {
+                for (int v = 0; v < nVar; ++v) q[v] = S.qn[(size_t)l * nVar + v] + ops[(size_t)m + (size_t)v * M.nMat];
+                const int k = S.find(q.data());
+                if (k < 0 || it.kept[k] == 0) continue;   // findFullSubspace (:396, :475)
+                SpecJob j;
+                j.k = k; j.l = l; j.kk = it.kept[k]; j.c0 = it.kept[l]; j.nl = nl; j.m = m;
+                j.part = part;
+                j.sgn = part == 0 ? 1.0 : -1.0;  // (E_k1 - E_l) (:442) | (E_l - E_k1) (:519)
+                j.cE = 1.0;
+                j.invpf = 0.0;
+                j.toPos = part;                  // negative bins (:458) | positive bins (:532)
+                j.rdm_off = it.rdm_off[k];
+                jobs.push_back(j);
+            }
+        }
+    }
+    return run_spec_jobs(ctx, it, jobs, nb_old, d_IMSold, M.scale(iteration), M.numberOfBin(),
+                         d_binPos, d_binNeg, d_tot);
+}
+
+int spike_t0_device(nrg_context* ctx, int iteration, const IterView& it,
+                    const std::vector<int>& gs_sectors, int nb_old, const double* d_IMSold,
+                    double* d_binPos, double* d_binNeg) {
+    const Model& M = ctx->model;
+    const Sectors& S = *it.S;
+    const int nVar = S.nVar;
+    const double pf = (double)gs_sectors.size();
+    std::vector<SpecJob> jobs;
+    std::vector<int> q(nVar);
+    for (int g : gs_sectors) {
+        for (int part = 0; part < 2; ++part) {
+            const std::vector<int>& ops = part == 0 ? M.pos_op : M.neg_op;
+            for (int m = 0; m < M.nMat; ++m) {
+                for (int v = 0; v < nVar; ++v) q[v] = S.qn[(size_t)g * nVar + v] + ops[(size_t)m + (size_t)v * M.nMat];
+                const int e = S.find(q.data());
+                if (e < 0) continue;
+                SpecJob j;
+                j.k = e; j.l = g; j.kk = S.dim[e]; j.c0 = 0; j.nl = 1; j.m = m;
+                j.part = part;
+                j.sgn = part == 0 ? 1.0 : -1.0;   // +E_ex (:154) | -E_ex (:200)
+                j.cE = 0.0;
+                j.invpf = 1.0 / pf;
+                j.toPos = part == 0 ? 1 : 0;
+                j.rdm_off = -1;
+                jobs.push_back(j);
+            }
+        }
+    }
+    DevBuf& tot = ctx->scratch.b[22];
+    NRG_TRY(tot.ensure(sizeof(double) * 2 * std::max(M.nMat, 1)));
+    return run_spec_jobs(ctx, it, jobs, nb_old, d_IMSold, M.scale(iteration), M.numberOfBin(),
+                         d_binPos, d_binNeg, tot.as<double>());
+}
+
+}  // namespace nrg

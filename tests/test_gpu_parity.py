@@ -1,0 +1,177 @@
+"""Parity of the CUDA drop-in routines with the oracle, routine by routine, on identical
+inputs: the oracle plays the reference's Fortran caller (prepareBasis, truncation, stock,
+restore) and at every iteration both the oracle routine and the C-ABI routine receive the
+same module arrays.
+
+Tolerances (written here, checked below):
+* eigenvalues: |dE| <= 1e-12 * max(1, |E|);
+* eigenvectors: projector difference per (near-)degenerate cluster <= 1e-9;
+* basis_output: bit-exact;
+* invariant matrices, density matrices: <= 1e-12 absolute (entries are O(1));
+* spectral bins: <= 1e-8 absolute per bin (spectra are O(1) in total weight);
+* spectral sum rule: |sum - 1| <= 1e-10.
+"""
+import numpy as np
+import pytest
+
+from oracle import nrg_oracle as O
+from nrg_b200 import model
+
+from helpers import eig_rel_err, small_siam, subspace_err, write_case, sector_blocks
+
+pytestmark = pytest.mark.gpu
+
+EIG_TOL = 1e-12
+VEC_TOL = 1e-9
+MAT_TOL = 1e-12
+BIN_TOL = 1e-8
+SUM_TOL = 1e-10
+
+
+def _drive(ctx_factory, inp):
+    """Runs the oracle step by step, calling the C-ABI routines on the same inputs."""
+    d = write_case(inp)
+    st = O.State(d)
+    ctx = ctx_factory(model.read_inputs(d))
+    nVar = st.nVar
+    rec = dict(eig=[], vec=[], bo=[], gs=[], im=[], ims=[])
+    for it in range(st.first, st.nIter + 1):
+        O.prepare_basis(st, it)
+        si, bi = st.subspaceInfo.copy(), st.basis_input.copy()
+        Eold, IMold = st.eigenvalue.copy(), st.im.copy(order="F")
+        E_g, V_g, bo_g, gs_g = ctx.diagonalization(it, si, bi, Eold, IMold)
+        O.diagonalization(st, it)
+        rec["eig"].append(eig_rel_err(E_g, st.eigenvalue))
+        rec["bo"].append(bool(np.array_equal(bo_g, st.basis_output)))
+        rec["gs"].append(abs(gs_g - st.ground_state_energy[it]) / max(1.0, abs(st.ground_state_energy[it])))
+        worst = 0.0
+        for (s, dd, Bo), (_, _, Bg) in zip(sector_blocks(si, st.eigenvector, nVar),
+                                           sector_blocks(si, V_g, nVar)):
+            s0 = int(si[s, nVar + 2]) - 1
+            worst = max(worst, subspace_err(Bg, Bo, st.eigenvalue[s0:s0 + dd]))
+        rec["vec"].append(worst)
+        # postprocess, with the invariant-matrix routines compared on the same inputs
+        st.thermo[it] = O.calc_thermo(st)
+        O.truncate(st, it)
+        if it < st.nIter:
+            ims_old = st.ims.copy(order="F")
+            im_g = ctx.invariant_matrix_dgemm(it, si, bi, st.nb, st.basis_output, st.eigenvector)
+            O.invariant_matrix_dgemm(st, it)
+            rec["im"].append(float(np.max(np.abs(im_g - st.im))) if st.im.size else 0.0)
+            ims_g = ctx.invariant_matrix_for_spectrum_dgemm(it, si, bi, st.nb, st.basis_output,
+                                                           st.eigenvector, ims_old)
+            O.invariant_matrix_for_spectrum_dgemm(st, it)
+            rec["ims"].append(float(np.max(np.abs(ims_g - st.ims))) if st.ims.size else 0.0)
+        st.numberOfBasis_old = st.nb
+        O.store_restore(st, it)
+        if it >= st.startTrancation:
+            O.stock_full(st, it)
+    return st, ctx, rec
+
+
+@pytest.fixture(scope="module")
+def driven(ctx_factory):
+    inp = small_siam(n_keep=48, n_iterations=14)
+    return _drive(ctx_factory, inp)
+
+
+def test_diagonalization_eigenvalues(driven):
+    _, _, rec = driven
+    assert max(rec["eig"]) <= EIG_TOL, rec["eig"]
+
+
+def test_diagonalization_eigenvectors(driven):
+    _, _, rec = driven
+    assert max(rec["vec"]) <= VEC_TOL, rec["vec"]
+
+
+def test_diagonalization_basis_output_and_ground_state(driven):
+    _, _, rec = driven
+    assert all(rec["bo"])
+    assert max(rec["gs"]) <= EIG_TOL
+
+
+def test_invariant_matrices(driven):
+    _, _, rec = driven
+    assert max(rec["im"]) <= MAT_TOL, rec["im"]
+    assert max(rec["ims"]) <= MAT_TOL, rec["ims"]
+
+
+def _full_arrays(st):
+    nVar = st.nVar
+    mp = np.zeros(st.nIter + 2, dtype=np.int32)
+    for k, v in st.mapFull.items():
+        mp[k + 1] = v
+    return mp
+
+
+def test_reduced_density_matrix(driven):
+    st, ctx, _ = driven
+    assert st.flag_truncation
+    O.initialize_reduced_density(st)
+    seed = st.rdm.copy()
+    point0 = st.pointReducedDensity
+    fsi0 = st.FSI.astype(np.int32).copy()
+    mp = _full_arrays(st)
+    rdm_g, fsi_g, point_g, trace_g = ctx.reduced_density_matrix(
+        st.nIter, st.startTrancation, mp, fsi0, st.FBI, st.FBO, st.FV, seed, point0)
+    O.reduced_density_matrix_calculation(st)
+    assert point_g == st.pointReducedDensity
+    assert np.array_equal(fsi_g, st.FSI.astype(np.int32))
+    assert float(np.max(np.abs(rdm_g - st.rdm))) <= MAT_TOL
+    # trace 1 at every backward step (reducedDensityMatrixDGEMM.F90:303-305)
+    assert np.all(np.abs(trace_g - 1.0) <= 1e-12)
+
+
+def test_spikes_per_iteration(driven):
+    st, ctx, _ = driven
+    if not hasattr(st, "rdm") or st.rdm_trace == {}:
+        O.initialize_reduced_density(st)
+        O.reduced_density_matrix_calculation(st)
+    mp = _full_arrays(st)
+    full = dict(fullSubspaceInfo=st.FSI.astype(np.int32), map=mp, rdm=st.rdm)
+    nb2 = st.numberOfBin * st.nMat
+    worst = 0.0
+    for N in range(st.startTrancation, st.nIter + 1):
+        R = O.get_restore(st, N)
+        nb_old = st.restore[N - 1]["numberOfBasis"]
+        st.binPos[:, 1] = 0.0
+        st.binNeg[:, 1] = 0.0
+        gp = np.zeros((nb2, 2), order="F")
+        gn = np.zeros((nb2, 2), order="F")
+        if N == st.nIter:
+            O.spike_zero_temperature(st, N, R)
+            gp, gn, _ = ctx.spike_zero_temperature(N, R, gp, gn, R["ims_prev"], nb_old)
+        else:
+            O.spike_cfs(st, N, R["numberOfBasis_full"], R)
+            gp, gn, tot = ctx.spike_cfs(N, R, gp, gn, R["ims_prev"], nb_old, full)
+            # binned vs raw sums agree (calculateSpectrumDGEMM.F90:559-596)
+            assert np.all(np.abs(tot[:, 2] - tot[:, 0]) < 1e-8)
+            assert np.all(np.abs(tot[:, 3] - tot[:, 1]) < 1e-8)
+        worst = max(worst, float(np.max(np.abs(gp[:, 1] - st.binPos[:, 1]))),
+                    float(np.max(np.abs(gn[:, 1] - st.binNeg[:, 1]))))
+    assert worst <= BIN_TOL, worst
+
+
+def test_device_resident_run_matches_oracle(ctx_factory):
+    inp = small_siam(n_keep=48, n_iterations=14)
+    d = write_case(inp)
+    st = O.run(d)
+    ctx = ctx_factory(model.read_inputs(d))
+    res = ctx.run(spectrum=True)
+    assert res["startTrancation"] == st.startTrancation
+    its = list(range(st.first, st.nIter + 1))
+    assert [int(k) for k in res["kept"]] == [st.kept[i] for i in its]
+    nbin = st.numberOfBin
+    assert res["numberOfBin"] == nbin
+    assert np.max(np.abs(res["binPos"][:, 1] - st.binPos[:, 1])) <= BIN_TOL
+    assert np.max(np.abs(res["binNeg"][:, 1] - st.binNeg[:, 1])) <= BIN_TOL
+    assert np.allclose(res["binPos"][:, 0], st.binPos[:, 0], rtol=1e-15, atol=0)
+    for m in range(st.nMat):
+        tot = res["binPos"][m * nbin:(m + 1) * nbin, 1].sum() + res["binNeg"][m * nbin:(m + 1) * nbin, 1].sum()
+        assert abs(tot - 1.0) <= SUM_TOL
+    for N in range(st.startTrancation, st.nIter):
+        assert abs(res["rdmTrace"][N] - 1.0) <= 1e-12
+    for k, i in enumerate(its):
+        flow = st.flow[i][:8]
+        assert np.max(np.abs(res["flow"][k][:len(flow)] - flow)) <= 1e-11
