@@ -9,7 +9,7 @@ OUT = os.path.join(HERE, "nrg_b200", "libnrgb200.so")
 SOURCES = ["capi.cu", "driver.cu", "routines.cu", "kernels.cu", "ggemm.cu", "eig.cu"]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo", "-O3", "-std=c++17",
-         "--extended-lambda", "-Xcompiler", "-fPIC", "-Xcompiler", "-fvisibility=hidden"]
+         "--extended-lambda", "-Xcompiler", "-fPIC", "-Xcompiler", "-fvisibility=hidden", "-Xcompiler", "-g"]
 
 
 def build(force: bool = False, verbose: bool = False) -> str:

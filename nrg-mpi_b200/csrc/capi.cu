@@ -5,11 +5,52 @@
 
 #include <algorithm>
 #include <cstdarg>
+#include <cstdlib>
 #include <cstring>
+#include <execinfo.h>
+#include <signal.h>
+#include <unistd.h>
 #include <vector>
 
 namespace {
 thread_local char g_err[1024] = "";
+
+// NRG_SEGV_TRACE=1: print the native call stack on a host crash, then hand the signal to
+// the previous handler (diagnostics only)
+struct sigaction g_prev_segv;
+char g_altstack[1 << 16];
+void segv_trace(int sig, siginfo_t* si, void* uc) {
+    static const char msg[] = "\n[nrg] SIGSEGV, native stack:\n";
+    if (write(2, msg, sizeof(msg) - 1) < 0) {}
+    void* buf[64];
+    const int n = backtrace(buf, 64);
+    backtrace_symbols_fd(buf, n, 2);
+    sigaction(SIGSEGV, &g_prev_segv, nullptr);
+    if (g_prev_segv.sa_flags & SA_SIGINFO) {
+        if (g_prev_segv.sa_sigaction) g_prev_segv.sa_sigaction(sig, si, uc);
+    } else if (g_prev_segv.sa_handler != SIG_DFL && g_prev_segv.sa_handler != SIG_IGN) {
+        g_prev_segv.sa_handler(sig);
+    }
+    signal(sig, SIG_DFL);
+    raise(sig);
+}
+__attribute__((constructor)) void install_segv_trace() {
+    const char* e = getenv("NRG_SEGV_TRACE");
+    if (!e || e[0] != '1') return;
+    void* warm[4];
+    backtrace(warm, 4);   // loads the unwinder outside the handler
+    stack_t ss;
+    ss.ss_sp = g_altstack;
+    ss.ss_size = sizeof(g_altstack);
+    ss.ss_flags = 0;
+    sigaltstack(&ss, nullptr);
+    struct sigaction sa;
+    memset(&sa, 0, sizeof(sa));
+    sa.sa_sigaction = segv_trace;
+    sa.sa_flags = SA_SIGINFO | SA_ONSTACK;
+    sigemptyset(&sa.sa_mask);
+    sigaction(SIGSEGV, &sa, &g_prev_segv);
+}
 }
 
 void nrg_set_error_message(const char* fmt, ...) {

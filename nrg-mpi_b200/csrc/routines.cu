@@ -328,6 +328,10 @@ int invmat_spec_device(nrg_context* ctx, const Sectors& S, const std::vector<int
         for (int a = 0; a < nOps; ++a) {
             const int cL = S.cnt(L, a), cR = S.cnt(R, a);
             if (cL == 0 || cR == 0) continue;
+            if (S.refBase[(size_t)L * nOps + a] + cL > nb_old || S.refBase[(size_t)R * nOps + a] + cR > nb_old) {
+                nrg_set_error_message("basis_input references exceed numberOfBasis_old=%d", nb_old);
+                return NRG_ERR_INVALID;
+            }
             GemmProblem P;
             std::memset(&P, 0, sizeof(P));
             P.M = cL; P.N = kept[R]; P.K = cR;
@@ -478,6 +482,10 @@ int run_spec_jobs(nrg_context* ctx, const IterView& it, std::vector<SpecJob>& jo
         for (int a = 0; a < nOps; ++a) {
             const int ck = S.cnt(k, a), cl = S.cnt(l, a);
             if (ck == 0 || cl == 0) continue;
+            if (S.refBase[(size_t)k * nOps + a] + ck > nb_old || S.refBase[(size_t)l * nOps + a] + cl > nb_old) {
+                nrg_set_error_message("basis_input references exceed numberOfBasis_old=%d", nb_old);
+                return NRG_ERR_INVALID;
+            }
             GemmProblem P;
             std::memset(&P, 0, sizeof(P));
             P.M = ck; P.N = j.nl; P.K = cl;

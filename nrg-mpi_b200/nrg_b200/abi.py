@@ -286,13 +286,21 @@ class Context:
         nsub, nb = si.size // rs, bi.size // rs
         dims = si.reshape(nsub, rs)[:, nVar].astype(np.int64)
         size = int(np.sum(dims * dims))
-        eo = np.ascontiguousarray(eigenvalue_old, dtype=np.float64)
-        im = _f64f(invariant_matrix)
+        # numberOfBasis_old is the order of the old invariant matrix; eigenvalue may hold
+        # more entries (the discarded states follow the kept ones, postprocess.F90:143-160)
+        im_arr = np.asarray(invariant_matrix, dtype=np.float64)
+        nbo = int(im_arr.shape[0])
+        if im_arr.shape != (nbo, nbo, self.inp.numberOfConductionMatrix):
+            raise ValueError(f"invariant_matrix must be (nb_old, nb_old, nCM), got {im_arr.shape}")
+        eo = np.ascontiguousarray(np.asarray(eigenvalue_old, dtype=np.float64).reshape(-1)[:nbo])
+        if eo.size != nbo:
+            raise ValueError("eigenvalue_old shorter than numberOfBasis_old")
+        im = _f64f(im_arr)
         E = np.zeros(nb)
         V = np.zeros(size)
         bo = np.zeros(nb * rs, dtype=np.int32)
         gs = c_double(0.0)
-        io = DiagIO(nsub, _p(si, c_int32), nb, _p(bi, c_int32), eo.size, _p(eo, c_double),
+        io = DiagIO(nsub, _p(si, c_int32), nb, _p(bi, c_int32), nbo, _p(eo, c_double),
                     _p(im, c_double), _p(E, c_double), _p(V, c_double), size, _p(bo, c_int32),
                     ctypes.pointer(gs))
         self._check(self.lib.nrg_diagonalization(self._h, iteration, ctypes.byref(io)),
@@ -357,6 +365,8 @@ class Context:
         bo = _i32(R["basis_output"])
         E = np.ascontiguousarray(R["eigenvalue"], dtype=np.float64)
         V = np.ascontiguousarray(R["eigenvector"], dtype=np.float64)
+        if np.asarray(ims_prev).shape != (nb_old, nb_old, self.inp.numberOfMatrix):
+            raise ValueError("invariant_matrix_spectrum must be (nb_old, nb_old, nMat)")
         ims = _f64f(ims_prev)
         tot = np.zeros(4 * self.inp.numberOfMatrix)
         nbin = binPos.shape[0] // self.inp.numberOfMatrix
@@ -423,11 +433,13 @@ class Context:
         flow = np.full(nit * flow_stride, np.nan)
         fin = np.zeros(max(final_capacity, 1))
         ph = np.zeros(4)
-        ro = RunOutput(0, _p(bp, c_double), _p(bn, c_double), bp.size // 2, 0, _p(kept, c_int32),
+        ro = RunOutput(0, _p(bp, c_double), _p(bn, c_double), bp.size, 0, _p(kept, c_int32),
                        _p(nfull, c_int32), _p(gse, c_double), _p(tr, c_double), _p(flow, c_double),
                        flow_stride, _p(fin, c_double), final_capacity, _p(ph, c_double))
         self._check(self.lib.nrg_run(self._h, ctypes.byref(ri), ctypes.byref(ro)), "nrg_run")
         nbin = ro.numberOfBin
+        if spectrum and inp.flag_spectrum and 2 * nbin * nmat > bp.size:
+            raise NrgError(4, "nrg_run", f"bin buffers too small for {nbin} bins")
         nw = nbin * nmat
         binPos = np.stack([bp[:nw], bp[nw:2 * nw]], axis=1)
         binNeg = np.stack([bn[:nw], bn[nw:2 * nw]], axis=1)
