@@ -1,0 +1,318 @@
+"""Benchmark of the NRG hot path on B200.
+
+One step = one full run of the reference's driver (main.F90) on the plain-FP64 SIAM
+workload: Lambda=2, U=0.2, Gamma=0.02, eps_d=-0.1, N_keep=2048, 60 NRG iterations, then
+the backward reduced density matrices and the T=0 CFS spectrum on the reference's
+1000-bins-per-decade grid.  Metric: NRG iterations per second (60 per step), whole job.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+
+* value: device-resident run (nrg_run), inputs resident, timed with CUDA events on the
+  stream the library launches on, barrier + synchronize on both sides, max over ranks.
+* e2e: the same metric through the drop-in entry points with host arrays (every routine
+  copies its module arrays host->device and back, as a Fortran caller would).
+* roofline: the batched FP64 eigensolver (the dominant kernel), algorithmic flops
+  sum_s (4/3+2) d_s^3 per launch over its event-timed duration, against a cuBLAS DGEMM
+  peak measured here.
+* cpu_baseline: the oracle (numpy/scipy port of the reference path, OpenBLAS on all host
+  threads) on a bounded sample of the same sweep.
+* --impl reference: the oracle port timed per NRG iteration of the same sweep (steps are
+  full-size iterations), rank 0 only.
+Multi-GPU: the path does not shard (one GPU per NRG instance), so N ranks run N replicas.
+"""
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+for _p in (ROOT, os.path.join(ROOT, "nrg-mpi_b200")):
+    if _p not in sys.path:
+        sys.path.insert(0, _p)
+
+import numpy as np  # noqa: E402
+
+WORKLOAD = dict(U=0.2, Gamma=0.02, eps_d=-0.1, Lambda=2.0, n_keep=2048, n_iterations=60)
+WORKLOAD_NAME = ("SIAM flat band Lambda=2.0 U=0.2 Gamma=0.02 eps_d=-0.1 N_keep=2048, "
+                 "60 NRG iterations + backward RDM + T=0 CFS spectrum (1000 bins/decade)")
+METRIC = "NRG iterations/s (full sweep + RDM + CFS spectrum, FP64, eig err <= 1e-12)"
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=3)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    p.add_argument("--no-e2e", action="store_true")
+    p.add_argument("--no-cpu", action="store_true")
+    return p.parse_args()
+
+
+def dist_env():
+    return (int(os.environ.get("RANK", "0")), int(os.environ.get("LOCAL_RANK", "0")),
+            int(os.environ.get("WORLD_SIZE", "1")))
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.path = tempfile.mktemp(prefix="clocks_", suffix=".csv")
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.f = open(self.path, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.device}", f"--query-gpu={self.QUERY}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=self.f, stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+            self.f.close()
+
+    def summary(self):
+        if self.proc is None or not os.path.exists(self.path):
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        rows = []
+        for line in open(self.path):
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                rows.append((float(parts[1]), float(parts[2]), float(parts[3]), parts[5:9]))
+            except ValueError:
+                continue
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i, v in enumerate(r[3]) if v.lower() == "active"})
+        loaded = [r[0] for r in rows if r[2] > 200.0] or [r[0] for r in rows]
+        return {"sm_mhz": statistics.median(loaded), "sm_max_mhz": max(r[1] for r in rows),
+                "reasons": reasons, "samples": len(rows)}
+
+
+def fp64_peak_tflops(torch, device):
+    """cuBLAS DGEMM throughput measured here (the FP64 roofline denominator)."""
+    n = 8192
+    a = torch.randn(n, n, dtype=torch.float64, device=device)
+    b = torch.randn(n, n, dtype=torch.float64, device=device)
+    for _ in range(2):
+        torch.matmul(a, b)
+    torch.cuda.synchronize(device)
+    best = float("inf")
+    for _ in range(5):
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s.record()
+        torch.matmul(a, b)
+        e.record()
+        e.synchronize()
+        best = min(best, s.elapsed_time(e) * 1e-3)
+    del a, b
+    return 2.0 * n ** 3 / best / 1e12
+
+
+def cpu_sample(n_timed=3):
+    """Oracle port on full-size iterations of the same sweep (forward path only)."""
+    from nrg_b200 import model
+    from oracle import nrg_oracle as O
+    inp = model.siam(**WORKLOAD)
+    d = tempfile.mkdtemp(prefix="nrg_cpu_")
+    model.write_inputs(inp, d)
+    st = O.State(d)
+    it = st.first
+    while st.numberOfBasis_old < st.truncation and it <= st.nIter:
+        O.nrg_iteration(st, it)    # grow to full size (untimed)
+        it += 1
+    t0 = time.perf_counter()
+    for _ in range(n_timed):
+        O.nrg_iteration(st, it)
+        it += 1
+    dt = time.perf_counter() - t0
+    return n_timed / dt, dt, it - n_timed, it - 1
+
+
+def reference_arm(args):
+    rank, _, world = dist_env()
+    if world > 1:
+        import torch.distributed as dist
+        dist.init_process_group("gloo")
+        if rank != 0:
+            dist.barrier()
+            dist.destroy_process_group()
+            return
+    from nrg_b200 import model
+    from oracle import nrg_oracle as O
+    inp = model.siam(**WORKLOAD)
+    d = tempfile.mkdtemp(prefix="nrg_ref_")
+    model.write_inputs(inp, d)
+    st = O.State(d)
+    it = st.first
+    while st.numberOfBasis_old < st.truncation and it <= st.nIter:
+        O.nrg_iteration(st, it)
+        it += 1
+    for _ in range(args.warmup):
+        O.nrg_iteration(st, it)
+        it += 1
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        O.nrg_iteration(st, it)
+        it += 1
+    dt = time.perf_counter() - t0
+    v = args.steps / dt
+    cores = os.cpu_count()
+    line = {
+        "impl": "reference", "metric": METRIC, "value": v, "unit": "iterations/s",
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": dt / args.steps * 1e3, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": WORKLOAD_NAME, "n_keep": 2048, "iterations": 60,
+                   "parallelism": "replicas", "step": "one full-size NRG iteration (nb ~ 8200)"},
+        "cpu_baseline": {"value": v, "unit": "iterations/s", "cores": cores, "kind": "port",
+                         "sample": f"forward NRG iterations {it - args.steps}..{it - 1} of the sweep "
+                                   "(prepareBasis, dsyev per sector, truncation, invariant matrices)"},
+        "e2e": {"value": v, "unit": "iterations/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        return reference_arm(args)
+    import torch
+    rank, local, world = dist_env()
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=600), device_id=dev)
+    from nrg_b200 import Context, model
+    inp = model.siam(**WORKLOAD)
+    n_it = inp.numberOfIteration - inp.indexOfFirstIteration + 1
+    ctx = Context(local)
+    ctx.set_model(inp)
+    stream = torch.cuda.current_stream(dev)
+    ctx.set_stream(stream.cuda_stream)
+    peak = fp64_peak_tflops(torch, dev) if rank == 0 else None
+    for _ in range(args.warmup):
+        res = ctx.run(spectrum=True)
+    torch.cuda.synchronize(dev)
+    ctx.set_profiling(True)
+    ctx.reset_stats()
+    l0 = ctx.launch_count
+    phases = []
+    with ClockSampler(local) as clk:
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize(dev)
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s.record(stream)
+        for _ in range(args.steps):
+            res = ctx.run(spectrum=True)
+            phases.append(res["phaseSeconds"].copy())
+        e.record(stream)
+        torch.cuda.synchronize(dev)
+        if dist is not None:
+            dist.barrier()
+    elapsed = s.elapsed_time(e) * 1e-3
+    launches = ctx.launch_count - l0
+    stats = ctx.stats()
+    ctx.set_profiling(False)
+    t_max = elapsed
+    if dist is not None:
+        t = torch.tensor([elapsed], device=dev, dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        t_max = float(t.item())
+    value = n_it * args.steps * world / t_max
+    # end to end through the drop-in entry points with host arrays
+    e2e = None
+    if not args.no_e2e:
+        ctx.reset_stats()
+        t0 = time.perf_counter()
+        r2 = ctx.run(spectrum=True, host_drop_in=True)
+        torch.cuda.synchronize(dev)
+        dt = time.perf_counter() - t0
+        st2 = ctx.stats()
+        if dist is not None:
+            t = torch.tensor([dt], device=dev, dtype=torch.float64)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            dt = float(t.item())
+        same = float(max(np.max(np.abs(r2["binPos"][:, 1] - res["binPos"][:, 1])),
+                         np.max(np.abs(r2["binNeg"][:, 1] - res["binNeg"][:, 1]))))
+        e2e = {"value": n_it * world / dt, "unit": "iterations/s",
+               "h2d_bytes_per_step": int(st2["h2d_bytes"]), "d2h_bytes_per_step": int(st2["d2h_bytes"]),
+               "path": "drop-in entry points with host arrays (Fortran caller's data flow)",
+               "max_bin_diff_vs_device_resident": same}
+    if rank == 0:
+        clocks = clk.summary()
+        nbin = res["numberOfBin"]
+        sums = [float(res["binPos"][m * nbin:(m + 1) * nbin, 1].sum() + res["binNeg"][m * nbin:(m + 1) * nbin, 1].sum())
+                for m in range(inp.numberOfMatrix)]
+        ph = np.mean(np.array(phases), axis=0)
+        syev_avg_s = stats["syev_ms"] * 1e-3 / max(stats["syev_launches"], 1)
+        flops_per_launch = stats["syev_flops"] / max(stats["syev_launches"], 1)
+        achieved = flops_per_launch / syev_avg_s / 1e12 if syev_avg_s > 0 else None
+        cpu = None
+        if not args.no_cpu:
+            v, dt, i0, i1 = cpu_sample()
+            cpu = {"value": v, "unit": "iterations/s", "cores": os.cpu_count(), "kind": "port",
+                   "sample": f"forward NRG iterations {i0}..{i1} of the same sweep (nb ~ 8200 each), "
+                             f"{dt:.1f} s, numpy/scipy-OpenBLAS oracle; forward path only"}
+        line = {
+            "metric": METRIC, "value": value, "unit": "iterations/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": t_max / args.steps * 1e3,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (generated Wilson chain and impurity tables)",
+            "config": {"workload": WORKLOAD_NAME, "n_keep": 2048, "iterations": n_it,
+                       "parallelism": f"replicas x{world}",
+                       "l2": "working set > L2: each step writes ~1 GB of eigenvector blocks"},
+            "phase_seconds": {"nrg_sweep": float(ph[0]), "rdm": float(ph[1]), "cfs_spectrum": float(ph[2])},
+            "spectrum_seconds": float(ph[2]),
+            "sum_rule": sums,
+            "gpu_launches": int(launches),
+            "roofline": {"kernel": "k_syev (batched FP64 tridiagonalisation + divide and conquer + back-transform)",
+                         "bound": "tensor", "pipe": "fp64",
+                         "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+                         "frac": (achieved / peak) if (achieved and peak) else None,
+                         "peak_source": "cuBLAS DGEMM 8192^3 measured in this run (MEASURED_PEAKS.json has no FP64 figure)",
+                         "flops_per_launch": flops_per_launch, "avg_launch_ms": syev_avg_s * 1e3,
+                         "launches": int(stats["syev_launches"]), "traffic": None},
+            "clocks": clocks,
+            "e2e": e2e,
+            "cpu_baseline": cpu,
+        }
+        print(json.dumps(line), flush=True)
+    ctx.close()
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

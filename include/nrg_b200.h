@@ -98,6 +98,21 @@ NRG_API int nrg_context_set_stream(nrg_context* ctx, void* stream);
 NRG_API int nrg_context_set_model(nrg_context* ctx, const nrg_model* model);
 /* Number of kernels this library launched on the context since creation. */
 NRG_API int64_t nrg_context_launch_count(const nrg_context* ctx);
+
+/* Counters for measurement (no counterpart in the reference; it times phases with
+ * count.f90).  Eigensolver times are taken with CUDA events around each batched launch
+ * when profiling is on; its algorithmic flops are sum over sectors of (4/3 + 2) d^3. */
+typedef struct nrg_stats {
+    int64_t launches;        /* kernels launched                                      */
+    int64_t syev_launches;   /* batched eigensolver launches                           */
+    double syev_ms;          /* their summed device time (profiling on)               */
+    double syev_flops;       /* algorithmic flops of those launches                   */
+    int64_t h2d_bytes;       /* host-to-device bytes moved by the library             */
+    int64_t d2h_bytes;       /* device-to-host bytes moved by the library             */
+} nrg_stats;
+NRG_API int nrg_context_get_stats(const nrg_context* ctx, nrg_stats* out);
+NRG_API int nrg_context_reset_stats(nrg_context* ctx);
+NRG_API int nrg_context_set_profiling(nrg_context* ctx, int on);
 NRG_API const char* nrg_last_error(void);
 NRG_API const char* nrg_status_string(int status);
 NRG_API int nrg_version(void);

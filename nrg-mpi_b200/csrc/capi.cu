@@ -93,6 +93,7 @@ int stage_in(nrg_context* ctx, const T* p, size_t n, size_t slot, const T** out)
     DevBuf& b = ctx->slot(slot);
     NRG_TRY(b.ensure(sizeof(T) * n));
     NRG_CUDA_TRY(cudaMemcpyAsync(b.p, p, sizeof(T) * n, cudaMemcpyHostToDevice, ctx->stream));
+    ctx->h2d += (long long)(sizeof(T) * n);
     *out = b.as<T>();
     return NRG_OK;
 }
@@ -111,6 +112,7 @@ template <class T>
 int finish_out(nrg_context* ctx, T* p, const T* dev, size_t n) {
     if (p == dev || n == 0) return NRG_OK;
     NRG_CUDA_TRY(cudaMemcpyAsync(p, dev, sizeof(T) * n, cudaMemcpyDeviceToHost, ctx->stream));
+    ctx->d2h += (long long)(sizeof(T) * n);
     return NRG_OK;
 }
 
@@ -208,6 +210,33 @@ int nrg_context_set_stream(nrg_context* ctx, void* stream) {
 }
 
 int64_t nrg_context_launch_count(const nrg_context* ctx) { return ctx ? ctx->launches : 0; }
+
+int nrg_context_get_stats(const nrg_context* ctx, nrg_stats* out) {
+    if (!ctx || !out) return NRG_ERR_INVALID;
+    out->launches = ctx->launches;
+    out->syev_launches = ctx->syev_launches;
+    out->syev_ms = ctx->syev_ms;
+    out->syev_flops = ctx->syev_flops;
+    out->h2d_bytes = ctx->h2d;
+    out->d2h_bytes = ctx->d2h;
+    return NRG_OK;
+}
+
+int nrg_context_reset_stats(nrg_context* ctx) {
+    if (!ctx) return NRG_ERR_INVALID;
+    ctx->syev_launches = 0;
+    ctx->syev_ms = 0.0;
+    ctx->syev_flops = 0.0;
+    ctx->h2d = 0;
+    ctx->d2h = 0;
+    return NRG_OK;
+}
+
+int nrg_context_set_profiling(nrg_context* ctx, int on) {
+    if (!ctx) return NRG_ERR_INVALID;
+    ctx->profiling = on != 0;
+    return NRG_OK;
+}
 
 int nrg_context_set_model(nrg_context* ctx, const nrg_model* m) {
     if (!ctx || !m) return NRG_ERR_INVALID;

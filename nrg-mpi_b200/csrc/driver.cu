@@ -1,9 +1,15 @@
-// Device-resident replay of the reference driver (main.F90:142-252): the forward NRG sweep
+// Replay of the reference driver (main.F90:142-252): the forward NRG sweep
 // (nrgIteration.F90 -> prepareBasis, diagonalization, postprocess), the backward reduced
-// density matrices and the CFS spectrum at T = 0.  Eigenvector blocks, invariant
-// matrices, density matrices and bins stay in device memory; the host keeps the integer
-// bookkeeping (basis records, sector tables, the truncation decision), which needs the
-// eigenvalues of each iteration (one small device-to-host copy per iteration).
+// density matrices and the CFS spectrum at T = 0.
+//
+// Two data flows:
+// * device resident (nrg_run_input.host_drop_in = 0): eigenvector blocks, invariant
+//   matrices, density matrices and bins stay in device memory; the host keeps the
+//   integer bookkeeping (basis records, sector tables, the truncation decision), which
+//   needs the eigenvalues of each iteration (one small device-to-host copy per step);
+// * host drop-in (host_drop_in = 1): every routine goes through its public entry point
+//   with host arrays, exactly as the Fortran caller would call the drop-in: module arrays
+//   live in host memory and cross to the device and back at every call.
 #include "internal.hpp"
 
 #include <algorithm>
@@ -58,6 +64,81 @@ void sort_basis(std::vector<int>& rec, int n, int nVar) {
         }
 }
 
+// prepareBasis (prepareBasis.F90:31-114): product basis, sort, sector table
+void prepare_basis_host(const Model& M, const std::vector<int>& bo, int nb_old, std::vector<int>* rec,
+                        std::vector<int>* si) {
+    const int nVar = M.nVar, rs = nVar + 3, nOps = M.nOps;
+    const int nb = nb_old * nOps;
+    rec->assign((size_t)nb * rs, 0);
+    for (int i = 0; i < nb_old; ++i)
+        for (int j = 0; j < nOps; ++j) {
+            int* r = &(*rec)[((size_t)i * nOps + j) * rs];
+            for (int v = 0; v < nVar; ++v) r[v] = bo[(size_t)i * rs + v] - M.op(j, v);
+            r[nVar] = i + 1;
+            r[nVar + 1] = bo[(size_t)i * rs + nVar];
+            r[nVar + 2] = j + 1;
+        }
+    sort_basis(*rec, nb, nVar);
+    si->clear();
+    int s0 = 0;
+    long long ce = 1;
+    for (int i = 1; i <= nb; ++i) {
+        bool brk = (i == nb);
+        if (!brk)
+            for (int v = 0; v < nVar; ++v)
+                if ((*rec)[(size_t)i * rs + v] != (*rec)[(size_t)s0 * rs + v]) { brk = true; break; }
+        if (brk) {
+            const int d = i - s0;
+            for (int v = 0; v < nVar; ++v) si->push_back((*rec)[(size_t)s0 * rs + v]);
+            si->push_back(d);
+            si->push_back((int)std::min(ce, 0x7fffffffLL));
+            si->push_back(s0 + 1);
+            ce += (long long)d * d;
+            s0 = i;
+        }
+    }
+}
+
+// sortWithIndex + truncation + sortByIndex (postprocess.F90:71-140).  E is indexed by
+// row (sector order); returns the kept count and the new order of the rows.
+int truncate_host(const Model& M, int it, const std::vector<double>& E, std::vector<int>* order,
+                  int* startTrancation, bool* flag_truncation) {
+    const int nb = (int)E.size();
+    order->resize(nb);
+    std::iota(order->begin(), order->end(), 0);
+    std::stable_sort(order->begin(), order->end(), [&](int a, int b) { return E[a] < E[b]; });
+    int nbk = nb;
+    if (it != M.first && it != M.nIter && nb > M.truncation) {
+        if (*startTrancation > it) { *startTrancation = it; *flag_truncation = true; }
+        const int limit = (int)(M.truncation * 1.2);
+        double Ecut = E[(*order)[M.truncation - 1]];
+        int i = M.truncation + 1, cutoff = M.truncation;
+        Ecut = Ecut + 0.000001;
+        while (i <= nb) {
+            if (E[(*order)[i - 1]] <= Ecut) cutoff++; else break;
+            ++i;
+        }
+        while (cutoff > limit) {
+            Ecut = Ecut - 0.001;
+            for (int q = cutoff; q >= 1; --q) {
+                if (E[(*order)[q - 1]] > Ecut) cutoff--; else break;
+            }
+        }
+        nbk = cutoff;
+    }
+    std::sort(order->begin(), order->begin() + nbk);
+    return nbk;
+}
+
+void record_flow(nrg_run_output* out, int idx, const std::vector<double>& E, const std::vector<int>& order, int nbk) {
+    if (!out || !out->flow || out->flowStride <= 0) return;
+    std::vector<double> e(nbk);
+    for (int q = 0; q < nbk; ++q) e[q] = E[order[q]];
+    std::sort(e.begin(), e.end());
+    for (int q = 0; q < out->flowStride; ++q)
+        out->flow[(size_t)idx * out->flowStride + q] = q < nbk ? e[q] : NAN;
+}
+
 struct IterRec {
     int nb_full = 0, nb_kept = 0;
     std::vector<int> kept;
@@ -65,22 +146,33 @@ struct IterRec {
     std::vector<long long> rdm_off;
 };
 
-}  // namespace
+void write_bins(const Model& M, nrg_run_output* out, int nbin, const double* pos_w, const double* neg_w,
+                bool device) {
+    const size_t nw = (size_t)nbin * M.nMat;
+    for (int m = 0; m < M.nMat; ++m)
+        for (int i = 0; i < nbin; ++i) {
+            const double e = std::pow(10.0, -15.0 + double(i) / 1000.0);   // main.F90:152-157
+            out->binnedSpikePositive[(size_t)m * nbin + i] = e;
+            out->binnedSpikeNegative[(size_t)m * nbin + i] = -e;
+        }
+    if (device) {
+        cudaMemcpy(out->binnedSpikePositive + nw, pos_w, sizeof(double) * nw, cudaMemcpyDeviceToHost);
+        cudaMemcpy(out->binnedSpikeNegative + nw, neg_w, sizeof(double) * nw, cudaMemcpyDeviceToHost);
+    } else {
+        std::memcpy(out->binnedSpikePositive + nw, pos_w, sizeof(double) * nw);
+        std::memcpy(out->binnedSpikeNegative + nw, neg_w, sizeof(double) * nw);
+    }
+}
 
-extern "C" int nrg_run(nrg_context* ctx, const nrg_run_input* in, nrg_run_output* out) {
-    if (!ctx || !in) return NRG_ERR_INVALID;
-    if (!ctx->model.set) { nrg_set_error_message("nrg_context_set_model has not been called"); return NRG_ERR_STATE; }
-    NRG_CUDA_TRY(cudaSetDevice(ctx->device));
+// ------------------------------------------------------------------------------------
+// device-resident data flow
+// ------------------------------------------------------------------------------------
+int run_device(nrg_context* ctx, const nrg_run_input* in, nrg_run_output* out, cudaEvent_t* ev) {
     const Model& M = ctx->model;
-    const int nVar = M.nVar, rs = nVar + 3, nOps = M.nOps, first = M.first, nIter = M.nIter;
+    const int nVar = M.nVar, rs = nVar + 3, first = M.first, nIter = M.nIter;
     const int nIt = nIter - first + 1;
     const bool spectrum = in->spectrum && M.nMat > 0;
     cudaStream_t st = ctx->stream;
-
-    cudaEvent_t ev[4];
-    for (auto& e : ev) NRG_CUDA_TRY(cudaEventCreate(&e));
-    NRG_CUDA_TRY(cudaEventRecord(ev[0], st));
-
     // ---- initial state (read_initial_basis) ----
     int nb_old = in->numberOfBasis;
     std::vector<int> bo(in->basis_output, in->basis_output + (size_t)nb_old * rs);
@@ -91,17 +183,20 @@ extern "C" int nrg_run(nrg_context* ctx, const nrg_run_input* in, nrg_run_output
     NRG_CUDA_TRY(cudaMemcpyAsync(bEold0.p, in->eigenvalue, sizeof(double) * nb_old, cudaMemcpyHostToDevice, st));
     NRG_CUDA_TRY(cudaMemcpyAsync(bIM0.p, in->invariant_matrix, sizeof(double) * (size_t)nb_old * nb_old * M.nCM,
                                  cudaMemcpyHostToDevice, st));
+    ctx->h2d += (long long)sizeof(double) * nb_old * (1 + (long long)nb_old * M.nCM);
     const double* dEold = bEold0.as<double>();
     const double* dIMold = bIM0.as<double>();
     const double* dIMSold = nullptr;
     if (spectrum) {
         DevBuf& b = ctx->slot(9);
-        NRG_TRY(b.ensure(sizeof(double) * (size_t)nb_old * nb_old * M.nMat));
-        NRG_CUDA_TRY(cudaMemcpyAsync(b.p, in->invariant_matrix_spectrum, sizeof(double) * (size_t)nb_old * nb_old * M.nMat,
-                                     cudaMemcpyHostToDevice, st));
+        const size_t n = (size_t)nb_old * nb_old * M.nMat;
+        NRG_TRY(b.ensure(sizeof(double) * n));
+        NRG_CUDA_TRY(cudaMemcpyAsync(b.p, in->invariant_matrix_spectrum, sizeof(double) * n, cudaMemcpyHostToDevice, st));
+        ctx->h2d += (long long)(sizeof(double) * n);
         dIMSold = b.as<double>();
     }
     if ((int)ctx->iter_sectors.size() < nIt) ctx->iter_sectors.resize(nIt);
+    ctx->slot(22 + 3 * (size_t)nIt);   // size the store once: references below stay valid
     std::vector<IterRec> recs(nIt);
     int startTrancation = nIter + 1;
     bool flag_truncation = false;
@@ -113,43 +208,14 @@ extern "C" int nrg_run(nrg_context* ctx, const nrg_run_input* in, nrg_run_output
     for (int it = first; it <= nIter; ++it) {
         const int idx = it - first;
         IterRec& R = recs[idx];
-        // prepareBasis (prepareBasis.F90:31-114)
-        const int nb = nb_old * nOps;
-        std::vector<int> rec((size_t)nb * rs);
-        for (int i = 0; i < nb_old; ++i)
-            for (int j = 0; j < nOps; ++j) {
-                int* r = &rec[((size_t)i * nOps + j) * rs];
-                for (int v = 0; v < nVar; ++v) r[v] = bo[(size_t)i * rs + v] - M.op(j, v);
-                r[nVar] = i + 1;
-                r[nVar + 1] = bo[(size_t)i * rs + nVar];
-                r[nVar + 2] = j + 1;
-            }
-        sort_basis(rec, nb, nVar);
-        std::vector<int> si;
-        {
-            int s0 = 0;
-            long long ce = 1;
-            for (int i = 1; i <= nb; ++i) {
-                bool brk = (i == nb);
-                if (!brk)
-                    for (int v = 0; v < nVar; ++v)
-                        if (rec[(size_t)i * rs + v] != rec[(size_t)s0 * rs + v]) { brk = true; break; }
-                if (brk) {
-                    const int d = i - s0;
-                    for (int v = 0; v < nVar; ++v) si.push_back(rec[(size_t)s0 * rs + v]);
-                    si.push_back(d);
-                    si.push_back((int)std::min(ce, 0x7fffffffLL));
-                    si.push_back(s0 + 1);
-                    ce += (long long)d * d;
-                    s0 = i;
-                }
-            }
-        }
+        std::vector<int> rec, si;
+        prepare_basis_host(M, bo, nb_old, &rec, &si);
+        const int nb = nb_old * M.nOps;
         const int nsub = (int)(si.size() / rs);
         Sectors& S = ctx->iter_sectors[idx];
-        NRG_TRY(S.build(nsub, si.data(), nb, rec.data(), nVar, nOps));
+        NRG_TRY(S.build(nsub, si.data(), nb, rec.data(), nVar, M.nOps));
         NRG_TRY(S.upload(st));
-        // diagonalization
+        ctx->h2d += (long long)sizeof(int) * ((long long)nb * rs + (long long)S.lst.size() + (long long)S.lstOff.size());
         DevBuf& bV = slotV(idx);
         DevBuf& bE = slotE(idx);
         NRG_TRY(bV.ensure(sizeof(double) * (size_t)S.sizeV));
@@ -160,38 +226,10 @@ extern "C" int nrg_run(nrg_context* ctx, const nrg_run_input* in, nrg_run_output
         R.Esec.resize(nb);
         NRG_CUDA_TRY(cudaMemcpyAsync(R.Esec.data(), bE.p, sizeof(double) * nb, cudaMemcpyDeviceToHost, st));
         NRG_CUDA_TRY(cudaStreamSynchronize(st));
-        // postprocess: truncation (postprocess.F90:71-160)
-        std::vector<int> order(nb);
-        std::iota(order.begin(), order.end(), 0);
-        std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return R.Esec[a] < R.Esec[b]; });
-        int nbk = nb;
-        if (it != first && it != nIter && nb > M.truncation) {
-            if (startTrancation > it) { startTrancation = it; flag_truncation = true; }
-            const int limit = (int)(M.truncation * 1.2);
-            double Ecut = R.Esec[order[M.truncation - 1]];
-            int i = M.truncation + 1, cutoff = M.truncation;
-            Ecut = Ecut + 0.000001;
-            while (i <= nb) {
-                if (R.Esec[order[i - 1]] <= Ecut) cutoff++; else break;
-                ++i;
-            }
-            while (cutoff > limit) {
-                Ecut = Ecut - 0.001;
-                for (int q = cutoff; q >= 1; --q) {
-                    if (R.Esec[order[q - 1]] > Ecut) cutoff--; else break;
-                }
-            }
-            nbk = cutoff;
-        }
-        std::sort(order.begin(), order.begin() + nbk);   // sortByIndex (:140)
-        if (out && out->flow && out->flowStride > 0) {
-            std::vector<double> e(nbk);
-            for (int q = 0; q < nbk; ++q) e[q] = R.Esec[order[q]];
-            std::sort(e.begin(), e.end());
-            for (int q = 0; q < out->flowStride; ++q)
-                out->flow[(size_t)idx * out->flowStride + q] = q < nbk ? e[q] : NAN;
-        }
-        // basis_output after truncation (:143-160)
+        ctx->d2h += (long long)sizeof(double) * nb;
+        std::vector<int> order;
+        const int nbk = truncate_host(M, it, R.Esec, &order, &startTrancation, &flag_truncation);
+        record_flow(out, idx, R.Esec, order, nbk);
         std::vector<int> rowSec(nb);
         for (int s = 0; s < nsub; ++s)
             for (int j = 0; j < S.dim[s]; ++j) rowSec[S.start[s] + j] = s;
@@ -209,10 +247,9 @@ extern "C" int nrg_run(nrg_context* ctx, const nrg_run_input* in, nrg_run_output
         R.nb_kept = nbk;
         if (out && out->kept) out->kept[idx] = nbk;
         if (out && out->numberOfBasisFull) out->numberOfBasisFull[idx] = nb;
-        // invariant matrices for the next iteration (postprocess.F90:189-204)
         const double* dIMnew = dIMold;
         const double* dIMSnew = dIMSold;
-        if (it < nIter) {
+        if (it < nIter) {   // postprocess.F90:189-204
             DevBuf& bIM = ctx->slot(1 + ((idx + 1) & 1));
             NRG_TRY(bIM.ensure(sizeof(double) * (size_t)nbk * nbk * M.nCM));
             NRG_TRY(invmat_device(ctx, S, R.kept, bV.as<double>(), bIM.as<double>()));
@@ -228,6 +265,7 @@ extern "C" int nrg_run(nrg_context* ctx, const nrg_run_input* in, nrg_run_output
         NRG_TRY(bEo.ensure(sizeof(double) * nbk));
         NRG_CUDA_TRY(cudaMemcpyAsync(bEo.p, Eold_next.data(), sizeof(double) * nbk, cudaMemcpyHostToDevice, st));
         NRG_CUDA_TRY(cudaStreamSynchronize(st));
+        ctx->h2d += (long long)sizeof(double) * nbk;
         dEold = bEo.as<double>();
         dIMold = dIMnew;
         dIMSold = dIMSnew;
@@ -257,7 +295,6 @@ extern "C" int nrg_run(nrg_context* ctx, const nrg_run_input* in, nrg_run_output
         }
         NRG_TRY(bRdm.ensure(sizeof(double) * (size_t)std::max(off, 1LL)));
         NRG_TRY(run_fill(ctx, bRdm.as<double>(), off, 0.0));
-        // T = 0 seed: projector on the ground states at the last iteration
         IterRec& RL = recs[last];
         const Sectors& SL = ctx->iter_sectors[last];
         int deg = 0;
@@ -265,9 +302,11 @@ extern "C" int nrg_run(nrg_context* ctx, const nrg_run_input* in, nrg_run_output
         const double inv = 1.0 / (double)deg;
         for (int s = 0; s < SL.nsub; ++s)
             for (int p = 0; p < RL.kept[s]; ++p)
-                if (RL.Esec[SL.start[s] + p] < 1.0e-8)
+                if (RL.Esec[SL.start[s] + p] < 1.0e-8) {
                     NRG_CUDA_TRY(cudaMemcpyAsync(bRdm.as<double>() + RL.rdm_off[s] + (long long)p * RL.kept[s] + p, &inv,
                                                  sizeof(double), cudaMemcpyHostToDevice, st));
+                    ctx->h2d += sizeof(double);
+                }
         NRG_CUDA_TRY(cudaStreamSynchronize(st));
         DevBuf& bTr = ctx->slot(7);
         NRG_TRY(bTr.ensure(sizeof(double) * (size_t)(nIter + 2)));
@@ -284,6 +323,7 @@ extern "C" int nrg_run(nrg_context* ctx, const nrg_run_input* in, nrg_run_output
             std::vector<double> tr(nIter + 1, NAN);
             NRG_CUDA_TRY(cudaMemcpyAsync(tr.data(), bTr.p, sizeof(double) * (nIter + 1), cudaMemcpyDeviceToHost, st));
             NRG_CUDA_TRY(cudaStreamSynchronize(st));
+            ctx->d2h += (long long)sizeof(double) * (nIter + 1);
             for (int N = 0; N <= nIter; ++N) out->rdmTrace[N] = (N >= startTrancation && N < nIter) ? tr[N] : NAN;
         }
     }
@@ -322,35 +362,228 @@ extern "C" int nrg_run(nrg_context* ctx, const nrg_run_input* in, nrg_run_output
     NRG_CUDA_TRY(cudaEventRecord(ev[3], st));
     NRG_CUDA_TRY(cudaStreamSynchronize(st));
     NRG_TRY(check_device_status(ctx));
-
     if (out) {
         out->numberOfBin = nbin;
         out->startTrancation = startTrancation;
-        if (out->binnedSpikePositive && out->binnedSpikeNegative && out->binCapacity >= (int64_t)(2 * nw) && spectrum) {
-            for (int m = 0; m < M.nMat; ++m)
-                for (int i = 0; i < nbin; ++i) {
-                    const double e = std::pow(10.0, -15.0 + double(i) / 1000.0);
-                    out->binnedSpikePositive[(size_t)m * nbin + i] = e;
-                    out->binnedSpikeNegative[(size_t)m * nbin + i] = -e;
-                }
-            NRG_CUDA_TRY(cudaMemcpy(out->binnedSpikePositive + nw, dPos, sizeof(double) * nw, cudaMemcpyDeviceToHost));
-            NRG_CUDA_TRY(cudaMemcpy(out->binnedSpikeNegative + nw, dNeg, sizeof(double) * nw, cudaMemcpyDeviceToHost));
+        if (spectrum && out->binnedSpikePositive && out->binnedSpikeNegative && out->binCapacity >= (int64_t)(2 * nw)) {
+            write_bins(M, out, nbin, dPos, dNeg, true);
+            ctx->d2h += (long long)(2 * nw * sizeof(double));
         }
         if (out->finalEigenvalue) {
             const IterRec& RL = recs[last];
             for (int i = 0; i < out->finalCapacity && i < RL.nb_full; ++i) out->finalEigenvalue[i] = RL.Esec[i];
         }
-        if (out->phaseSeconds) {
-            float a = 0, b = 0, c = 0;
-            cudaEventElapsedTime(&a, ev[0], ev[1]);
-            cudaEventElapsedTime(&b, ev[1], ev[2]);
-            cudaEventElapsedTime(&c, ev[2], ev[3]);
-            out->phaseSeconds[0] = a * 1e-3;
-            out->phaseSeconds[1] = b * 1e-3;
-            out->phaseSeconds[2] = c * 1e-3;
-            out->phaseSeconds[3] = (a + b + c) * 1e-3;
+    }
+    return NRG_OK;
+}
+
+// ------------------------------------------------------------------------------------
+// host drop-in data flow: the Fortran caller's view
+// ------------------------------------------------------------------------------------
+struct HostRestore {
+    std::vector<double> E, V, ims;
+    std::vector<int> bo, bi, si;
+    int nb = 0, nb_full = 0, nsub = 0;
+};
+
+int run_drop_in(nrg_context* ctx, const nrg_run_input* in, nrg_run_output* out, cudaEvent_t* ev) {
+    const Model& M = ctx->model;
+    const int nVar = M.nVar, rs = nVar + 3, rsf = nVar + 6, first = M.first, nIter = M.nIter;
+    const int nIt = nIter - first + 1;
+    const bool spectrum = in->spectrum && M.nMat > 0;
+    int nb_old = in->numberOfBasis;
+    std::vector<int> bo(in->basis_output, in->basis_output + (size_t)nb_old * rs);
+    std::vector<double> E(in->eigenvalue, in->eigenvalue + nb_old);
+    std::vector<double> IM(in->invariant_matrix, in->invariant_matrix + (size_t)nb_old * nb_old * M.nCM);
+    std::vector<double> IMS;
+    if (spectrum) IMS.assign(in->invariant_matrix_spectrum, in->invariant_matrix_spectrum + (size_t)nb_old * nb_old * M.nMat);
+    std::vector<HostRestore> rest(nIt);
+    int startTrancation = nIter + 1;
+    bool flag_truncation = false;
+    // the "full" stock (postprocess.F90:221-374)
+    std::vector<int> fsi, fbi, fbo, map(nIter + 2, 0);
+    std::vector<double> fE, fV;
+    long long pointFBI = 1, pointFBO = 1, pointFS = 1, pointFV = 1, sizeRDM = 0;
+    for (int it = first; it <= nIter; ++it) {
+        const int idx = it - first;
+        std::vector<int> bi, si;
+        prepare_basis_host(M, bo, nb_old, &bi, &si);
+        const int nb = nb_old * M.nOps;
+        const int nsub = (int)(si.size() / rs);
+        long long sizeV = 0;
+        for (int s = 0; s < nsub; ++s) sizeV += (long long)si[(size_t)s * rs + nVar] * si[(size_t)s * rs + nVar];
+        std::vector<double> Enew(nb), Vnew((size_t)sizeV);
+        std::vector<int> bo_sec((size_t)nb * rs);
+        double gse = 0.0;
+        nrg_diagonalization_io dio;
+        dio.numberOfSubspace = nsub; dio.subspaceInfo = si.data(); dio.numberOfBasis = nb;
+        dio.basis_input = bi.data(); dio.numberOfBasis_old = nb_old; dio.eigenvalue_old = E.data();
+        dio.invariant_matrix = IM.data(); dio.eigenvalue = Enew.data(); dio.eigenvector = Vnew.data();
+        dio.sizeOfEigenvector = sizeV; dio.basis_output = bo_sec.data(); dio.groundStateEnergy = &gse;
+        NRG_TRY(nrg_diagonalization(ctx, it, &dio));
+        if (out && out->groundStateEnergy) out->groundStateEnergy[idx] = gse;
+        std::vector<int> order;
+        const int nbk = truncate_host(M, it, Enew, &order, &startTrancation, &flag_truncation);
+        record_flow(out, idx, Enew, order, nbk);
+        std::vector<int> bo_re((size_t)nb * rs);
+        std::vector<double> E_re(nb);
+        for (int q = 0; q < nb; ++q) {
+            std::memcpy(&bo_re[(size_t)q * rs], &bo_sec[(size_t)order[q] * rs], sizeof(int) * rs);
+            E_re[q] = Enew[order[q]];
+        }
+        if (out && out->kept) out->kept[idx] = nbk;
+        if (out && out->numberOfBasisFull) out->numberOfBasisFull[idx] = nb;
+        std::vector<double> IMn, IMSn;
+        if (it < nIter) {
+            IMn.assign((size_t)nbk * nbk * M.nCM, 0.0);
+            nrg_invariant_matrix_io iio;
+            iio.numberOfSubspace = nsub; iio.subspaceInfo = si.data(); iio.numberOfBasisFull = nb;
+            iio.basis_input = bi.data(); iio.numberOfBasis = nbk; iio.basis_output = bo_re.data();
+            iio.eigenvector = Vnew.data(); iio.sizeOfEigenvector = sizeV; iio.numberOfBasis_old = nb_old;
+            iio.invariant_matrix_spectrum_old = nullptr; iio.invariant_matrix = IMn.data();
+            NRG_TRY(nrg_invariant_matrix_dgemm(ctx, it, &iio));
+            if (spectrum) {
+                IMSn.assign((size_t)nbk * nbk * M.nMat, 0.0);
+                iio.invariant_matrix_spectrum_old = IMS.data();
+                iio.invariant_matrix = IMSn.data();
+                NRG_TRY(nrg_invariant_matrix_for_spectrum_dgemm(ctx, it, &iio));
+            }
+        }
+        if (spectrum) {
+            HostRestore& R = rest[idx];
+            R.E = E_re; R.V = Vnew; R.bo = bo_re; R.bi = bi; R.si = si; R.nb = nbk; R.nb_full = nb; R.nsub = nsub;
+            if (it < nIter) R.ims = IMSn;
+            if (it >= startTrancation) {
+                map[it + 1] = (int)pointFS;
+                fbo.insert(fbo.end(), bo_re.begin(), bo_re.begin() + (size_t)nbk * rs);
+                fE.insert(fE.end(), E_re.begin(), E_re.begin() + nbk);
+                fbi.insert(fbi.end(), bi.begin(), bi.end());
+                for (int s = 0; s < nsub; ++s) {
+                    int k = 0, first_out = -1;
+                    for (int j = 0; j < nbk; ++j) {
+                        bool eq = true;
+                        for (int v = 0; v < nVar; ++v)
+                            if (si[(size_t)s * rs + v] != bo_re[(size_t)j * rs + v]) { eq = false; break; }
+                        if (eq) { if (first_out < 0) first_out = j; ++k; }
+                    }
+                    if (k == 0) continue;
+                    const int d = si[(size_t)s * rs + nVar];
+                    for (int v = 0; v < nVar; ++v) fsi.push_back(si[(size_t)s * rs + v]);
+                    fsi.push_back(d);
+                    fsi.push_back(k);
+                    fsi.push_back((int)pointFV);
+                    fsi.push_back((int)(pointFBI + si[(size_t)s * rs + nVar + 2] - 1));
+                    fsi.push_back((int)(pointFBO + first_out));
+                    fsi.push_back(0);
+                    sizeRDM += (long long)k * k;
+                    const long long c0 = (long long)si[(size_t)s * rs + nVar + 1] - 1;
+                    fV.insert(fV.end(), Vnew.begin() + c0, Vnew.begin() + c0 + (long long)d * k);
+                    pointFV += (long long)d * k;
+                    ++pointFS;
+                }
+                pointFBI += nb;
+                pointFBO += nbk;
+            }
+        }
+        E.swap(E_re);
+        bo.swap(bo_re);
+        IM.swap(IMn);
+        IMS.swap(IMSn);
+        nb_old = nbk;
+    }
+    NRG_CUDA_TRY(cudaEventRecord(ev[1], ctx->stream));
+    const int nbin = M.numberOfBin();
+    const size_t nw = (size_t)nbin * std::max(M.nMat, 1);
+    std::vector<double> binPos(2 * nw, 0.0), binNeg(2 * nw, 0.0);
+    std::vector<double> rdm;
+    const int elementNum = (int)(pointFS - 1);
+    if (spectrum && flag_truncation) {
+        // initializeReducedDensity.F90:32-78
+        int deg = 0;
+        for (int i = 0; i < nb_old; ++i) deg += E[i] < 1.0e-8;
+        const double pf = (double)deg;
+        rdm.assign((size_t)sizeRDM, 0.0);
+        const int r0 = map[nIter + 1] - 1;
+        int point = 1;
+        for (int j = r0; j < elementNum; ++j) {
+            int* f = &fsi[(size_t)j * rsf];
+            f[nVar + 5] = point;
+            const int k = f[nVar + 1];
+            for (int a = 0; a < k; ++a)
+                if (fE[(size_t)f[nVar + 4] - 1 + a] < 1.0e-8) rdm[(size_t)point - 1 + (size_t)a * k + a] = 1.0 / pf;
+            point += k * k;
+        }
+        nrg_reduced_density_io rio;
+        rio.numberOfIteration = nIter; rio.startTrancation = startTrancation; rio.mapFullSubspaceInfo = map.data();
+        rio.elementNumFullSubspace = elementNum; rio.fullSubspaceInfo = fsi.data();
+        rio.fullBasisInput = fbi.data(); rio.numFullBasisInput = (int64_t)(fbi.size() / rs);
+        rio.fullBasisOutput = fbo.data(); rio.numFullBasisOutput = (int64_t)(fbo.size() / rs);
+        rio.fullEigenvector = fV.data(); rio.numFullEigenvector = (int64_t)fV.size();
+        rio.reducedDensityMatrix = rdm.data(); rio.sizeOfReducedDensity = (int64_t)rdm.size();
+        rio.pointReducedDensity = &point;
+        std::vector<double> tr(std::max(nIter - startTrancation, 1));
+        rio.trace = tr.data();
+        NRG_TRY(nrg_reduced_density_matrix(ctx, &rio));
+        if (out && out->rdmTrace)
+            for (int N = 0; N <= nIter; ++N)
+                out->rdmTrace[N] = (N >= startTrancation && N < nIter) ? tr[nIter - 1 - N] : NAN;
+    }
+    NRG_CUDA_TRY(cudaEventRecord(ev[2], ctx->stream));
+    if (spectrum) {
+        std::vector<double> tot(4 * M.nMat);
+        for (int N = startTrancation; N <= nIter; ++N) {
+            const HostRestore& R = rest[N - first];
+            const HostRestore& P = rest[N - 1 - first];
+            nrg_spike_io sio;
+            std::memset(&sio, 0, sizeof(sio));
+            sio.numberOfSubspace = R.nsub; sio.subspaceInfo = R.si.data(); sio.numberOfBasis = R.nb;
+            sio.numberOfBasisFull = R.nb_full; sio.basis_input = R.bi.data(); sio.basis_output = R.bo.data();
+            sio.eigenvalue = R.E.data(); sio.eigenvector = R.V.data(); sio.sizeOfEigenvector = (int64_t)R.V.size();
+            sio.numberOfBasis_old = P.nb; sio.invariant_matrix_spectrum = P.ims.data();
+            sio.fullSubspaceInfo = fsi.data(); sio.mapFullSubspaceInfo = map.data();
+            sio.elementNumFullSubspace = elementNum; sio.reducedDensityMatrix = rdm.data();
+            sio.sizeOfReducedDensity = (int64_t)rdm.size(); sio.numberOfBin = nbin;
+            sio.binnedSpikePositive = binPos.data(); sio.binnedSpikeNegative = binNeg.data();
+            sio.total_sum = tot.data();
+            if (N == nIter) NRG_TRY(nrg_spike_zero_temperature(ctx, N, &sio));
+            else NRG_TRY(nrg_spike_cfs(ctx, N, &sio));
         }
     }
-    for (auto& e : ev) cudaEventDestroy(e);
+    NRG_CUDA_TRY(cudaEventRecord(ev[3], ctx->stream));
+    NRG_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+    if (out) {
+        out->numberOfBin = nbin;
+        out->startTrancation = startTrancation;
+        if (spectrum && out->binnedSpikePositive && out->binnedSpikeNegative && out->binCapacity >= (int64_t)(2 * nw))
+            write_bins(M, out, nbin, binPos.data() + nw, binNeg.data() + nw, false);
+        if (out->finalEigenvalue) {
+            // the last iteration keeps every state in sector order (no truncation)
+            for (int i = 0; i < out->finalCapacity && i < (int)E.size(); ++i) out->finalEigenvalue[i] = E[i];
+        }
+    }
     return NRG_OK;
+}
+
+}  // namespace
+
+extern "C" int nrg_run(nrg_context* ctx, const nrg_run_input* in, nrg_run_output* out) {
+    if (!ctx || !in) return NRG_ERR_INVALID;
+    if (!ctx->model.set) { nrg_set_error_message("nrg_context_set_model has not been called"); return NRG_ERR_STATE; }
+    NRG_CUDA_TRY(cudaSetDevice(ctx->device));
+    cudaEvent_t ev[4];
+    for (auto& e : ev) NRG_CUDA_TRY(cudaEventCreate(&e));
+    NRG_CUDA_TRY(cudaEventRecord(ev[0], ctx->stream));
+    const int rc = in->host_drop_in ? run_drop_in(ctx, in, out, ev) : run_device(ctx, in, out, ev);
+    if (rc == NRG_OK && out && out->phaseSeconds) {
+        float a = 0, b = 0, c = 0;
+        cudaEventElapsedTime(&a, ev[0], ev[1]);
+        cudaEventElapsedTime(&b, ev[1], ev[2]);
+        cudaEventElapsedTime(&c, ev[2], ev[3]);
+        out->phaseSeconds[0] = a * 1e-3;
+        out->phaseSeconds[1] = b * 1e-3;
+        out->phaseSeconds[2] = c * 1e-3;
+        out->phaseSeconds[3] = (a + b + c) * 1e-3;
+    }
+    for (auto& e : ev) cudaEventDestroy(e);
+    return rc;
 }

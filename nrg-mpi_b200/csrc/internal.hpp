@@ -90,6 +90,11 @@ struct nrg_context {
     nrg::Scratch scratch;
     nrg::DevBuf d_status;
     long long launches = 0;
+    // measurement counters (nrg_context_get_stats)
+    bool profiling = false;
+    long long syev_launches = 0;
+    double syev_ms = 0.0, syev_flops = 0.0;
+    long long h2d = 0, d2h = 0;
     // driver-owned persistent storage, reused across runs
     std::deque<nrg::DevBuf> store;
     std::vector<nrg::Sectors> iter_sectors;

@@ -210,14 +210,35 @@ int diag_device(nrg_context* ctx, int iteration, Sectors& S, const double* d_Eol
     NRG_CUDA_TRY(cudaMemcpyAsync(bsec.p, secs.data(), sizeof(SyevSector) * nsec, cudaMemcpyHostToDevice, ctx->stream));
     NRG_CUDA_TRY(cudaMemcpyAsync(bcol.p, colPrefix.data(), sizeof(long long) * nsec, cudaMemcpyHostToDevice, ctx->stream));
     NRG_CUDA_TRY(cudaMemcpyAsync(bstart.p, secStart.data(), sizeof(int) * nsec, cudaMemcpyHostToDevice, ctx->stream));
+    ctx->h2d += (long long)nsec * (sizeof(SyevSector) + sizeof(long long) + sizeof(int));
     NRG_TRY(run_assemble(ctx, iteration, S, bsec.as<SyevSector>(), bcol.as<long long>(), bstart.as<int>(),
                          nsec, cols, d_Eold, nb_old, d_IMold, d_V));
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    if (ctx->profiling) {
+        NRG_CUDA_TRY(cudaEventCreate(&e0));
+        NRG_CUDA_TRY(cudaEventCreate(&e1));
+        NRG_CUDA_TRY(cudaEventRecord(e0, ctx->stream));
+    }
     NRG_TRY(launch_syev(bsec.as<SyevSector>(), nsec, max_n, d_V, d_E, bwd.as<double>(), bwi.as<int>(),
                         ctx->d_status.as<int>(), ctx->stream));
     ctx->launches++;
+    if (ctx->profiling) {
+        NRG_CUDA_TRY(cudaEventRecord(e1, ctx->stream));
+        NRG_CUDA_TRY(cudaEventSynchronize(e1));
+        float ms = 0.f;
+        NRG_CUDA_TRY(cudaEventElapsedTime(&ms, e0, e1));
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        ctx->syev_ms += ms;
+        ctx->syev_launches++;
+        double f = 0.0;
+        for (int s = 0; s < nsec; ++s) f += (4.0 / 3.0 + 2.0) * double(S.dim[s]) * S.dim[s] * S.dim[s];
+        ctx->syev_flops += f;
+    }
     NRG_TRY(run_eig_finalize(ctx, d_E, S.nb, S.sizeV, d_V, bmin.as<double>()));
     double mg[2];
     NRG_CUDA_TRY(cudaMemcpyAsync(mg, bmin.p, sizeof(double) * 2, cudaMemcpyDeviceToHost, ctx->stream));
+    ctx->d2h += sizeof(mg);
     NRG_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
     if (out) out->groundStateEnergy = mg[1];
     return check_device_status(ctx);

@@ -42,7 +42,8 @@ EXPORTS = [
     "nrg_context_set_model", "nrg_context_launch_count", "nrg_last_error", "nrg_status_string",
     "nrg_version", "nrg_diagonalization", "nrg_invariant_matrix_dgemm",
     "nrg_invariant_matrix_for_spectrum_dgemm", "nrg_reduced_density_matrix",
-    "nrg_spike_zero_temperature", "nrg_spike_cfs", "nrg_run",
+    "nrg_spike_zero_temperature", "nrg_spike_cfs", "nrg_run", "nrg_context_get_stats",
+    "nrg_context_reset_stats", "nrg_context_set_profiling",
 ]
 
 
@@ -136,6 +137,11 @@ class RunOutput(ctypes.Structure):
     ]
 
 
+class Stats(ctypes.Structure):
+    _fields_ = [("launches", c_int64), ("syev_launches", c_int64), ("syev_ms", c_double),
+                ("syev_flops", c_double), ("h2d_bytes", c_int64), ("d2h_bytes", c_int64)]
+
+
 _lib = None
 
 
@@ -163,6 +169,9 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
     lib.nrg_spike_zero_temperature.argtypes = [c_void_p, c_int32, POINTER(SpikeIO)]
     lib.nrg_spike_cfs.argtypes = [c_void_p, c_int32, POINTER(SpikeIO)]
     lib.nrg_run.argtypes = [c_void_p, POINTER(RunInput), POINTER(RunOutput)]
+    lib.nrg_context_get_stats.argtypes = [c_void_p, POINTER(Stats)]
+    lib.nrg_context_reset_stats.argtypes = [c_void_p]
+    lib.nrg_context_set_profiling.argtypes = [c_void_p, ctypes.c_int]
     _lib = lib
     return lib
 
@@ -221,6 +230,17 @@ class Context:
 
     def set_stream(self, stream_handle: int):
         self._check(self.lib.nrg_context_set_stream(self._h, c_void_p(stream_handle)), "set_stream")
+
+    def set_profiling(self, on: bool = True):
+        self._check(self.lib.nrg_context_set_profiling(self._h, int(bool(on))), "set_profiling")
+
+    def reset_stats(self):
+        self._check(self.lib.nrg_context_reset_stats(self._h), "reset_stats")
+
+    def stats(self) -> dict:
+        s = Stats()
+        self._check(self.lib.nrg_context_get_stats(self._h, ctypes.byref(s)), "get_stats")
+        return {k: getattr(s, k) for k, _ in Stats._fields_}
 
     # ------------------------------------------------------------------
     def set_model(self, inp):
@@ -410,8 +430,13 @@ class Context:
                            nb_old, full=full)
 
     # ------------------------------------------------------------------
-    def run(self, spectrum: bool = True, flow_stride: int = 8, final_capacity: int = 0):
-        """main.F90:142-252 on the device; returns bins and per-iteration statistics."""
+    def run(self, spectrum: bool = True, flow_stride: int = 8, final_capacity: int = 0,
+            host_drop_in: bool = False):
+        """main.F90:142-252; returns bins and per-iteration statistics.
+
+        ``host_drop_in=True`` drives every routine through its drop-in entry point with
+        host arrays (the Fortran caller's data flow) instead of keeping state on the device.
+        """
         inp = self.inp
         rs = inp.numberOfVariation + 3
         nb = inp.numberOfBasis
@@ -420,7 +445,7 @@ class Context:
         im = _f64f(inp.invariant_matrix)
         ims = _f64f(inp.invariant_matrix_spectrum) if inp.flag_spectrum else None
         ri = RunInput(nb, _p(bo, c_int32), _p(E, c_double), _p(im, c_double), _p(ims, c_double),
-                      int(bool(spectrum)), 0)
+                      int(bool(spectrum)), int(bool(host_drop_in)))
         nit = inp.numberOfIteration - inp.indexOfFirstIteration + 1
         nmat = max(inp.numberOfMatrix, 1)
         nbin_cap = 20001

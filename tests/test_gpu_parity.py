@@ -175,3 +175,10 @@ def test_device_resident_run_matches_oracle(ctx_factory):
     for k, i in enumerate(its):
         flow = st.flow[i][:8]
         assert np.max(np.abs(res["flow"][k][:len(flow)] - flow)) <= 1e-11
+    # the same run through the drop-in entry points with host arrays
+    res2 = ctx.run(spectrum=True, host_drop_in=True)
+    assert [int(k) for k in res2["kept"]] == [int(k) for k in res["kept"]]
+    assert np.max(np.abs(res2["binPos"][:, 1] - st.binPos[:, 1])) <= BIN_TOL
+    assert np.max(np.abs(res2["binNeg"][:, 1] - st.binNeg[:, 1])) <= BIN_TOL
+    for N in range(st.startTrancation, st.nIter):
+        assert abs(res2["rdmTrace"][N] - 1.0) <= 1e-12
