@@ -51,7 +51,15 @@ def parse():
     p.add_argument("--impl", default="b200", choices=["b200", "reference"])
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-cpu", action="store_true")
-    return p.parse_args()
+    # profiling helpers: a shorter sweep of the same model (not the headline workload)
+    p.add_argument("--iterations", type=int, default=None)
+    p.add_argument("--n-keep", type=int, default=None)
+    a = p.parse_args()
+    if a.iterations is not None:
+        WORKLOAD["n_iterations"] = a.iterations
+    if a.n_keep is not None:
+        WORKLOAD["n_keep"] = a.n_keep
+    return a
 
 
 def dist_env():
