@@ -215,6 +215,26 @@ typedef struct nrg_spike_io {
 NRG_API int nrg_spike_zero_temperature(nrg_context* ctx, int32_t iteration, const nrg_spike_io* io);
 NRG_API int nrg_spike_cfs(nrg_context* ctx, int32_t iteration, const nrg_spike_io* io);
 
+/* ---- one symmetric block without any device allocation --------------------------------
+ * No counterpart in the reference.  For callers that cannot allocate device memory: a
+ * host application whose pool allocator owns the whole device, or a caller that must not
+ * trigger the implicit device synchronisation of cudaMalloc/cudaFree inside a pipelined
+ * stream of work.  Diagonalises one symmetric FP64 block (column-major, order n <=
+ * NRG_NOALLOC_MAX_ORDER) with the same per-sector eigensolver kernel nrg_diagonalization
+ * uses (without the |V| < 1e-14 chop): eigenvalues ascending, eigenvectors in the same
+ * column order.  H, eigenvalues and eigenvectors are caller-owned device arrays (H may
+ * equal eigenvectors).  No context is needed: the call runs on the current device and on
+ * `stream` (NULL = default stream), and returns after the stream has drained.
+ * Its workspace is a static device array of about 417 KB, present on every device that
+ * loads the library until the process exits.  The first call on a device looks up that
+ * array's address (cudaGetSymbolAddress), so make the first call before any stream
+ * capture.  Every call shares the one array: calls that overlap on the GPU (concurrent
+ * streams, threads) race and must be serialised by the caller.  Orders above the maximum
+ * return NRG_ERR_TOO_LARGE. */
+#define NRG_NOALLOC_MAX_ORDER 128
+NRG_API int nrg_block_eigh_noalloc(const double* H, int32_t n, double* eigenvalues,
+                                   double* eigenvectors, void* stream);
+
 /* ---- whole run: main.F90:142-252 with everything device resident ---------------------
  * Replays the reference's driver (forward NRG sweep, backward reduced density matrices,
  * CFS spectrum at T = 0) on one device.  Initial state as read from initial.dat. */
