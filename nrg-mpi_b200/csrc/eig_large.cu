@@ -1,0 +1,588 @@
+// FP64 eigensolver for the large symmetry sectors of one iteration (order > 128), spread
+// over the whole GPU instead of one block per sector.  All large sectors advance together:
+//   1. blocked Householder tridiagonalisation (panels of 32 columns, the dlatrd scheme):
+//      per column one block per sector updates the column with the pending panel
+//      reflectors and forms the Householder vector, then a many-block kernel computes the
+//      symmetric matrix-vector product with the trailing matrix (column dot products,
+//      coalesced); after each panel the trailing matrix takes the rank-64 update
+//      A -= [V W][W V]^T as one grouped GEMM;
+//   2. divide and conquer: merges up to 128 rows inside one block per sector; larger
+//      merges in phases (deflation, secular roots, Gu-Eisenstat z, rank-one eigenvectors,
+//      final order) with the eigenvector update Z(:, kept) * U as a grouped GEMM;
+//   3. back-transformation in panels of 64 reflectors: Gram matrix and V^T Z as grouped
+//      GEMMs, the triangular factor T in one block, then Z -= (V T)(V^T Z).
+#include "eig_common.cuh"
+#include "internal.hpp"
+
+#include <algorithm>
+#include <cstring>
+#include <vector>
+
+namespace {
+
+constexpr int NB = 32;        // tridiagonalisation panel
+constexpr int NBB = 64;       // back-transformation panel
+constexpr int DC_LOW = 128;   // merges of up to this many rows run inside one block
+constexpr int TPB = 256;
+constexpr int CB = 32;        // columns per block in the symmetric matrix-vector product
+
+struct LSec {
+    long long a_off, e_off, w_off, i_off;
+    int n, pad;
+};
+
+long long lws_doubles(long long n) { return 3 * n * n + 2LL * NB * n + n + 16 * n + 64; }
+long long lws_ints(long long n) { return 12 * n + 64; }
+
+struct LView {
+    double *A, *Z, *U, *Qt, *VW, *y, *vec, *D, *E, *TAU;
+    int* I;
+    Scratch S;
+    int n;
+};
+
+__device__ LView lview(const LSec& s, double* eigbuf, double* wsd, int* wsi) {
+    LView v;
+    const long long n = s.n, sq = n * n;
+    v.n = s.n;
+    v.A = eigbuf + s.a_off;
+    double* W = wsd + s.w_off;
+    v.Z = W;
+    v.U = W + sq;
+    v.Qt = W + 2 * sq;
+    v.VW = W + 3 * sq;
+    v.y = v.VW + 2LL * NB * n;
+    v.vec = v.y + n;
+    v.D = v.vec;
+    v.E = v.vec + n;
+    v.TAU = v.vec + 2 * n;
+    v.I = wsi + s.i_off;
+    v.S = scratch_at(v.vec, v.I, s.n);
+    return v;
+}
+
+// ---------------------------------------------------------------------------------
+// tridiagonalisation
+// ---------------------------------------------------------------------------------
+
+// W(:, jj) for column c of the panel (rows c+1..n-1): dlatrd's w update
+__device__ void finish_w(LView& L, int c, int jj, const double* t1s, double* t1, double* t2, double* red) {
+    (void)t1s;
+    const int n = L.n, tid = threadIdx.x, T = blockDim.x;
+    const int warp = tid >> 5, lane = tid & 31, nw = T >> 5;
+    const double* V = L.VW;
+    double* W = L.VW + (size_t)NB * n;
+    const double* v = V + (size_t)jj * n;
+    for (int q = warp; q < 2 * jj; q += nw) {
+        const double* col = q < jj ? W + (size_t)q * n : V + (size_t)(q - jj) * n;
+        double s = 0.0;
+        for (int i = c + 1 + lane; i < n; i += 32) s = fma(col[i], v[i], s);
+        for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+        if (lane == 0) { if (q < jj) t1[q] = s; else t2[q - jj] = s; }
+    }
+    __syncthreads();
+    const double tau = L.TAU[c];
+    double* w = W + (size_t)jj * n;
+    double part = 0.0;
+    for (int i = c + 1 + tid; i < n; i += T) {
+        double s = L.y[i];
+        for (int q = 0; q < jj; ++q) s -= V[i + (size_t)q * n] * t1[q] + W[i + (size_t)q * n] * t2[q];
+        s *= tau;
+        w[i] = s;
+        part += s * v[i];
+    }
+    const double wv = block_sum(part, red);
+    const double al = -0.5 * tau * wv;
+    for (int i = c + 1 + tid; i < n; i += T) w[i] += al * v[i];
+    __syncthreads();
+}
+
+__global__ void __launch_bounds__(TPB) k_tri_col(const LSec* __restrict__ secs, int k, double* eigbuf,
+                                                 double* wsd, int* wsi) {
+    __shared__ double red[32];
+    __shared__ double t1[NB], t2[NB];
+    const LSec sec = secs[blockIdx.x];
+    if (k > sec.n - 2) return;
+    LView L = lview(sec, eigbuf, wsd, wsi);
+    const int n = L.n, tid = threadIdx.x, T = blockDim.x;
+    const int j = k % NB;
+    if (j > 0) finish_w(L, k - 1, j - 1, nullptr, t1, t2, red);
+    double* V = L.VW;
+    double* W = L.VW + (size_t)NB * n;
+    double* col = L.A + (size_t)k * n;
+    // column k takes the pending updates of the panel's first j reflectors
+    for (int i = k + tid; i < n; i += T) {
+        double s = 0.0;
+        for (int q = 0; q < j; ++q)
+            s += V[i + (size_t)q * n] * W[k + (size_t)q * n] + W[i + (size_t)q * n] * V[k + (size_t)q * n];
+        col[i] -= s;
+    }
+    __syncthreads();
+    if (tid == 0) L.D[k] = col[k];
+    const double alpha = col[k + 1];
+    double part = 0.0;
+    for (int i = k + 2 + tid; i < n; i += T) part += col[i] * col[i];
+    const double xn2 = block_sum(part, red);
+    double* v = V + (size_t)j * n;
+    if (xn2 == 0.0) {
+        for (int i = k + 1 + tid; i < n; i += T) v[i] = (i == k + 1) ? 1.0 : 0.0;
+        if (tid == 0) { L.E[k] = alpha; L.TAU[k] = 0.0; }
+        return;
+    }
+    const double beta = -copysign(sqrt(alpha * alpha + xn2), alpha);
+    const double tt = (beta - alpha) / beta;
+    const double scal = 1.0 / (alpha - beta);
+    for (int i = k + 1 + tid; i < n; i += T) {
+        double vi = 1.0;
+        if (i > k + 1) { vi = col[i] * scal; col[i] = vi; }
+        v[i] = vi;
+    }
+    if (tid == 0) { L.E[k] = beta; L.TAU[k] = tt; }
+}
+
+// y(i) = sum_{l > k} A(l, i) v(l) for i > k: one warp per column, CB columns per block
+__global__ void __launch_bounds__(TPB) k_tri_symv(const LSec* __restrict__ secs, int nsec, int k,
+                                                  double* eigbuf, double* wsd, int* wsi) {
+    extern __shared__ double vsm[];
+    // find this block's sector among those still active at column k
+    int s = 0, base = 0;
+    for (; s < nsec; ++s) {
+        const int n = secs[s].n;
+        if (k > n - 2) continue;
+        const int nb = (n - k - 1 + CB - 1) / CB;
+        if ((int)blockIdx.x < base + nb) break;
+        base += nb;
+    }
+    if (s >= nsec) return;
+    LView L = lview(secs[s], eigbuf, wsd, wsi);
+    const int n = L.n, m = n - k - 1;
+    const int j = k % NB;
+    const double* v = L.VW + (size_t)j * n + (k + 1);
+    for (int i = threadIdx.x; i < m; i += blockDim.x) vsm[i] = v[i];
+    __syncthreads();
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+    const int c0 = ((int)blockIdx.x - base) * CB;
+    for (int cc = warp; cc < CB; cc += nw) {
+        const int ci = c0 + cc;
+        if (ci >= m) break;
+        const double* col = L.A + (size_t)(k + 1 + ci) * n + (k + 1);
+        double s0 = 0.0, s1 = 0.0;
+        int l = lane;
+        for (; l + 32 < m; l += 64) {
+            s0 = fma(col[l], vsm[l], s0);
+            s1 = fma(col[l + 32], vsm[l + 32], s1);
+        }
+        if (l < m) s0 = fma(col[l], vsm[l], s0);
+        double sum = s0 + s1;
+        for (int o = 16; o > 0; o >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, o);
+        if (lane == 0) L.y[k + 1 + ci] = sum;
+    }
+}
+
+// W for the last column a sector processed in the panel starting at p
+__global__ void __launch_bounds__(TPB) k_tri_finish(const LSec* __restrict__ secs, int p, double* eigbuf,
+                                                    double* wsd, int* wsi) {
+    __shared__ double red[32];
+    __shared__ double t1[NB], t2[NB];
+    const LSec sec = secs[blockIdx.x];
+    const int c = min(p + NB - 1, sec.n - 2);
+    if (c < p) return;
+    LView L = lview(sec, eigbuf, wsd, wsi);
+    finish_w(L, c, c - p, nullptr, t1, t2, red);
+}
+
+__global__ void k_tri_end(const LSec* __restrict__ secs, double* eigbuf, double* wsd, int* wsi) {
+    const LSec sec = secs[blockIdx.x];
+    if (threadIdx.x != 0) return;
+    LView L = lview(sec, eigbuf, wsd, wsi);
+    const int n = L.n;
+    L.D[n - 1] = L.A[(size_t)(n - 1) + (size_t)(n - 1) * n];
+    L.E[n - 1] = 0.0;
+}
+
+// ---------------------------------------------------------------------------------
+// divide and conquer
+// ---------------------------------------------------------------------------------
+__global__ void __launch_bounds__(512) k_dc_low(const LSec* __restrict__ secs, double* eigbuf, double* wsd,
+                                                int* wsi, int* status) {
+    extern __shared__ double sm[];
+    LView L = lview(secs[blockIdx.x], eigbuf, wsd, wsi);
+    const int n = L.n, tid = threadIdx.x, T = blockDim.x;
+    double* red = sm;
+    double* gsm = sm + 32;
+    const long long sq = (long long)n * n;
+    for (long long e = tid; e < sq; e += T) L.Z[e] = 0.0;
+    __syncthreads();
+    for (int i = tid; i < n; i += T) {
+        L.Z[(size_t)i + (size_t)i * n] = 1.0;
+        double dv = L.D[i];
+        if (i > 0) dv -= fabs(L.E[i - 1]);
+        if (i < n - 1) dv -= fabs(L.E[i]);
+        L.S.vals[i] = dv;
+    }
+    __syncthreads();
+    for (int i = tid; i < n; i += T) L.D[i] = L.S.vals[i];
+    __syncthreads();
+    const int warp = tid >> 5, lane = tid & 31, nwarps = T >> 5;
+    for (int s = 1; 2 * s <= DC_LOW && s < n; s *= 2) {
+        if (2 * s <= 32) {
+            WarpG wg{lane};
+            int mi = 0;
+            for (int a = 0; a + s < n; a += 2 * s, ++mi) {
+                if (mi % nwarps != warp) continue;
+                dc_merge(wg, a, a + s, min(a + 2 * s, n), n, L.Z, L.D, L.E, L.S, L.U, L.Qt, red, gsm, status);
+            }
+            __syncthreads();
+        } else {
+            BlockG bg;
+            for (int a = 0; a + s < n; a += 2 * s)
+                dc_merge(bg, a, a + s, min(a + 2 * s, n), n, L.Z, L.D, L.E, L.S, L.U, L.Qt, red, gsm, status);
+        }
+    }
+}
+
+struct Merge {
+    int sec, a, mid, b;
+    int blk0, nblk;   // blocks of the parallel phases
+};
+
+__device__ int find_merge(const Merge* ms, int nm) {
+    int lo = 0, hi = nm - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (ms[mid].blk0 <= (int)blockIdx.x) lo = mid; else hi = mid - 1;
+    }
+    return lo;
+}
+
+__global__ void __launch_bounds__(512) k_dc_prep(const LSec* __restrict__ secs, const Merge* __restrict__ ms,
+                                                 double* eigbuf, double* wsd, int* wsi) {
+    __shared__ double red[32];
+    const Merge m = ms[blockIdx.x];
+    LView L = lview(secs[m.sec], eigbuf, wsd, wsi);
+    merge_prep(BlockG{}, m.a, m.mid, m.b, L.n, L.Z, L.D, L.E, L.S, red);
+}
+
+// phase 1 roots, 2 zhat, 3 rank-one vectors + values, 4 final order + GEMM index lists,
+// 5 deflated copies, 6 copy back
+__global__ void __launch_bounds__(TPB) k_dc_phase(const LSec* __restrict__ secs, const Merge* __restrict__ ms,
+                                                  int nm, int phase, double* eigbuf, double* wsd, int* wsi,
+                                                  int* status) {
+    const int mi = find_merge(ms, nm);
+    const Merge m = ms[mi];
+    LView L = lview(secs[m.sec], eigbuf, wsd, wsi);
+    const int t = ((int)blockIdx.x - m.blk0) * blockDim.x + threadIdx.x;
+    const int T = m.nblk * blockDim.x;
+    switch (phase) {
+        case 1: merge_roots(t, T, m.a, m.mid, L.E, L.S, status); break;
+        case 2: merge_zhat(t, T, m.a, m.mid, L.E, L.S); break;
+        case 3: merge_ucols(t, T, m.a, m.b, L.n, L.S, L.U); break;
+        case 4: {
+            merge_rank(t, T, m.a, m.b, L.S);
+            const int K = L.S.mk[m.a];
+            // gathered columns of Z for the GEMM: a + perm[nd[q]] (ra reused after prep)
+            for (int q = t; q < K; q += T) L.S.ra[m.a + q] = m.a + L.S.perm[m.a + L.S.nd[m.a + q]];
+            break;
+        }
+        case 5: merge_deflated(t, T, m.a, m.b, L.n, L.Z, L.Qt, L.S); break;
+        case 6: merge_copyback(t, T, m.a, m.b, L.n, L.Z, L.D, L.Qt, L.S); break;
+        default: break;
+    }
+}
+
+// scatter columns a + pos[j] of the nondeflated eigenvectors (rb reused)
+__global__ void k_dc_poscols(const LSec* __restrict__ secs, const Merge* __restrict__ ms, int nm,
+                             double* eigbuf, double* wsd, int* wsi) {
+    const int mi = find_merge(ms, nm);
+    const Merge m = ms[mi];
+    LView L = lview(secs[m.sec], eigbuf, wsd, wsi);
+    const int t = ((int)blockIdx.x - m.blk0) * blockDim.x + threadIdx.x;
+    const int T = m.nblk * blockDim.x;
+    const int K = L.S.mk[m.a];
+    for (int j = t; j < K; j += T) L.S.rb[m.a + j] = m.a + L.S.pos[m.a + j];
+}
+
+// ---------------------------------------------------------------------------------
+// back-transformation
+// ---------------------------------------------------------------------------------
+// explicit V panel (mr x b, ld mr) of reflectors jb .. jb+b-1 into U
+__global__ void k_bt_vpanel(const LSec* __restrict__ secs, int q, double* eigbuf, double* wsd, int* wsi) {
+    const LSec sec = secs[blockIdx.y];
+    const int n = sec.n, nr = n - 1, jb = q * NBB;
+    if (jb >= nr) return;
+    LView L = lview(sec, eigbuf, wsd, wsi);
+    const int b = min(NBB, nr - jb), r0 = jb + 1, mr = n - r0;
+    const long long tot = (long long)mr * b;
+    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < tot; e += (long long)gridDim.x * blockDim.x) {
+        const int i = (int)(e % mr), c = (int)(e / mr);
+        const int k = jb + c, row = r0 + i;
+        double v = 0.0;
+        if (row == k + 1) v = 1.0;
+        else if (row > k + 1) v = L.A[(size_t)row + (size_t)k * n];
+        L.U[e] = v;
+    }
+}
+
+// triangular factor T of the panel from the Gram matrix G (in Qt, b x b) and tau; T goes
+// to Qt + NBB*NBB (b x b, ld NBB)
+__global__ void k_bt_tfactor(const LSec* __restrict__ secs, int q, double* eigbuf, double* wsd, int* wsi) {
+    __shared__ double Ts[NBB * NBB];
+    const LSec sec = secs[blockIdx.x];
+    const int n = sec.n, nr = n - 1, jb = q * NBB;
+    if (jb >= nr) return;
+    LView L = lview(sec, eigbuf, wsd, wsi);
+    const int b = min(NBB, nr - jb);
+    const double* G = L.Qt;   // ld NBB
+    const int p = threadIdx.x;
+    for (int e = threadIdx.x; e < NBB * NBB; e += blockDim.x) Ts[e] = 0.0;
+    __syncthreads();
+    for (int c = 0; c < b; ++c) {
+        const double tc = L.TAU[jb + c];
+        double acc = 0.0;
+        if (p < c)
+            for (int qq = p; qq < c; ++qq) acc += Ts[p + qq * NBB] * (-tc * G[qq + c * NBB]);
+        __syncthreads();
+        if (p < c) Ts[p + c * NBB] = acc;
+        if (p == 0) Ts[c + c * NBB] = tc;
+        __syncthreads();
+    }
+    for (int e = threadIdx.x; e < NBB * NBB; e += blockDim.x) L.Qt[NBB * NBB + e] = Ts[e];
+}
+
+__global__ void k_large_out(const LSec* __restrict__ secs, double* eigbuf, double* evals, double* wsd, int* wsi) {
+    const LSec sec = secs[blockIdx.y];
+    LView L = lview(sec, eigbuf, wsd, wsi);
+    const long long n = sec.n, sq = n * n;
+    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < sq; e += (long long)gridDim.x * blockDim.x)
+        L.A[e] = L.Z[e];
+    if (blockIdx.x == 0)
+        for (int i = threadIdx.x; i < sec.n; i += blockDim.x) evals[sec.e_off + i] = L.D[i];
+}
+
+}  // namespace
+
+namespace nrg {
+
+// ---------------------------------------------------------------------------------
+// host orchestration
+// ---------------------------------------------------------------------------------
+int syev_large(nrg_context* ctx, const std::vector<SyevSector>& in, double* d_V, double* d_E) {
+    const int ns = (int)in.size();
+    if (ns == 0) return NRG_OK;
+    cudaStream_t st = ctx->stream;
+    std::vector<LSec> secs(ns);
+    long long wd = 0, wi = 0;
+    int maxn = 0;
+    for (int s = 0; s < ns; ++s) {
+        secs[s].a_off = in[s].a_off;
+        secs[s].e_off = in[s].e_off;
+        secs[s].n = in[s].n;
+        secs[s].pad = 0;
+        secs[s].w_off = wd;
+        secs[s].i_off = wi;
+        wd += lws_doubles(in[s].n);
+        wi += lws_ints(in[s].n);
+        maxn = std::max(maxn, in[s].n);
+    }
+    DevBuf& bsec = ctx->scratch.b[24];
+    DevBuf& bwd = ctx->scratch.b[25];
+    DevBuf& bwi = ctx->scratch.b[26];
+    DevBuf& bidx = ctx->scratch.b[27];
+    DevBuf& bmrg = ctx->scratch.b[28];
+    NRG_TRY(bsec.ensure(sizeof(LSec) * ns));
+    NRG_TRY(bwd.ensure(sizeof(double) * (size_t)wd));
+    NRG_TRY(bwi.ensure(sizeof(int) * (size_t)wi));
+    NRG_CUDA_TRY(cudaMemcpyAsync(bsec.p, secs.data(), sizeof(LSec) * ns, cudaMemcpyHostToDevice, st));
+    ctx->h2d += (long long)sizeof(LSec) * ns;
+    const LSec* dsec = bsec.as<LSec>();
+    double* wsd = bwd.as<double>();
+    int* wsi = bwi.as<int>();
+    // column index lists of the panel update [V W] and [W V] for every panel width jc
+    {
+        std::vector<int> idx(2 * NB * 2 * NB);
+        for (int jc = 1; jc <= NB; ++jc)
+            for (int q = 0; q < 2 * NB; ++q) {
+                idx[(size_t)(jc - 1) * 4 * NB + q] = q < jc ? q : NB + (q - jc);            // [V W]
+                idx[(size_t)(jc - 1) * 4 * NB + 2 * NB + q] = q < jc ? NB + q : q - jc;     // [W V]
+            }
+        NRG_TRY(bidx.ensure(sizeof(int) * idx.size()));
+        NRG_CUDA_TRY(cudaMemcpyAsync(bidx.p, idx.data(), sizeof(int) * idx.size(), cudaMemcpyHostToDevice, st));
+        NRG_CUDA_TRY(cudaStreamSynchronize(st));
+    }
+    const int* didx = bidx.as<int>();
+    const size_t symv_smem = sizeof(double) * (size_t)maxn;
+    if (symv_smem > 48 * 1024)
+        NRG_CUDA_TRY(cudaFuncSetAttribute(k_tri_symv, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)symv_smem));
+
+    // ---- 1. tridiagonalisation ----
+    for (int p = 0; p < maxn - 1; p += NB) {
+        for (int j = 0; j < NB; ++j) {
+            const int k = p + j;
+            if (k > maxn - 2) break;
+            k_tri_col<<<ns, TPB, 0, st>>>(dsec, k, d_V, wsd, wsi);
+            int nblk = 0;
+            for (int s = 0; s < ns; ++s)
+                if (k <= secs[s].n - 2) nblk += (secs[s].n - k - 1 + CB - 1) / CB;
+            k_tri_symv<<<nblk, TPB, symv_smem, st>>>(dsec, ns, k, d_V, wsd, wsi);
+            ctx->launches += 2;
+        }
+        k_tri_finish<<<ns, TPB, 0, st>>>(dsec, p, d_V, wsd, wsi);
+        ctx->launches++;
+        NRG_CUDA_TRY(cudaGetLastError());
+        std::vector<GemmProblem> probs;
+        for (int s = 0; s < ns; ++s) {
+            const int n = secs[s].n;
+            const int c = std::min(p + NB - 1, n - 2);
+            if (c < p) continue;
+            const int jc = c - p + 1, r0 = p + jc;
+            if (r0 >= n) continue;
+            double* VW = wsd + secs[s].w_off + 3LL * n * n;
+            GemmProblem P;
+            std::memset(&P, 0, sizeof(P));
+            P.M = n - r0; P.N = n - r0; P.K = 2 * jc;
+            P.alpha = -1.0; P.beta = 1.0;
+            P.A = VW + r0; P.a_si = 1; P.a_sk = n; P.a_ki = didx + (size_t)(jc - 1) * 4 * NB;
+            P.B = VW + r0; P.b_sk = n; P.b_ki = didx + (size_t)(jc - 1) * 4 * NB + 2 * NB; P.b_sj = 1;
+            P.C = d_V + secs[s].a_off + r0 + (long long)r0 * n; P.c_si = 1; P.c_sj = n;
+            probs.push_back(P);
+        }
+        NRG_TRY(launch_ggemm(ctx, probs, 29));
+    }
+    k_tri_end<<<ns, 32, 0, st>>>(dsec, d_V, wsd, wsi);
+    ctx->launches++;
+
+    // ---- 2. divide and conquer ----
+    {
+        const int gsz = 16 * (4 * (512 / 16) + 1) + 16 * 65;
+        const size_t smem = sizeof(double) * (32 + gsz);
+        k_dc_low<<<ns, 512, smem, st>>>(dsec, d_V, wsd, wsi, ctx->d_status.as<int>());
+        ctx->launches++;
+        NRG_CUDA_TRY(cudaGetLastError());
+    }
+    for (int s = DC_LOW; s < maxn; s *= 2) {
+        std::vector<Merge> ms;
+        int blk = 0;
+        for (int x = 0; x < ns; ++x) {
+            const int n = secs[x].n;
+            for (int a = 0; a + s < n; a += 2 * s) {
+                Merge m;
+                m.sec = x; m.a = a; m.mid = a + s; m.b = std::min(a + 2 * s, n);
+                m.nblk = (m.b - m.a + TPB - 1) / TPB;
+                m.blk0 = blk;
+                blk += m.nblk;
+                ms.push_back(m);
+            }
+        }
+        if (ms.empty()) continue;
+        const int nm = (int)ms.size();
+        NRG_TRY(bmrg.ensure(sizeof(Merge) * nm));
+        NRG_CUDA_TRY(cudaMemcpyAsync(bmrg.p, ms.data(), sizeof(Merge) * nm, cudaMemcpyHostToDevice, st));
+        ctx->h2d += (long long)sizeof(Merge) * nm;
+        const Merge* dms = bmrg.as<Merge>();
+        k_dc_prep<<<nm, 512, 0, st>>>(dsec, dms, d_V, wsd, wsi);
+        for (int ph = 1; ph <= 4; ++ph)
+            k_dc_phase<<<blk, TPB, 0, st>>>(dsec, dms, nm, ph, d_V, wsd, wsi, ctx->d_status.as<int>());
+        k_dc_poscols<<<blk, TPB, 0, st>>>(dsec, dms, nm, d_V, wsd, wsi);
+        ctx->launches += 6;
+        NRG_CUDA_TRY(cudaGetLastError());
+        // K of every merge (sizes the GEMMs)
+        std::vector<int> Ks(nm);
+        for (int i = 0; i < nm; ++i) {
+            int* mk = wsi + secs[ms[i].sec].i_off + 7LL * secs[ms[i].sec].n + ms[i].a;
+            NRG_CUDA_TRY(cudaMemcpyAsync(&Ks[i], mk, sizeof(int), cudaMemcpyDeviceToHost, st));
+        }
+        NRG_CUDA_TRY(cudaStreamSynchronize(st));
+        ctx->d2h += (long long)sizeof(int) * nm;
+        std::vector<GemmProblem> probs;
+        for (int i = 0; i < nm; ++i) {
+            const Merge& m = ms[i];
+            const int n = secs[m.sec].n, nn = m.b - m.a, K = Ks[i];
+            if (K == 0) continue;
+            double* W = wsd + secs[m.sec].w_off;
+            const long long sq = (long long)n * n;
+            int* I = wsi + secs[m.sec].i_off;
+            GemmProblem P;
+            std::memset(&P, 0, sizeof(P));
+            P.M = nn; P.N = K; P.K = K; P.alpha = 1.0; P.beta = 0.0;
+            P.A = W + m.a; P.a_si = 1; P.a_sk = n; P.a_ki = I + 5LL * n + m.a;          // Z(:, a+perm[nd[q]])
+            P.B = W + sq + m.a + (long long)m.a * n; P.b_sk = 1; P.b_sj = n;           // U block
+            P.C = W + 2 * sq + m.a; P.c_si = 1; P.c_sj = n; P.c_ji = I + 6LL * n + m.a;  // Qt(:, a+pos[j])
+            probs.push_back(P);
+        }
+        NRG_TRY(launch_ggemm(ctx, probs, 29));
+        k_dc_phase<<<blk, TPB, 0, st>>>(dsec, dms, nm, 5, d_V, wsd, wsi, ctx->d_status.as<int>());
+        k_dc_phase<<<blk, TPB, 0, st>>>(dsec, dms, nm, 6, d_V, wsd, wsi, ctx->d_status.as<int>());
+        ctx->launches += 2;
+        NRG_CUDA_TRY(cudaGetLastError());
+    }
+
+    // ---- 3. back-transformation, panels of NBB reflectors, last panel first ----
+    const int qmax = (maxn - 2) / NBB;   // panels cover reflectors 0 .. n-2
+    for (int q = qmax; q >= 0; --q) {
+        std::vector<int> act;
+        for (int s = 0; s < ns; ++s)
+            if (q * NBB < secs[s].n - 1) act.push_back(s);
+        if (act.empty()) continue;
+        k_bt_vpanel<<<dim3(16, ns), TPB, 0, st>>>(dsec, q, d_V, wsd, wsi);
+        ctx->launches++;
+        std::vector<GemmProblem> g1;
+        for (int s : act) {
+            const int n = secs[s].n, nr = n - 1, jb = q * NBB, b = std::min(NBB, nr - jb);
+            const int r0 = jb + 1, mr = n - r0;
+            double* W = wsd + secs[s].w_off;
+            const long long sq = (long long)n * n;
+            double* Vb = W + sq;            // U
+            double* G = W + 2 * sq;         // Qt: G (NBB x NBB), T, then V^T Z
+            GemmProblem P;
+            std::memset(&P, 0, sizeof(P));
+            P.M = b; P.N = b; P.K = mr; P.alpha = 1.0; P.beta = 0.0;
+            P.A = Vb; P.a_si = mr; P.a_sk = 1;
+            P.B = Vb; P.b_sk = 1; P.b_sj = mr;
+            P.C = G; P.c_si = 1; P.c_sj = NBB;
+            g1.push_back(P);
+            GemmProblem Q;
+            std::memset(&Q, 0, sizeof(Q));
+            Q.M = b; Q.N = n; Q.K = mr; Q.alpha = 1.0; Q.beta = 0.0;
+            Q.A = Vb; Q.a_si = mr; Q.a_sk = 1;
+            Q.B = W + r0; Q.b_sk = 1; Q.b_sj = n;                       // Z(r0:, :)
+            Q.C = G + 2 * NBB * NBB; Q.c_si = 1; Q.c_sj = b;            // Wt (b x n)
+            g1.push_back(Q);
+        }
+        NRG_TRY(launch_ggemm(ctx, g1, 29));
+        k_bt_tfactor<<<ns, NBB, 0, st>>>(dsec, q, d_V, wsd, wsi);
+        ctx->launches++;
+        std::vector<GemmProblem> g2, g3;
+        for (int s : act) {
+            const int n = secs[s].n, nr = n - 1, jb = q * NBB, b = std::min(NBB, nr - jb);
+            const int r0 = jb + 1, mr = n - r0;
+            double* W = wsd + secs[s].w_off;
+            const long long sq = (long long)n * n;
+            double* Vb = W + sq;
+            double* Tm = W + 2 * sq + NBB * NBB;
+            double* Wt = W + 2 * sq + 2 * NBB * NBB;
+            double* VT = Vb + (long long)mr * NBB;     // (mr x b) after Vb in U
+            GemmProblem P;
+            std::memset(&P, 0, sizeof(P));
+            P.M = mr; P.N = b; P.K = b; P.alpha = 1.0; P.beta = 0.0;
+            P.A = Vb; P.a_si = 1; P.a_sk = mr;
+            P.B = Tm; P.b_sk = 1; P.b_sj = NBB;
+            P.C = VT; P.c_si = 1; P.c_sj = mr;
+            g2.push_back(P);
+            GemmProblem Q;
+            std::memset(&Q, 0, sizeof(Q));
+            Q.M = mr; Q.N = n; Q.K = b; Q.alpha = -1.0; Q.beta = 1.0;
+            Q.A = VT; Q.a_si = 1; Q.a_sk = mr;
+            Q.B = Wt; Q.b_sk = 1; Q.b_sj = b;
+            Q.C = W + r0; Q.c_si = 1; Q.c_sj = n;
+            g3.push_back(Q);
+        }
+        NRG_TRY(launch_ggemm(ctx, g2, 29));
+        NRG_TRY(launch_ggemm(ctx, g3, 29));
+    }
+    k_large_out<<<dim3(32, ns), TPB, 0, st>>>(dsec, d_V, d_E, wsd, wsi);
+    ctx->launches++;
+    NRG_CUDA_TRY(cudaGetLastError());
+    return NRG_OK;
+}
+
+}  // namespace nrg

@@ -6,9 +6,9 @@
 // through index lists instead.
 //
 //   C(i,j) = alpha * sum_k A(i,k) B(k,j) + beta * C(i,j)
-//   A(i,k) = A[ri(i)*a_si + k*a_sk]              ri = a_ri ? a_ri[i] : i
+//   A(i,k) = A[ri(i)*a_si + ki(k)*a_sk]          ri = a_ri ? a_ri[i] : i, ki likewise
 //   B(k,j) = B[ki(k)*b_sk + ji(j)*b_sj]          ki = b_ki ? b_ki[k] : k, ji likewise
-//   C(i,j) = C[ci(i)*c_si + j*c_sj]              ci = c_ri ? c_ri[i] : i
+//   C(i,j) = C[ci(i)*c_si + cj(j)*c_sj]          ci = c_ri ? c_ri[i] : i, cj likewise
 //
 // 64x64 output tiles, 256 threads with 4x4 register tiles, k slabs of 16 staged in
 // shared memory, double buffered.  Loads are coalesced along whichever index of each
@@ -33,7 +33,8 @@ __device__ __forceinline__ void load_slab(const GemmProblem& P, int i0, int j0, 
         double v = 0.0;
         if (gi < P.M && gk < P.K) {
             const long long ri = P.a_ri ? P.a_ri[gi] : gi;
-            v = P.A[ri * P.a_si + (long long)gk * P.a_sk];
+            const long long ki = P.a_ki ? P.a_ki[gk] : gk;
+            v = P.A[ri * P.a_si + ki * P.a_sk];
         }
         As[kk * LDS + ii] = v;
     }
@@ -106,7 +107,8 @@ __global__ void __launch_bounds__(NT) k_ggemm(const GemmProblem* __restrict__ pr
         for (int c = 0; c < 4; ++c) {
             const int gj = j0 + tx + 16 * c;
             if (gj >= P.N) continue;
-            double* out = P.C + ci * P.c_si + (long long)gj * P.c_sj;
+            const long long cj = P.c_ji ? P.c_ji[gj] : gj;
+            double* out = P.C + ci * P.c_si + cj * P.c_sj;
             const double v = P.alpha * acc[r][c];
             *out = (P.beta == 0.0) ? v : P.beta * *out + v;
         }

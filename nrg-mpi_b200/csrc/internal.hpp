@@ -78,7 +78,7 @@ struct Sectors {
 // the context
 // ------------------------------------------------------------------------------------
 struct Scratch {
-    DevBuf b[24];
+    DevBuf b[40];
 };
 
 }  // namespace nrg
@@ -112,11 +112,18 @@ struct GemmProblem {
     int M, N, K;
     int tiles;              // filled by the launcher
     double alpha, beta;
-    const double* A; long long a_si, a_sk; const int* a_ri;   // A(i,k) = A[ri(i)*a_si + k*a_sk]
+    // A(i,k) = A[ri(i)*a_si + ki(k)*a_sk], ri = a_ri ? a_ri[i] : i, ki = a_ki ? a_ki[k] : k
+    const double* A; long long a_si, a_sk; const int* a_ri; const int* a_ki;
     const double* B; long long b_sk, b_sj; const int* b_ki; const int* b_ji;
-    double* C; long long c_si, c_sj; const int* c_ri;
+    // C(i,j) = C[ri(i)*c_si + ji(j)*c_sj]
+    double* C; long long c_si, c_sj; const int* c_ri; const int* c_ji;
 };
 int launch_ggemm(nrg_context* ctx, std::vector<GemmProblem>& probs, int scratch_slot);
+
+// eigensolver for sectors of order > 128 across the whole GPU (eig_large.cu); the
+// descriptors use a_off / e_off / n only
+int syev_large(nrg_context* ctx, const std::vector<SyevSector>& secs, double* d_V, double* d_E);
+constexpr int kLargeSector = 128;
 
 // ---- kernels (kernels.cu) ------------------------------------------------------------
 int run_assemble(nrg_context* ctx, int iteration, const Sectors& S, const SyevSector* d_secs,

@@ -178,22 +178,30 @@ int diag_device(nrg_context* ctx, int iteration, Sectors& S, const double* d_Eol
     std::vector<long long> colPrefix(nsec);
     std::vector<int> secStart(nsec);
     long long wsd = 0, wsi = 0, cols = 0;
-    int max_n = 1;
+    int max_n = 1, nlarge = 0;
+    std::vector<SyevSector> large;
     for (int x = 0; x < nsec; ++x) {
         const int s = order[x];
         SyevSector& q = secs[x];
         q.n = S.dim[s];
         q.a_off = S.ce[s];
         q.e_off = S.start[s];
-        q.w_off = wsd;
-        q.i_off = wsi;
+        q.w_off = 0;
+        q.i_off = 0;
         q.pad = 0;
-        wsd += syev_ws_doubles(q.n);
-        wsi += syev_ws_ints(q.n);
+        if (q.n > kLargeSector) {
+            large.push_back(q);
+            ++nlarge;
+        } else {
+            q.w_off = wsd;
+            q.i_off = wsi;
+            wsd += syev_ws_doubles(q.n);
+            wsi += syev_ws_ints(q.n);
+            max_n = std::max(max_n, q.n);
+        }
         colPrefix[x] = cols;
         cols += q.n;
         secStart[x] = S.start[s];
-        max_n = std::max(max_n, q.n);
     }
     DevBuf& bsec = ctx->scratch.b[0];
     DevBuf& bcol = ctx->scratch.b[1];
@@ -204,8 +212,8 @@ int diag_device(nrg_context* ctx, int iteration, Sectors& S, const double* d_Eol
     NRG_TRY(bsec.ensure(sizeof(SyevSector) * nsec));
     NRG_TRY(bcol.ensure(sizeof(long long) * nsec));
     NRG_TRY(bstart.ensure(sizeof(int) * nsec));
-    NRG_TRY(bwd.ensure(sizeof(double) * (size_t)wsd));
-    NRG_TRY(bwi.ensure(sizeof(int) * (size_t)wsi));
+    NRG_TRY(bwd.ensure(sizeof(double) * (size_t)std::max(wsd, 1LL)));
+    NRG_TRY(bwi.ensure(sizeof(int) * (size_t)std::max(wsi, 1LL)));
     NRG_TRY(bmin.ensure(sizeof(double) * 2));
     NRG_CUDA_TRY(cudaMemcpyAsync(bsec.p, secs.data(), sizeof(SyevSector) * nsec, cudaMemcpyHostToDevice, ctx->stream));
     NRG_CUDA_TRY(cudaMemcpyAsync(bcol.p, colPrefix.data(), sizeof(long long) * nsec, cudaMemcpyHostToDevice, ctx->stream));
@@ -219,9 +227,13 @@ int diag_device(nrg_context* ctx, int iteration, Sectors& S, const double* d_Eol
         NRG_CUDA_TRY(cudaEventCreate(&e1));
         NRG_CUDA_TRY(cudaEventRecord(e0, ctx->stream));
     }
-    NRG_TRY(launch_syev(bsec.as<SyevSector>(), nsec, max_n, d_V, d_E, bwd.as<double>(), bwi.as<int>(),
-                        ctx->d_status.as<int>(), ctx->stream));
-    ctx->launches++;
+    // sectors of order <= 128: one block each; larger ones: the multi-kernel pipeline
+    if (nsec > nlarge) {
+        NRG_TRY(launch_syev(bsec.as<SyevSector>() + nlarge, nsec - nlarge, max_n, d_V, d_E, bwd.as<double>(),
+                            bwi.as<int>(), ctx->d_status.as<int>(), ctx->stream));
+        ctx->launches++;
+    }
+    NRG_TRY(syev_large(ctx, large, d_V, d_E));
     if (ctx->profiling) {
         NRG_CUDA_TRY(cudaEventRecord(e1, ctx->stream));
         NRG_CUDA_TRY(cudaEventSynchronize(e1));

@@ -153,6 +153,52 @@ def test_spikes_per_iteration(driven):
     assert worst <= BIN_TOL, worst
 
 
+def test_large_sector_diagonalization(ctx_factory):
+    # N_keep = 512: sectors of order up to ~200 take the multi-kernel eigensolver
+    inp = small_siam(n_keep=512, n_iterations=9)
+    d = write_case(inp)
+    st = O.State(d)
+    ctx = ctx_factory(model.read_inputs(d))
+    nVar = st.nVar
+    worst_e, worst_v, largest = 0.0, 0.0, 0
+    for it in range(st.first, st.nIter + 1):
+        O.prepare_basis(st, it)
+        si, bi = st.subspaceInfo.copy(), st.basis_input.copy()
+        Eold, IMold = st.eigenvalue.copy(), st.im.copy(order="F")
+        E_g, V_g, bo_g, _ = ctx.diagonalization(it, si, bi, Eold, IMold)
+        O.diagonalization(st, it)
+        assert np.array_equal(bo_g, st.basis_output)
+        worst_e = max(worst_e, eig_rel_err(E_g, st.eigenvalue))
+        for (s, dd, Bo), (_, _, Bg) in zip(sector_blocks(si, st.eigenvector, nVar), sector_blocks(si, V_g, nVar)):
+            s0 = int(si[s, nVar + 2]) - 1
+            worst_v = max(worst_v, subspace_err(Bg, Bo, st.eigenvalue[s0:s0 + dd]))
+            largest = max(largest, dd)
+        O.postprocess(st, it)
+    assert largest > 128
+    assert worst_e <= EIG_TOL, worst_e
+    assert worst_v <= VEC_TOL, worst_v
+
+
+def test_config1_full_run(ctx_factory):
+    # the CPU-runnable workload: SIAM Lambda=2.5, U=0.1, N_keep=512, 40 iterations
+    inp = model.config(1)
+    d = write_case(inp)
+    st = O.run(d)
+    ctx = ctx_factory(model.read_inputs(d))
+    res = ctx.run(spectrum=True)
+    its = list(range(st.first, st.nIter + 1))
+    assert [int(k) for k in res["kept"]] == [st.kept[i] for i in its]
+    assert np.max(np.abs(res["binPos"][:, 1] - st.binPos[:, 1])) <= BIN_TOL
+    assert np.max(np.abs(res["binNeg"][:, 1] - st.binNeg[:, 1])) <= BIN_TOL
+    nbin = st.numberOfBin
+    for m in range(st.nMat):
+        tot = res["binPos"][m * nbin:(m + 1) * nbin, 1].sum() + res["binNeg"][m * nbin:(m + 1) * nbin, 1].sum()
+        assert abs(tot - 1.0) <= SUM_TOL
+    for k, i in enumerate(its):
+        flow = st.flow[i][:8]
+        assert np.max(np.abs(res["flow"][k][:len(flow)] - flow) / np.maximum(1.0, np.abs(flow))) <= 1e-11
+
+
 def test_device_resident_run_matches_oracle(ctx_factory):
     inp = small_siam(n_keep=48, n_iterations=14)
     d = write_case(inp)
