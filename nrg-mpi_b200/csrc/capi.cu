@@ -69,6 +69,12 @@ nrg_context::~nrg_context() {
     for (nrg::DevBuf* b : {&M.d_operation, &M.d_dflag, &M.d_dtype, &M.d_dch, &M.d_dswp, &M.d_bflag,
                            &M.d_bch, &M.d_dcoef, &M.d_imflag, &M.d_imcoef})
         b->release();
+    for (auto& c : stage_inflight) {
+        cudaEventSynchronize(c.ev);
+        cudaEventDestroy(c.ev);
+    }
+    for (cudaEvent_t e : event_pool) cudaEventDestroy(e);
+    if (stage_host) cudaFreeHost(stage_host);
 }
 
 using namespace nrg;
@@ -354,7 +360,7 @@ int nrg_diagonalization(nrg_context* ctx, int32_t iteration, const nrg_diagonali
     NRG_TRY(st);
     Sectors S;
     int rc = S.build(io->numberOfSubspace, si.data(), io->numberOfBasis, bi.data(), M.nVar, M.nOps);
-    if (rc == NRG_OK) rc = S.upload(ctx->stream);
+    if (rc == NRG_OK) rc = S.upload(ctx);
     if (rc != NRG_OK) { S.d_bi.release(); S.d_lst.release(); S.d_lstOff.release(); return rc; }
     const int nbo = io->numberOfBasis_old;
     if (io->sizeOfEigenvector < S.sizeV || nbo < 1) {
@@ -407,7 +413,7 @@ static int invmat_common(nrg_context* ctx, int32_t iteration, const nrg_invarian
     NRG_TRY(st);
     Sectors S;
     int rc = S.build(io->numberOfSubspace, si.data(), io->numberOfBasisFull, bi.data(), M.nVar, M.nOps);
-    if (rc == NRG_OK) rc = S.upload(ctx->stream);
+    if (rc == NRG_OK) rc = S.upload(ctx);
     std::vector<int> kept;
     if (rc == NRG_OK) {
         kept = kept_per_sector(S, io->numberOfBasis, bo.data());
@@ -499,7 +505,7 @@ int build_full_iter(nrg_context* ctx, const int* fsi, int r0, int r1, const int*
     }
     NRG_TRY(out->S.build(nsub, si.data(), rowpos, bi.data(), nVar, M.nOps));
     out->S.ce = ce;
-    return out->S.upload(ctx->stream);
+    return out->S.upload(ctx);
 }
 
 int full_range(const int* map, int nIter, int first, int elementNum, int N, int* r0, int* r1) {
@@ -609,7 +615,7 @@ static int spike_common(nrg_context* ctx, int32_t iteration, const nrg_spike_io*
     auto E = to_host(ctx, io->eigenvalue, (size_t)nbf, &st); NRG_TRY(st);
     Sectors S;
     int rc = S.build(io->numberOfSubspace, si.data(), nbf, bi.data(), nVar, M.nOps);
-    if (rc == NRG_OK) rc = S.upload(ctx->stream);
+    if (rc == NRG_OK) rc = S.upload(ctx);
     if (rc != NRG_OK) { S.d_bi.release(); S.d_lst.release(); S.d_lstOff.release(); return rc; }
     // eigenvalues back in sector order (the caller's array is in the truncation order)
     std::vector<double> Esec(nbf, 0.0);

@@ -214,7 +214,7 @@ int run_device(nrg_context* ctx, const nrg_run_input* in, nrg_run_output* out, c
         const int nsub = (int)(si.size() / rs);
         Sectors& S = ctx->iter_sectors[idx];
         NRG_TRY(S.build(nsub, si.data(), nb, rec.data(), nVar, M.nOps));
-        NRG_TRY(S.upload(st));
+        NRG_TRY(S.upload(ctx));
         ctx->h2d += (long long)sizeof(int) * ((long long)nb * rs + (long long)S.lst.size() + (long long)S.lstOff.size());
         DevBuf& bV = slotV(idx);
         DevBuf& bE = slotE(idx);
@@ -263,8 +263,7 @@ int run_device(nrg_context* ctx, const nrg_run_input* in, nrg_run_output* out, c
         }
         DevBuf& bEo = ctx->slot(3 + ((idx + 1) & 1));
         NRG_TRY(bEo.ensure(sizeof(double) * nbk));
-        NRG_CUDA_TRY(cudaMemcpyAsync(bEo.p, Eold_next.data(), sizeof(double) * nbk, cudaMemcpyHostToDevice, st));
-        NRG_CUDA_TRY(cudaStreamSynchronize(st));
+        NRG_TRY(h2d_async(ctx, bEo.p, Eold_next.data(), sizeof(double) * nbk));
         ctx->h2d += (long long)sizeof(double) * nbk;
         dEold = bEo.as<double>();
         dIMold = dIMnew;
@@ -303,11 +302,10 @@ int run_device(nrg_context* ctx, const nrg_run_input* in, nrg_run_output* out, c
         for (int s = 0; s < SL.nsub; ++s)
             for (int p = 0; p < RL.kept[s]; ++p)
                 if (RL.Esec[SL.start[s] + p] < 1.0e-8) {
-                    NRG_CUDA_TRY(cudaMemcpyAsync(bRdm.as<double>() + RL.rdm_off[s] + (long long)p * RL.kept[s] + p, &inv,
-                                                 sizeof(double), cudaMemcpyHostToDevice, st));
+                    NRG_TRY(h2d_async(ctx, bRdm.as<double>() + RL.rdm_off[s] + (long long)p * RL.kept[s] + p, &inv,
+                                      sizeof(double)));
                     ctx->h2d += sizeof(double);
                 }
-        NRG_CUDA_TRY(cudaStreamSynchronize(st));
         DevBuf& bTr = ctx->slot(7);
         NRG_TRY(bTr.ensure(sizeof(double) * (size_t)(nIter + 2)));
         for (int N = nIter - 1; N >= startTrancation; --N) {

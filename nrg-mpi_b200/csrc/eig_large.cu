@@ -392,8 +392,7 @@ int syev_large(nrg_context* ctx, const std::vector<SyevSector>& in, double* d_V,
     NRG_TRY(bsec.ensure(sizeof(LSec) * ns));
     NRG_TRY(bwd.ensure(sizeof(double) * (size_t)wd));
     NRG_TRY(bwi.ensure(sizeof(int) * (size_t)wi));
-    NRG_CUDA_TRY(cudaMemcpyAsync(bsec.p, secs.data(), sizeof(LSec) * ns, cudaMemcpyHostToDevice, st));
-    ctx->h2d += (long long)sizeof(LSec) * ns;
+    NRG_TRY(h2d_async(ctx, bsec.p, secs.data(), sizeof(LSec) * ns));
     const LSec* dsec = bsec.as<LSec>();
     double* wsd = bwd.as<double>();
     int* wsi = bwi.as<int>();
@@ -406,8 +405,7 @@ int syev_large(nrg_context* ctx, const std::vector<SyevSector>& in, double* d_V,
                 idx[(size_t)(jc - 1) * 4 * NB + 2 * NB + q] = q < jc ? NB + q : q - jc;     // [W V]
             }
         NRG_TRY(bidx.ensure(sizeof(int) * idx.size()));
-        NRG_CUDA_TRY(cudaMemcpyAsync(bidx.p, idx.data(), sizeof(int) * idx.size(), cudaMemcpyHostToDevice, st));
-        NRG_CUDA_TRY(cudaStreamSynchronize(st));
+        NRG_TRY(h2d_async(ctx, bidx.p, idx.data(), sizeof(int) * idx.size()));
     }
     const int* didx = bidx.as<int>();
     const size_t symv_smem = sizeof(double) * (size_t)maxn;
@@ -476,8 +474,7 @@ int syev_large(nrg_context* ctx, const std::vector<SyevSector>& in, double* d_V,
         if (ms.empty()) continue;
         const int nm = (int)ms.size();
         NRG_TRY(bmrg.ensure(sizeof(Merge) * nm));
-        NRG_CUDA_TRY(cudaMemcpyAsync(bmrg.p, ms.data(), sizeof(Merge) * nm, cudaMemcpyHostToDevice, st));
-        ctx->h2d += (long long)sizeof(Merge) * nm;
+        NRG_TRY(h2d_async(ctx, bmrg.p, ms.data(), sizeof(Merge) * nm));
         const Merge* dms = bmrg.as<Merge>();
         k_dc_prep<<<nm, 512, 0, st>>>(dsec, dms, d_V, wsd, wsi);
         for (int ph = 1; ph <= 4; ++ph)
@@ -485,25 +482,19 @@ int syev_large(nrg_context* ctx, const std::vector<SyevSector>& in, double* d_V,
         k_dc_poscols<<<blk, TPB, 0, st>>>(dsec, dms, nm, d_V, wsd, wsi);
         ctx->launches += 6;
         NRG_CUDA_TRY(cudaGetLastError());
-        // K of every merge (sizes the GEMMs)
-        std::vector<int> Ks(nm);
-        for (int i = 0; i < nm; ++i) {
-            int* mk = wsi + secs[ms[i].sec].i_off + 7LL * secs[ms[i].sec].n + ms[i].a;
-            NRG_CUDA_TRY(cudaMemcpyAsync(&Ks[i], mk, sizeof(int), cudaMemcpyDeviceToHost, st));
-        }
-        NRG_CUDA_TRY(cudaStreamSynchronize(st));
-        ctx->d2h += (long long)sizeof(int) * nm;
+        // the number K of non-deflated roots of each merge stays on the device: the
+        // GEMM is launched for K = nn and reads the true K (I[7n + a]) itself
         std::vector<GemmProblem> probs;
         for (int i = 0; i < nm; ++i) {
             const Merge& m = ms[i];
-            const int n = secs[m.sec].n, nn = m.b - m.a, K = Ks[i];
-            if (K == 0) continue;
+            const int n = secs[m.sec].n, nn = m.b - m.a;
             double* W = wsd + secs[m.sec].w_off;
             const long long sq = (long long)n * n;
             int* I = wsi + secs[m.sec].i_off;
             GemmProblem P;
             std::memset(&P, 0, sizeof(P));
-            P.M = nn; P.N = K; P.K = K; P.alpha = 1.0; P.beta = 0.0;
+            P.M = nn; P.N = nn; P.K = nn; P.alpha = 1.0; P.beta = 0.0;
+            P.dyn_nk = I + 7LL * n + m.a;
             P.A = W + m.a; P.a_si = 1; P.a_sk = n; P.a_ki = I + 5LL * n + m.a;          // Z(:, a+perm[nd[q]])
             P.B = W + sq + m.a + (long long)m.a * n; P.b_sk = 1; P.b_sj = n;           // U block
             P.C = W + 2 * sq + m.a; P.c_si = 1; P.c_sj = n; P.c_ji = I + 6LL * n + m.a;  // Qt(:, a+pos[j])

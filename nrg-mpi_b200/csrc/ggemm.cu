@@ -64,10 +64,16 @@ __global__ void __launch_bounds__(NT) k_ggemm(const GemmProblem* __restrict__ pr
         const int mid = (lo + hi + 1) >> 1;
         if (tilePrefix[mid] <= bid) lo = mid; else hi = mid - 1;
     }
-    const GemmProblem P = probs[lo];
+    GemmProblem P = probs[lo];
     const int t = bid - tilePrefix[lo];
     const int tilesN = (P.N + TN - 1) / TN;
     const int i0 = (t / tilesN) * TM, j0 = (t % tilesN) * TN;
+    if (P.dyn_nk) {
+        const int v = *P.dyn_nk;
+        P.N = min(P.N, v);
+        P.K = v;
+        if (j0 >= P.N) return;
+    }
     const bool a_kfast = (P.a_sk == 1 && P.a_si != 1);
     const bool b_kfast = (P.b_sk == 1 && P.b_sj != 1);
     const int tx = threadIdx.x % 16, ty = threadIdx.x / 16;
@@ -137,13 +143,11 @@ int launch_ggemm(nrg_context* ctx, std::vector<GemmProblem>& probs, int scratch_
     DevBuf& dq = ctx->scratch.b[scratch_slot + 1];
     NRG_TRY(dp.ensure(sizeof(GemmProblem) * np));
     NRG_TRY(dq.ensure(sizeof(int) * np));
-    NRG_CUDA_TRY(cudaMemcpyAsync(dp.p, live.data(), sizeof(GemmProblem) * np, cudaMemcpyHostToDevice, ctx->stream));
-    NRG_CUDA_TRY(cudaMemcpyAsync(dq.p, prefix.data(), sizeof(int) * np, cudaMemcpyHostToDevice, ctx->stream));
+    NRG_TRY(h2d_async(ctx, dp.p, live.data(), sizeof(GemmProblem) * np));
+    NRG_TRY(h2d_async(ctx, dq.p, prefix.data(), sizeof(int) * np));
     k_ggemm<<<(unsigned)total, NT, 0, ctx->stream>>>(dp.as<GemmProblem>(), dq.as<int>(), np);
     ctx->launches++;
     NRG_CUDA_TRY(cudaGetLastError());
-    // the problem table is host memory owned by this frame
-    NRG_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
     return NRG_OK;
 }
 

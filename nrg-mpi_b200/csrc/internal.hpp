@@ -69,7 +69,7 @@ struct Sectors {
     // device copies
     DevBuf d_bi, d_lst, d_lstOff;
     int build(int nsub, const int* si, int nb, const int* bi, int nVar, int nOps);
-    int upload(cudaStream_t st);
+    int upload(nrg_context* ctx);
     int find(const int* q) const;       // findSubspace: first sector with these qn, or -1
     int cnt(int s, int a) const { return lstOff[s * nOps + a + 1] - lstOff[s * nOps + a]; }
 };
@@ -98,6 +98,13 @@ struct nrg_context {
     // driver-owned persistent storage, reused across runs
     std::deque<nrg::DevBuf> store;
     std::vector<nrg::Sectors> iter_sectors;
+    // pinned staging ring for small host-to-device uploads (tables, index lists): a copy
+    // from pageable memory would wait for the stream to drain first
+    struct StageChunk { size_t begin, end; cudaEvent_t ev; };
+    char* stage_host = nullptr;
+    size_t stage_cap = 0, stage_head = 0;
+    std::deque<StageChunk> stage_inflight;
+    std::vector<cudaEvent_t> event_pool;
     nrg::DevBuf& slot(size_t i) {
         if (store.size() <= i) store.resize(i + 1);
         return store[i];
@@ -106,6 +113,10 @@ struct nrg_context {
 };
 
 namespace nrg {
+
+// stream-ordered upload of a small host array through the pinned staging ring (the host
+// array may be reused as soon as the call returns)
+int h2d_async(nrg_context* ctx, void* dst, const void* src, size_t bytes);
 
 // ---- grouped gather GEMM -------------------------------------------------------------
 struct GemmProblem {
@@ -117,6 +128,9 @@ struct GemmProblem {
     const double* B; long long b_sk, b_sj; const int* b_ki; const int* b_ji;
     // C(i,j) = C[ri(i)*c_si + ji(j)*c_sj]
     double* C; long long c_si, c_sj; const int* c_ri; const int* c_ji;
+    // when set, N and K are read from device memory (N = min(N, *dyn_nk), K = *dyn_nk);
+    // the launch is sized for the static N
+    const int* dyn_nk;
 };
 int launch_ggemm(nrg_context* ctx, std::vector<GemmProblem>& probs, int scratch_slot);
 

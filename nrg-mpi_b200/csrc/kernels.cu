@@ -292,16 +292,14 @@ int run_im_gather(nrg_context* ctx, const Sectors& S, std::vector<ImGatherProb>&
     DevBuf& dq = ctx->scratch.b[17];
     NRG_TRY(dp.ensure(sizeof(ImGatherProb) * np));
     NRG_TRY(dq.ensure(sizeof(long long) * np));
-    NRG_CUDA_TRY(cudaMemcpyAsync(dp.p, probs.data(), sizeof(ImGatherProb) * np, cudaMemcpyHostToDevice, ctx->stream));
-    NRG_CUDA_TRY(cudaMemcpyAsync(dq.p, prefix.data(), sizeof(long long) * np, cudaMemcpyHostToDevice, ctx->stream));
+    NRG_TRY(h2d_async(ctx, dp.p, probs.data(), sizeof(ImGatherProb) * np));
+    NRG_TRY(h2d_async(ctx, dq.p, prefix.data(), sizeof(long long) * np));
     k_im_gather<<<grid_for(total, 256), 256, 0, ctx->stream>>>(
         dp.as<ImGatherProb>(), dq.as<long long>(), np, S.d_bi.as<int>(), M.nVar + 3, M.nVar, M.nOps,
         M.nCM, S.d_lst.as<int>(), S.d_lstOff.as<int>(), M.d_imflag.as<int>(), M.d_imcoef.as<double>(),
         d_V, d_T, total);
     ctx->launches++;
     NRG_CUDA_TRY(cudaGetLastError());
-    // the host vectors must stay alive until the copies ran
-    NRG_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
     return NRG_OK;
 }
 
@@ -319,13 +317,12 @@ int run_spikes(nrg_context* ctx, std::vector<SpikeProb>& probs, const double* d_
     DevBuf& dq = ctx->scratch.b[19];
     NRG_TRY(dp.ensure(sizeof(SpikeProb) * np));
     NRG_TRY(dq.ensure(sizeof(long long) * np));
-    NRG_CUDA_TRY(cudaMemcpyAsync(dp.p, probs.data(), sizeof(SpikeProb) * np, cudaMemcpyHostToDevice, ctx->stream));
-    NRG_CUDA_TRY(cudaMemcpyAsync(dq.p, prefix.data(), sizeof(long long) * np, cudaMemcpyHostToDevice, ctx->stream));
+    NRG_TRY(h2d_async(ctx, dp.p, probs.data(), sizeof(SpikeProb) * np));
+    NRG_TRY(h2d_async(ctx, dq.p, prefix.data(), sizeof(long long) * np));
     k_spikes<<<grid_for(total, 256), 256, 0, ctx->stream>>>(dp.as<SpikeProb>(), dq.as<long long>(), np, d_work,
                                                           d_E, nbin, d_binPos, d_binNeg, d_tot, total);
     ctx->launches++;
     NRG_CUDA_TRY(cudaGetLastError());
-    NRG_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
     return NRG_OK;
 }
 

@@ -124,7 +124,7 @@ int Sectors::build(int nsub_, const int* si, int nb_, const int* bi, int nVar_, 
     return NRG_OK;
 }
 
-int Sectors::upload(cudaStream_t st) {
+int Sectors::upload(nrg_context* ctx) {
     const int rs = nVar + 3;
     std::vector<int> bi((size_t)nb * rs, 0);
     for (int i = 0; i < nb; ++i) {
@@ -135,11 +135,50 @@ int Sectors::upload(cudaStream_t st) {
     NRG_TRY(d_bi.ensure(sizeof(int) * bi.size()));
     NRG_TRY(d_lst.ensure(sizeof(int) * (lst.size() + 1)));
     NRG_TRY(d_lstOff.ensure(sizeof(int) * lstOff.size()));
-    NRG_CUDA_TRY(cudaMemcpyAsync(d_bi.p, bi.data(), sizeof(int) * bi.size(), cudaMemcpyHostToDevice, st));
-    if (!lst.empty())
-        NRG_CUDA_TRY(cudaMemcpyAsync(d_lst.p, lst.data(), sizeof(int) * lst.size(), cudaMemcpyHostToDevice, st));
-    NRG_CUDA_TRY(cudaMemcpyAsync(d_lstOff.p, lstOff.data(), sizeof(int) * lstOff.size(), cudaMemcpyHostToDevice, st));
-    NRG_CUDA_TRY(cudaStreamSynchronize(st));
+    NRG_TRY(h2d_async(ctx, d_bi.p, bi.data(), sizeof(int) * bi.size()));
+    NRG_TRY(h2d_async(ctx, d_lst.p, lst.data(), sizeof(int) * lst.size()));
+    NRG_TRY(h2d_async(ctx, d_lstOff.p, lstOff.data(), sizeof(int) * lstOff.size()));
+    return NRG_OK;
+}
+
+int h2d_async(nrg_context* ctx, void* dst, const void* src, size_t bytes) {
+    if (bytes == 0) return NRG_OK;
+    ctx->h2d += (long long)bytes;
+    const size_t need = (bytes + 255) & ~size_t(255);
+    if (!ctx->stage_host) {
+        const size_t cap = size_t(64) << 20;
+        void* p = nullptr;
+        NRG_CUDA_TRY(cudaHostAlloc(&p, cap, cudaHostAllocDefault));
+        ctx->stage_host = static_cast<char*>(p);
+        ctx->stage_cap = cap;
+        ctx->stage_head = 0;
+    }
+    if (need > ctx->stage_cap / 2) {   // large: plain copy (waits for the stream)
+        NRG_CUDA_TRY(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, ctx->stream));
+        return NRG_OK;
+    }
+    size_t begin = ctx->stage_head;
+    if (begin + need > ctx->stage_cap) begin = 0;
+    const size_t end = begin + need;
+    auto& fl = ctx->stage_inflight;
+    while (!fl.empty() && cudaEventQuery(fl.front().ev) == cudaSuccess) {
+        ctx->event_pool.push_back(fl.front().ev);
+        fl.pop_front();
+    }
+    for (auto& c : fl)
+        if (c.begin < end && begin < c.end) NRG_CUDA_TRY(cudaEventSynchronize(c.ev));
+    std::memcpy(ctx->stage_host + begin, src, bytes);
+    NRG_CUDA_TRY(cudaMemcpyAsync(dst, ctx->stage_host + begin, bytes, cudaMemcpyHostToDevice, ctx->stream));
+    cudaEvent_t ev;
+    if (!ctx->event_pool.empty()) {
+        ev = ctx->event_pool.back();
+        ctx->event_pool.pop_back();
+    } else {
+        NRG_CUDA_TRY(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+    }
+    NRG_CUDA_TRY(cudaEventRecord(ev, ctx->stream));
+    fl.push_back({begin, end, ev});
+    ctx->stage_head = end;
     return NRG_OK;
 }
 
@@ -215,10 +254,9 @@ int diag_device(nrg_context* ctx, int iteration, Sectors& S, const double* d_Eol
     NRG_TRY(bwd.ensure(sizeof(double) * (size_t)std::max(wsd, 1LL)));
     NRG_TRY(bwi.ensure(sizeof(int) * (size_t)std::max(wsi, 1LL)));
     NRG_TRY(bmin.ensure(sizeof(double) * 2));
-    NRG_CUDA_TRY(cudaMemcpyAsync(bsec.p, secs.data(), sizeof(SyevSector) * nsec, cudaMemcpyHostToDevice, ctx->stream));
-    NRG_CUDA_TRY(cudaMemcpyAsync(bcol.p, colPrefix.data(), sizeof(long long) * nsec, cudaMemcpyHostToDevice, ctx->stream));
-    NRG_CUDA_TRY(cudaMemcpyAsync(bstart.p, secStart.data(), sizeof(int) * nsec, cudaMemcpyHostToDevice, ctx->stream));
-    ctx->h2d += (long long)nsec * (sizeof(SyevSector) + sizeof(long long) + sizeof(int));
+    NRG_TRY(h2d_async(ctx, bsec.p, secs.data(), sizeof(SyevSector) * nsec));
+    NRG_TRY(h2d_async(ctx, bcol.p, colPrefix.data(), sizeof(long long) * nsec));
+    NRG_TRY(h2d_async(ctx, bstart.p, secStart.data(), sizeof(int) * nsec));
     NRG_TRY(run_assemble(ctx, iteration, S, bsec.as<SyevSector>(), bcol.as<long long>(), bstart.as<int>(),
                          nsec, cols, d_Eold, nb_old, d_IMold, d_V));
     cudaEvent_t e0 = nullptr, e1 = nullptr;
@@ -464,10 +502,9 @@ int rdm_step_device(nrg_context* ctx, const IterView& P, const IterView& C, doub
         DevBuf& bd = ctx->scratch.b[13];
         NRG_TRY(bo.ensure(sizeof(long long) * offs.size()));
         NRG_TRY(bd.ensure(sizeof(int) * dims.size()));
-        NRG_CUDA_TRY(cudaMemcpyAsync(bo.p, offs.data(), sizeof(long long) * offs.size(), cudaMemcpyHostToDevice, ctx->stream));
-        NRG_CUDA_TRY(cudaMemcpyAsync(bd.p, dims.data(), sizeof(int) * dims.size(), cudaMemcpyHostToDevice, ctx->stream));
+        NRG_TRY(h2d_async(ctx, bo.p, offs.data(), sizeof(long long) * offs.size()));
+        NRG_TRY(h2d_async(ctx, bd.p, dims.data(), sizeof(int) * dims.size()));
         NRG_TRY(run_trace(ctx, d_rdm, bo.as<long long>(), bd.as<int>(), (int)blocks.size(), d_trace_out));
-        NRG_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
     }
     return NRG_OK;
 }
