@@ -14,9 +14,13 @@
 #include "eig_common.cuh"
 #include "internal.hpp"
 
+#include <cooperative_groups.h>
+
 #include <algorithm>
 #include <cstring>
 #include <vector>
+
+namespace cg = cooperative_groups;
 
 namespace {
 
@@ -25,6 +29,7 @@ constexpr int NBB = 64;       // back-transformation panel
 constexpr int DC_LOW = 128;   // merges of up to this many rows run inside one block
 constexpr int TPB = 256;
 constexpr int CB = 32;        // columns per block in the symmetric matrix-vector product
+constexpr int kTriCL = 8;     // blocks per cluster of the one-launch tridiagonalisation
 
 struct LSec {
     long long a_off, e_off, w_off, i_off;
@@ -191,6 +196,204 @@ __global__ void __launch_bounds__(TPB) k_tri_finish(const LSec* __restrict__ sec
     finish_w(L, c, c - p, nullptr, t1, t2, red);
 }
 
+// ---------------------------------------------------------------------------------
+// tridiagonalisation by one thread-block cluster per sector
+// ---------------------------------------------------------------------------------
+// The same panel scheme (dlatrd) in one launch: the CL blocks of a cluster split the
+// indices of the sector cyclically (index i belongs to block i % CL, as a row and as a
+// column), keep the panel rows V(i, :), W(i, :) of their own indices in shared memory,
+// and meet at three cluster barriers per column:
+//   A  own rows of column k take the pending panel updates (read as row k of the own
+//      columns, the trailing matrix being stored in full); partial |x|^2 and alpha are
+//      pushed to every block's shared memory; barrier; every block forms the same beta,
+//      tau and scale, and writes the Householder vector for its own rows;
+//   B  partial y = A(:, own) v(own) over the own columns for all rows (coalesced column
+//      reads), partial W^T v, V^T v over the own rows; barrier;
+//   C  own rows sum the partial y of all blocks through distributed shared memory, form
+//      w before the alpha correction, push the partial w.v (and the next pivot row's w);
+//      barrier; the correction is applied and W written.
+// After each panel every block applies A -= V W^T + W V^T to its own columns.  Only
+// blocks of the same cluster touch each other's data, so nothing waits across clusters.
+constexpr int TT = 512;     // threads per block of the cluster kernel
+constexpr int TRW = 64;     // rows per staged chunk of the trailing update
+
+struct TriLayout {
+    int MM, PN;
+    __host__ __device__ long long doubles(int CL) const {
+        return 2LL * NB * MM + PN + 6LL * NB + 2LL * (CL + 1) + MM + 32 + 2LL * NB * TRW;
+    }
+};
+
+__device__ __forceinline__ double warp_sum(double v) {
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+template <int CL>
+__global__ void __launch_bounds__(TT, 1) k_tri_cluster(const LSec* __restrict__ secs, TriLayout lay,
+                                                      double* eigbuf, double* wsd, int* wsi) {
+    extern __shared__ double sm[];
+    cg::cluster_group cluster = cg::this_cluster();
+    const int rank = (int)cluster.block_rank();
+    const LSec sec = secs[blockIdx.x / CL];
+    LView L = lview(sec, eigbuf, wsd, wsi);
+    const int n = L.n, MM = lay.MM;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    double* VO = sm;                       // NB x MM: V(own row m, q) at q*MM + m
+    double* WO = VO + (size_t)NB * MM;     // NB x MM
+    double* ppart = WO + (size_t)NB * MM;  // partial y, by row
+    double* tpart = ppart + lay.PN;        // 2 NB: partial W^T v | V^T v
+    double* tsum = tpart + 2 * NB;         // 2 NB: totals
+    double* piv = tsum + 2 * NB;           // 2 NB: W(k, q) | V(k, q) of the pivot row
+    double* redA = piv + 2 * NB;           // CL partial |x|^2, then alpha
+    double* redC = redA + CL + 1;          // CL partial w.v, then w of the next pivot row
+    double* ys = redC + CL + 1;            // MM
+    double* red = ys + MM;                 // 32
+    double* stV = red + 32;                // NB x TRW staged rows of V (transposed)
+    double* stW = stV + NB * TRW;          // NB x TRW
+    double* Vg = L.VW;
+    double* Wg = L.VW + (size_t)NB * n;
+    double* A = L.A;
+    const int cnt = (n - rank + CL - 1) / CL;               // own indices rank + CL*m, m < cnt
+    auto first_own = [&](int i0) { return (i0 - rank + CL - 1) / CL; };   // i0 >= 0
+
+    for (int p = 0; p < n - 1; p += NB) {
+        const int last = min(p + NB - 1, n - 2);
+        for (int k = p; k <= last; ++k) {
+            const int j = k - p;
+            // ---- A ----
+            if (tid + 1 < j) {   // q < j - 1 from the panel in global memory; q = j - 1 came with barrier C
+                piv[tid] = __ldcg(Wg + k + (size_t)tid * n);
+                piv[NB + tid] = __ldcg(Vg + k + (size_t)tid * n);
+            }
+            __syncthreads();
+            const int m = first_own(k) + tid;
+            const bool act = m < cnt;
+            const int i = rank + CL * m;
+            double c = 0.0, ss = 0.0;
+            if (act) {
+                c = A[(size_t)k + (size_t)i * n];
+                double s = 0.0;
+                for (int q = 0; q < j; ++q) s += VO[q * MM + m] * piv[q] + WO[q * MM + m] * piv[NB + q];
+                c -= s;
+                if (i >= k + 2) ss = c * c;
+                if (i == k) L.D[k] = c;
+            }
+            const double ssb = block_sum(ss, red);
+            if (tid < CL) cluster.map_shared_rank(redA, tid)[rank] = ssb;
+            if (act && i == k + 1)
+                for (int r = 0; r < CL; ++r) cluster.map_shared_rank(redA, r)[CL] = c;
+            cluster.sync();
+            double xn2 = 0.0;
+            for (int r = 0; r < CL; ++r) xn2 += redA[r];
+            const double alpha = redA[CL];
+            double beta = alpha, tau = 0.0, scal = 0.0;
+            if (xn2 != 0.0) {
+                beta = -copysign(sqrt(alpha * alpha + xn2), alpha);
+                tau = (beta - alpha) / beta;
+                scal = 1.0 / (alpha - beta);
+            }
+            if (act && i >= k + 1) {
+                const double v = (i == k + 1) ? 1.0 : (xn2 == 0.0 ? 0.0 : c * scal);
+                VO[j * MM + m] = v;
+                Vg[(size_t)i + (size_t)j * n] = v;
+                if (i > k + 1) A[(size_t)i + (size_t)k * n] = v;
+            }
+            if (rank == 0 && tid == 0) { L.E[k] = beta; L.TAU[k] = tau; }
+            __syncthreads();
+            // ---- B ----
+            const int mB = first_own(k + 1);
+            const double* vj = VO + j * MM;
+            for (int r = k + 1 + tid; r < n; r += TT) {
+                double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
+                int mm = mB;
+                for (; mm + 3 < cnt; mm += 4) {
+                    const size_t l = (size_t)(rank + CL * mm);
+                    s0 = fma(A[r + l * n], vj[mm], s0);
+                    s1 = fma(A[r + (l + CL) * n], vj[mm + 1], s1);
+                    s2 = fma(A[r + (l + 2 * CL) * n], vj[mm + 2], s2);
+                    s3 = fma(A[r + (l + 3 * CL) * n], vj[mm + 3], s3);
+                }
+                for (; mm < cnt; ++mm) s0 = fma(A[r + (size_t)(rank + CL * mm) * n], vj[mm], s0);
+                ppart[r] = (s0 + s1) + (s2 + s3);
+            }
+            for (int o = warp; o < 2 * j; o += TT / 32) {
+                const double* col = (o < j) ? WO + o * MM : VO + (o - j) * MM;
+                double s = 0.0;
+                for (int mm = mB + lane; mm < cnt; mm += 32) s = fma(col[mm], vj[mm], s);
+                s = warp_sum(s);
+                if (lane == 0) tpart[o] = s;
+            }
+            cluster.sync();
+            // ---- C ----
+            for (int base = mB; base < cnt; base += TT / CL) {
+                const int mm = base + tid / CL, r = tid % CL;
+                double v = 0.0;
+                if (mm < cnt) v = cluster.map_shared_rank(ppart, r)[rank + CL * mm];
+                for (int o = CL / 2; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+                if (mm < cnt && r == 0) ys[mm] = v;
+            }
+            for (int base = 0; base < 2 * j * CL; base += TT) {
+                const int e = base + tid, o = e / CL, r = e % CL;
+                double v = 0.0;
+                if (o < 2 * j) v = cluster.map_shared_rank(tpart, r)[o];
+                for (int h = CL / 2; h > 0; h >>= 1) v += __shfl_xor_sync(0xffffffffu, v, h);
+                if (o < 2 * j && r == 0) tsum[o < j ? o : NB + (o - j)] = v;
+            }
+            __syncthreads();
+            const int mc = mB + tid;
+            double part = 0.0;
+            if (mc < cnt) {
+                double s = ys[mc];
+                for (int q = 0; q < j; ++q) s -= VO[q * MM + mc] * tsum[q] + WO[q * MM + mc] * tsum[NB + q];
+                s *= tau;
+                WO[j * MM + mc] = s;
+                part = s * vj[mc];
+                if (rank + CL * mc == k + 1)
+                    for (int r = 0; r < CL; ++r) cluster.map_shared_rank(redC, r)[CL] = s;
+            }
+            const double pb = block_sum(part, red);
+            if (tid < CL) cluster.map_shared_rank(redC, tid)[rank] = pb;
+            cluster.sync();
+            double wv = 0.0;
+            for (int r = 0; r < CL; ++r) wv += redC[r];
+            const double al = -0.5 * tau * wv;
+            if (mc < cnt) {
+                const double w = WO[j * MM + mc] + al * vj[mc];
+                WO[j * MM + mc] = w;
+                Wg[(size_t)(rank + CL * mc) + (size_t)j * n] = w;
+            }
+            if (tid == 0) { piv[j] = redC[CL] + al * 1.0; piv[NB + j] = 1.0; }
+            __syncthreads();
+        }
+        // ---- trailing update of the own columns l >= r0, rows >= r0 ----
+        const int r0 = last + 1, jc = last - p + 1;
+        cluster.sync();
+        const int mR = first_own(r0);
+        for (int ib = r0; ib < n; ib += TRW) {
+            for (int e = tid; e < jc * TRW; e += TT) {
+                const int q = e / TRW, r = e % TRW, row = ib + r;
+                stV[q * TRW + r] = row < n ? __ldcg(Vg + row + (size_t)q * n) : 0.0;
+                stW[q * TRW + r] = row < n ? __ldcg(Wg + row + (size_t)q * n) : 0.0;
+            }
+            __syncthreads();
+            const int r = tid % TRW, g = tid / TRW, row = ib + r;
+            if (row < n)
+                for (int mm = mR + g; mm < cnt; mm += TT / TRW) {
+                    const size_t l = (size_t)(rank + CL * mm);
+                    double s = 0.0;
+                    for (int q = 0; q < jc; ++q)
+                        s += stV[q * TRW + r] * WO[q * MM + mm] + stW[q * TRW + r] * VO[q * MM + mm];
+                    A[row + l * n] -= s;
+                }
+            __syncthreads();
+        }
+    }
+    if ((n - 1) % CL == rank && tid == 0) L.D[n - 1] = A[(size_t)(n - 1) + (size_t)(n - 1) * n];
+    if (rank == 0 && tid == 0) L.E[n - 1] = 0.0;
+    cluster.sync();   // no block leaves while another may still read its shared memory
+}
+
 __global__ void k_tri_end(const LSec* __restrict__ secs, double* eigbuf, double* wsd, int* wsi) {
     const LSec sec = secs[blockIdx.x];
     if (threadIdx.x != 0) return;
@@ -203,40 +406,51 @@ __global__ void k_tri_end(const LSec* __restrict__ secs, double* eigbuf, double*
 // ---------------------------------------------------------------------------------
 // divide and conquer
 // ---------------------------------------------------------------------------------
-__global__ void __launch_bounds__(512) k_dc_low(const LSec* __restrict__ secs, double* eigbuf, double* wsd,
-                                                int* wsi, int* status) {
+// leaves of the divide and conquer: one block per aligned range of DC_LOW rows of a
+// sector runs every merge inside that range (all merges up to DC_LOW rows stay inside)
+__global__ void __launch_bounds__(512) k_dc_low(const LSec* __restrict__ secs, int nsec, double* eigbuf,
+                                                double* wsd, int* wsi, int* status) {
     extern __shared__ double sm[];
-    LView L = lview(secs[blockIdx.x], eigbuf, wsd, wsi);
+    int bid = blockIdx.x, sidx = 0;
+    for (; sidx < nsec; ++sidx) {
+        const int nc = (secs[sidx].n + DC_LOW - 1) / DC_LOW;
+        if (bid < nc) break;
+        bid -= nc;
+    }
+    if (sidx >= nsec) return;
+    LView L = lview(secs[sidx], eigbuf, wsd, wsi);
     const int n = L.n, tid = threadIdx.x, T = blockDim.x;
+    const int c0 = bid * DC_LOW, c1 = min(c0 + DC_LOW, n);
     double* red = sm;
     double* gsm = sm + 32;
-    const long long sq = (long long)n * n;
-    for (long long e = tid; e < sq; e += T) L.Z[e] = 0.0;
-    __syncthreads();
-    for (int i = tid; i < n; i += T) {
-        L.Z[(size_t)i + (size_t)i * n] = 1.0;
+    // columns c0 .. c1-1 of Z start as the identity
+    const long long ne = (long long)n * (c1 - c0);
+    for (long long e = tid; e < ne; e += T) {
+        const long long col = c0 + e / n, row = e % n;
+        L.Z[row + col * n] = (row == col) ? 1.0 : 0.0;
+    }
+    // rank-one tearing at every boundary: each leaf is 1 x 1
+    for (int i = c0 + tid; i < c1; i += T) {
         double dv = L.D[i];
         if (i > 0) dv -= fabs(L.E[i - 1]);
         if (i < n - 1) dv -= fabs(L.E[i]);
-        L.S.vals[i] = dv;
+        L.D[i] = dv;
     }
     __syncthreads();
-    for (int i = tid; i < n; i += T) L.D[i] = L.S.vals[i];
-    __syncthreads();
     const int warp = tid >> 5, lane = tid & 31, nwarps = T >> 5;
-    for (int s = 1; 2 * s <= DC_LOW && s < n; s *= 2) {
+    for (int s = 1; 2 * s <= DC_LOW && c0 + s < c1; s *= 2) {
         if (2 * s <= 32) {
             WarpG wg{lane};
             int mi = 0;
-            for (int a = 0; a + s < n; a += 2 * s, ++mi) {
+            for (int a = c0; a + s < c1; a += 2 * s, ++mi) {
                 if (mi % nwarps != warp) continue;
-                dc_merge(wg, a, a + s, min(a + 2 * s, n), n, L.Z, L.D, L.E, L.S, L.U, L.Qt, red, gsm, status);
+                dc_merge(wg, a, a + s, min(a + 2 * s, c1), n, L.Z, L.D, L.E, L.S, L.U, L.Qt, red, gsm, status);
             }
             __syncthreads();
         } else {
             BlockG bg;
-            for (int a = 0; a + s < n; a += 2 * s)
-                dc_merge(bg, a, a + s, min(a + 2 * s, n), n, L.Z, L.D, L.E, L.S, L.U, L.Qt, red, gsm, status);
+            for (int a = c0; a + s < c1; a += 2 * s)
+                dc_merge(bg, a, a + s, min(a + 2 * s, c1), n, L.Z, L.D, L.E, L.S, L.U, L.Qt, red, gsm, status);
         }
     }
 }
@@ -366,6 +580,45 @@ namespace nrg {
 // ---------------------------------------------------------------------------------
 // host orchestration
 // ---------------------------------------------------------------------------------
+// One cluster of kTriCL blocks per sector when the own panel rows fit in shared memory
+// and the device can place such a cluster; *done = false leaves the multi-kernel path.
+static int tri_cluster(nrg_context* ctx, const LSec* dsec, int ns, int maxn, double* d_V, double* wsd,
+                       int* wsi, bool* done) {
+    constexpr int CL = kTriCL;
+    *done = false;
+    TriLayout lay;
+    lay.MM = (maxn + CL - 1) / CL;
+    lay.PN = maxn + (maxn & 1);
+    if (lay.MM > TT) return NRG_OK;
+    const size_t smem = sizeof(double) * (size_t)lay.doubles(CL);
+    int dev = 0, optin = 0;
+    NRG_CUDA_TRY(cudaGetDevice(&dev));
+    NRG_CUDA_TRY(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+    if (smem > (size_t)optin) return NRG_OK;
+    NRG_CUDA_TRY(cudaFuncSetAttribute(k_tri_cluster<CL>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((unsigned)(CL * ns));
+    cfg.blockDim = dim3(TT);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = ctx->stream;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeClusterDimension;
+    at[0].val.clusterDim.x = CL;
+    at[0].val.clusterDim.y = 1;
+    at[0].val.clusterDim.z = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    int clusters = 0;
+    if (cudaOccupancyMaxActiveClusters(&clusters, k_tri_cluster<CL>, &cfg) != cudaSuccess || clusters < 1) {
+        cudaGetLastError();
+        return NRG_OK;
+    }
+    NRG_CUDA_TRY(cudaLaunchKernelEx(&cfg, k_tri_cluster<CL>, dsec, lay, d_V, wsd, wsi));
+    ctx->launches++;
+    *done = true;
+    return NRG_OK;
+}
+
 int syev_large(nrg_context* ctx, const std::vector<SyevSector>& in, double* d_V, double* d_E) {
     const int ns = (int)in.size();
     if (ns == 0) return NRG_OK;
@@ -413,7 +666,9 @@ int syev_large(nrg_context* ctx, const std::vector<SyevSector>& in, double* d_V,
         NRG_CUDA_TRY(cudaFuncSetAttribute(k_tri_symv, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)symv_smem));
 
     // ---- 1. tridiagonalisation ----
-    for (int p = 0; p < maxn - 1; p += NB) {
+    bool clustered = false;
+    NRG_TRY(tri_cluster(ctx, dsec, ns, maxn, d_V, wsd, wsi, &clustered));
+    for (int p = 0; !clustered && p < maxn - 1; p += NB) {
         for (int j = 0; j < NB; ++j) {
             const int k = p + j;
             if (k > maxn - 2) break;
@@ -446,14 +701,18 @@ int syev_large(nrg_context* ctx, const std::vector<SyevSector>& in, double* d_V,
         }
         NRG_TRY(launch_ggemm(ctx, probs, 29));
     }
-    k_tri_end<<<ns, 32, 0, st>>>(dsec, d_V, wsd, wsi);
-    ctx->launches++;
+    if (!clustered) {
+        k_tri_end<<<ns, 32, 0, st>>>(dsec, d_V, wsd, wsi);
+        ctx->launches++;
+    }
 
     // ---- 2. divide and conquer ----
     {
         const int gsz = 16 * (4 * (512 / 16) + 1) + 16 * 65;
         const size_t smem = sizeof(double) * (32 + gsz);
-        k_dc_low<<<ns, 512, smem, st>>>(dsec, d_V, wsd, wsi, ctx->d_status.as<int>());
+        int nchunk = 0;
+        for (int x = 0; x < ns; ++x) nchunk += (secs[x].n + DC_LOW - 1) / DC_LOW;
+        k_dc_low<<<nchunk, 512, smem, st>>>(dsec, ns, d_V, wsd, wsi, ctx->d_status.as<int>());
         ctx->launches++;
         NRG_CUDA_TRY(cudaGetLastError());
     }
