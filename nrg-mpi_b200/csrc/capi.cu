@@ -74,6 +74,9 @@ nrg_context::~nrg_context() {
         cudaEventDestroy(c.ev);
     }
     for (cudaEvent_t e : event_pool) cudaEventDestroy(e);
+    if (ev_fork) cudaEventDestroy(ev_fork);
+    if (ev_join) cudaEventDestroy(ev_join);
+    if (aux) cudaStreamDestroy(aux);
     if (stage_host) cudaFreeHost(stage_host);
 }
 

@@ -70,23 +70,50 @@ __device__ Scratch scratch_at(double* vec, int* I, int n) {
     return S;
 }
 
+// How the O(K) sums of one secular root, one zhat entry or one rank-one eigenvector are
+// split: one thread runs the whole sum, or the 32 lanes of a warp take every 32nd term
+// and combine them with a butterfly (every lane ends with the same value).
+struct SeqLanes {
+    __device__ int first() const { return 0; }
+    __device__ int step() const { return 1; }
+    __device__ bool leader() const { return true; }
+    __device__ double sum(double v) const { return v; }
+    __device__ double prod(double v) const { return v; }
+};
+struct WarpLanes {
+    int lane;
+    __device__ int first() const { return lane; }
+    __device__ int step() const { return 32; }
+    __device__ bool leader() const { return lane == 0; }
+    __device__ double sum(double v) const {
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+        return v;
+    }
+    __device__ double prod(double v) const {
+        for (int o = 16; o > 0; o >>= 1) v *= __shfl_xor_sync(0xffffffffu, v, o);
+        return v;
+    }
+};
+
 // Root j of 1 + rho * sum_i zz_i^2 / (dd_i - lambda) = 0 (rho > 0, dd ascending, zz != 0),
 // returned as lambda = dd[org] + tau with org the pole nearer to the root, so that every
 // difference dd_i - lambda = (dd_i - dd[org]) - tau keeps full relative accuracy.
 // Iteration: the two-pole rational model of the secular function (the poles bounding
 // the root carry the near terms, Bunch-Nielsen-Sorensen), solved as a quadratic, kept
 // inside a bisection bracket; at most 100 steps.
-__device__ void secular_root(int K, const double* dd, const double* zz, double rho, int j,
+template <class R>
+__device__ void secular_root(R r, int K, const double* dd, const double* zz, double rho, int j,
                              int* org, double* tau, int* status) {
     double zsq = 0.0;
-    for (int i = 0; i < K; ++i) zsq += zz[i] * zz[i];
+    for (int i = r.first(); i < K; i += r.step()) zsq += zz[i] * zz[i];
+    zsq = r.sum(zsq);
     int o;
     double lo, hi;
     auto gval = [&](int oo, double t) {
         double s = 0.0;
         const double base = dd[oo];
-        for (int i = 0; i < K; ++i) s += zz[i] * zz[i] / ((dd[i] - base) - t);
-        return 1.0 + rho * s;
+        for (int i = r.first(); i < K; i += r.step()) s += zz[i] * zz[i] / ((dd[i] - base) - t);
+        return 1.0 + rho * r.sum(s);
     };
     if (j < K - 1) {
         const double gap = dd[j + 1] - dd[j];
@@ -101,11 +128,12 @@ __device__ void secular_root(int K, const double* dd, const double* zz, double r
     double t = 0.5 * (lo + hi);
     for (int it = 0; it < 100; ++it) {
         double psi = 0.0, dpsi = 0.0, phi = 0.0, dphi = 0.0;
-        for (int i = 0; i < K; ++i) {
+        for (int i = r.first(); i < K; i += r.step()) {
             const double del = (dd[i] - base) - t;
             const double q = zz[i] * zz[i] / del;
             if (i <= j) { psi += q; dpsi += q / del; } else { phi += q; dphi += q / del; }
         }
+        psi = r.sum(psi); dpsi = r.sum(dpsi); phi = r.sum(phi); dphi = r.sum(dphi);
         psi *= rho; dpsi *= rho; phi *= rho; dphi *= rho;
         const double f = 1.0 + psi + phi;
         if (f > 0.0) hi = t;
@@ -144,9 +172,11 @@ __device__ void secular_root(int K, const double* dd, const double* zz, double r
         t = tn;
         if (hi - lo <= 2.0 * kEps * fmax(fabs(lo), fabs(hi))) break;
     }
-    if (!(t == t)) atomicOr(status, NRG_DEV_SECULAR);
-    *org = o;
-    *tau = t;
+    if (r.leader()) {
+        if (!(t == t)) atomicOr(status, NRG_DEV_SECULAR);
+        *org = o;
+        *tau = t;
+    }
 }
 
 // dd_i - lambda_j
@@ -261,45 +291,61 @@ __device__ void merge_prep(G g, int a, int mid, int b, int n, double* Z, const d
     }
 }
 
-__device__ void merge_roots(int t, int T, int a, int mid, const double* E, Scratch S, int* status) {
+// (t, T): this thread's rank among the T threads of the merge, each taking whole items;
+// with R = WarpLanes, t and T count warps and the lanes of a warp share one item.
+template <class R = SeqLanes>
+__device__ void merge_roots(int t, int T, int a, int mid, const double* E, Scratch S, int* status,
+                            R r = R{}) {
     const int K = S.mk[a];
     const double rho = 2.0 * fabs(E[mid - 1]);
     for (int j = t; j < K; j += T)
-        secular_root(K, S.dd + a, S.zz + a, rho, j, S.org + a + j, S.tau + a + j, status);
+        secular_root(r, K, S.dd + a, S.zz + a, rho, j, S.org + a + j, S.tau + a + j, status);
 }
 
 // Gu-Eisenstat zhat
-__device__ void merge_zhat(int t, int T, int a, int mid, const double* E, Scratch S) {
+template <class R = SeqLanes>
+__device__ void merge_zhat(int t, int T, int a, int mid, const double* E, Scratch S, R r = R{}) {
     const int K = S.mk[a];
     const double rho = 2.0 * fabs(E[mid - 1]);
     const double* dd = S.dd + a;
     const int* org = S.org + a;
     const double* tau = S.tau + a;
     for (int i = t; i < K; i += T) {
-        double p = -sec_delta(dd, org, tau, i, K - 1) / rho;
-        for (int j = 0; j < i; ++j) p *= sec_delta(dd, org, tau, i, j) / (dd[i] - dd[j]);
-        for (int j = i; j < K - 1; ++j) p *= sec_delta(dd, org, tau, i, j) / (dd[i] - dd[j + 1]);
-        S.zh[a + i] = copysign(sqrt(fmax(p, 0.0)), S.zz[a + i]);
+        double p = 1.0;
+        for (int j = r.first(); j < K - 1; j += r.step())
+            p *= (j < i) ? sec_delta(dd, org, tau, i, j) / (dd[i] - dd[j])
+                         : sec_delta(dd, org, tau, i, j) / (dd[i] - dd[j + 1]);
+        p = r.prod(p) * (-sec_delta(dd, org, tau, i, K - 1) / rho);
+        if (r.leader()) S.zh[a + i] = copysign(sqrt(fmax(p, 0.0)), S.zz[a + i]);
     }
 }
 
-// eigenvectors of the rank-one problem (K x K at U[a.., a..], leading dim n) and the values
-__device__ void merge_ucols(int t, int T, int a, int b, int n, Scratch S, double* U) {
-    const int K = S.mk[a], nn = b - a;
+// eigenvectors of the rank-one problem (K x K at U[a.., a..], leading dim n)
+template <class R = SeqLanes>
+__device__ void merge_ucols(int t, int T, int a, int n, Scratch S, double* U, R r = R{}) {
+    const int K = S.mk[a];
     const double* dd = S.dd + a;
     const int* org = S.org + a;
     const double* tau = S.tau + a;
     for (int j = t; j < K; j += T) {
         double nrm = 0.0;
         double* uc = U + (size_t)a + (size_t)(a + j) * n;
-        for (int i = 0; i < K; ++i) {
+        for (int i = r.first(); i < K; i += r.step()) {
             const double u = S.zh[a + i] / sec_delta(dd, org, tau, i, j);
             uc[i] = u;
             nrm += u * u;
         }
-        nrm = 1.0 / sqrt(nrm);
-        for (int i = 0; i < K; ++i) uc[i] *= nrm;
+        nrm = 1.0 / sqrt(r.sum(nrm));
+        for (int i = r.first(); i < K; i += r.step()) uc[i] *= nrm;
     }
+}
+
+// the merged values in list order: nondeflated roots, then the deflated values
+__device__ void merge_vals(int t, int T, int a, int b, Scratch S) {
+    const int K = S.mk[a], nn = b - a;
+    const double* dd = S.dd + a;
+    const int* org = S.org + a;
+    const double* tau = S.tau + a;
     for (int e = t; e < nn; e += T)
         S.vals[a + e] = e < K ? dd[org[e]] + tau[e] : S.ds[a + S.df[a + (e - K)]];
 }
@@ -353,7 +399,8 @@ __device__ void dc_merge(G g, int a, int mid, int b, int n, double* Z, double* D
     g.sync();
     merge_zhat(t, T, a, mid, E, S);
     g.sync();
-    merge_ucols(t, T, a, b, n, S, U);
+    merge_ucols(t, T, a, n, S, U);
+    merge_vals(t, T, a, b, S);
     g.sync();
     merge_rank(t, T, a, b, S);
     g.sync();

@@ -457,14 +457,19 @@ __global__ void __launch_bounds__(512) k_dc_low(const LSec* __restrict__ secs, i
 
 struct Merge {
     int sec, a, mid, b;
-    int blk0, nblk;   // blocks of the parallel phases
+    // block ranges of the parallel phases for the three thread mappings: one thread per
+    // item (kMapItem), one warp per item (kMapWarp), one thread per few matrix entries
+    // of the nn x nn merged block (kMapWide)
+    int blk0[3], nblk[3];
 };
+constexpr int kMapItem = 0, kMapWarp = 1, kMapWide = 2;
+constexpr int kWideItems = 8;   // matrix entries per thread in kMapWide
 
-__device__ int find_merge(const Merge* ms, int nm) {
+__device__ int find_merge(const Merge* ms, int nm, int map) {
     int lo = 0, hi = nm - 1;
     while (lo < hi) {
         const int mid = (lo + hi + 1) >> 1;
-        if (ms[mid].blk0 <= (int)blockIdx.x) lo = mid; else hi = mid - 1;
+        if (ms[mid].blk0[map] <= (int)blockIdx.x) lo = mid; else hi = mid - 1;
     }
     return lo;
 }
@@ -477,20 +482,26 @@ __global__ void __launch_bounds__(512) k_dc_prep(const LSec* __restrict__ secs, 
     merge_prep(BlockG{}, m.a, m.mid, m.b, L.n, L.Z, L.D, L.E, L.S, red);
 }
 
-// phase 1 roots, 2 zhat, 3 rank-one vectors + values, 4 final order + GEMM index lists,
-// 5 deflated copies, 6 copy back
+// phase 1 roots, 2 zhat, 3 rank-one vectors + values (one warp per root / entry / column),
+// 4 final order + GEMM index lists (one thread per item), 5 deflated copies, 6 copy back
+// (one thread per few entries)
 __global__ void __launch_bounds__(TPB) k_dc_phase(const LSec* __restrict__ secs, const Merge* __restrict__ ms,
                                                   int nm, int phase, double* eigbuf, double* wsd, int* wsi,
                                                   int* status) {
-    const int mi = find_merge(ms, nm);
+    const int map = phase <= 3 ? kMapWarp : (phase == 4 ? kMapItem : kMapWide);
+    const int mi = find_merge(ms, nm, map);
     const Merge m = ms[mi];
     LView L = lview(secs[m.sec], eigbuf, wsd, wsi);
-    const int t = ((int)blockIdx.x - m.blk0) * blockDim.x + threadIdx.x;
-    const int T = m.nblk * blockDim.x;
+    const int t = ((int)blockIdx.x - m.blk0[map]) * blockDim.x + threadIdx.x;
+    const int T = m.nblk[map] * blockDim.x;
+    const WarpLanes wl{(int)(threadIdx.x & 31)};
     switch (phase) {
-        case 1: merge_roots(t, T, m.a, m.mid, L.E, L.S, status); break;
-        case 2: merge_zhat(t, T, m.a, m.mid, L.E, L.S); break;
-        case 3: merge_ucols(t, T, m.a, m.b, L.n, L.S, L.U); break;
+        case 1: merge_roots(t >> 5, T >> 5, m.a, m.mid, L.E, L.S, status, wl); break;
+        case 2: merge_zhat(t >> 5, T >> 5, m.a, m.mid, L.E, L.S, wl); break;
+        case 3:
+            merge_ucols(t >> 5, T >> 5, m.a, L.n, L.S, L.U, wl);
+            merge_vals(t, T, m.a, m.b, L.S);
+            break;
         case 4: {
             merge_rank(t, T, m.a, m.b, L.S);
             const int K = L.S.mk[m.a];
@@ -507,11 +518,11 @@ __global__ void __launch_bounds__(TPB) k_dc_phase(const LSec* __restrict__ secs,
 // scatter columns a + pos[j] of the nondeflated eigenvectors (rb reused)
 __global__ void k_dc_poscols(const LSec* __restrict__ secs, const Merge* __restrict__ ms, int nm,
                              double* eigbuf, double* wsd, int* wsi) {
-    const int mi = find_merge(ms, nm);
+    const int mi = find_merge(ms, nm, kMapItem);
     const Merge m = ms[mi];
     LView L = lview(secs[m.sec], eigbuf, wsd, wsi);
-    const int t = ((int)blockIdx.x - m.blk0) * blockDim.x + threadIdx.x;
-    const int T = m.nblk * blockDim.x;
+    const int t = ((int)blockIdx.x - m.blk0[kMapItem]) * blockDim.x + threadIdx.x;
+    const int T = m.nblk[kMapItem] * blockDim.x;
     const int K = L.S.mk[m.a];
     for (int j = t; j < K; j += T) L.S.rb[m.a + j] = m.a + L.S.pos[m.a + j];
 }
@@ -540,15 +551,19 @@ __global__ void k_bt_vpanel(const LSec* __restrict__ secs, int q, double* eigbuf
 // triangular factor T of the panel from the Gram matrix G (in Qt, b x b) and tau; T goes
 // to Qt + NBB*NBB (b x b, ld NBB)
 __global__ void k_bt_tfactor(const LSec* __restrict__ secs, int q, double* eigbuf, double* wsd, int* wsi) {
-    __shared__ double Ts[NBB * NBB];
+    extern __shared__ double tsm[];
+    double* Ts = tsm;               // NBB x NBB
+    double* G = tsm + NBB * NBB;    // the Gram matrix, staged
     const LSec sec = secs[blockIdx.x];
     const int n = sec.n, nr = n - 1, jb = q * NBB;
     if (jb >= nr) return;
     LView L = lview(sec, eigbuf, wsd, wsi);
     const int b = min(NBB, nr - jb);
-    const double* G = L.Qt;   // ld NBB
     const int p = threadIdx.x;
-    for (int e = threadIdx.x; e < NBB * NBB; e += blockDim.x) Ts[e] = 0.0;
+    for (int e = threadIdx.x; e < NBB * NBB; e += blockDim.x) {
+        Ts[e] = 0.0;
+        G[e] = L.Qt[e];
+    }
     __syncthreads();
     for (int c = 0; c < b; ++c) {
         const double tc = L.TAU[jb + c];
@@ -718,15 +733,20 @@ int syev_large(nrg_context* ctx, const std::vector<SyevSector>& in, double* d_V,
     }
     for (int s = DC_LOW; s < maxn; s *= 2) {
         std::vector<Merge> ms;
-        int blk = 0;
+        int blk[3] = {0, 0, 0};
         for (int x = 0; x < ns; ++x) {
             const int n = secs[x].n;
             for (int a = 0; a + s < n; a += 2 * s) {
                 Merge m;
                 m.sec = x; m.a = a; m.mid = a + s; m.b = std::min(a + 2 * s, n);
-                m.nblk = (m.b - m.a + TPB - 1) / TPB;
-                m.blk0 = blk;
-                blk += m.nblk;
+                const long long nn = m.b - m.a;
+                m.nblk[kMapItem] = (int)((nn + TPB - 1) / TPB);
+                m.nblk[kMapWarp] = (int)((nn * 32 + TPB - 1) / TPB);
+                m.nblk[kMapWide] = (int)((nn * nn + (long long)TPB * kWideItems - 1) / ((long long)TPB * kWideItems));
+                for (int q = 0; q < 3; ++q) {
+                    m.blk0[q] = blk[q];
+                    blk[q] += m.nblk[q];
+                }
                 ms.push_back(m);
             }
         }
@@ -737,8 +757,9 @@ int syev_large(nrg_context* ctx, const std::vector<SyevSector>& in, double* d_V,
         const Merge* dms = bmrg.as<Merge>();
         k_dc_prep<<<nm, 512, 0, st>>>(dsec, dms, d_V, wsd, wsi);
         for (int ph = 1; ph <= 4; ++ph)
-            k_dc_phase<<<blk, TPB, 0, st>>>(dsec, dms, nm, ph, d_V, wsd, wsi, ctx->d_status.as<int>());
-        k_dc_poscols<<<blk, TPB, 0, st>>>(dsec, dms, nm, d_V, wsd, wsi);
+            k_dc_phase<<<blk[ph <= 3 ? kMapWarp : kMapItem], TPB, 0, st>>>(dsec, dms, nm, ph, d_V, wsd, wsi,
+                                                                           ctx->d_status.as<int>());
+        k_dc_poscols<<<blk[kMapItem], TPB, 0, st>>>(dsec, dms, nm, d_V, wsd, wsi);
         ctx->launches += 6;
         NRG_CUDA_TRY(cudaGetLastError());
         // the number K of non-deflated roots of each merge stays on the device: the
@@ -760,14 +781,16 @@ int syev_large(nrg_context* ctx, const std::vector<SyevSector>& in, double* d_V,
             probs.push_back(P);
         }
         NRG_TRY(launch_ggemm(ctx, probs, 29));
-        k_dc_phase<<<blk, TPB, 0, st>>>(dsec, dms, nm, 5, d_V, wsd, wsi, ctx->d_status.as<int>());
-        k_dc_phase<<<blk, TPB, 0, st>>>(dsec, dms, nm, 6, d_V, wsd, wsi, ctx->d_status.as<int>());
+        k_dc_phase<<<blk[kMapWide], TPB, 0, st>>>(dsec, dms, nm, 5, d_V, wsd, wsi, ctx->d_status.as<int>());
+        k_dc_phase<<<blk[kMapWide], TPB, 0, st>>>(dsec, dms, nm, 6, d_V, wsd, wsi, ctx->d_status.as<int>());
         ctx->launches += 2;
         NRG_CUDA_TRY(cudaGetLastError());
     }
 
     // ---- 3. back-transformation, panels of NBB reflectors, last panel first ----
     const int qmax = (maxn - 2) / NBB;   // panels cover reflectors 0 .. n-2
+    const size_t tf_smem = sizeof(double) * 2 * NBB * NBB;
+    NRG_CUDA_TRY(cudaFuncSetAttribute(k_bt_tfactor, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tf_smem));
     for (int q = qmax; q >= 0; --q) {
         std::vector<int> act;
         for (int s = 0; s < ns; ++s)
@@ -799,7 +822,7 @@ int syev_large(nrg_context* ctx, const std::vector<SyevSector>& in, double* d_V,
             g1.push_back(Q);
         }
         NRG_TRY(launch_ggemm(ctx, g1, 29));
-        k_bt_tfactor<<<ns, NBB, 0, st>>>(dsec, q, d_V, wsd, wsi);
+        k_bt_tfactor<<<ns, NBB, tf_smem, st>>>(dsec, q, d_V, wsd, wsi);
         ctx->launches++;
         std::vector<GemmProblem> g2, g3;
         for (int s : act) {

@@ -105,6 +105,10 @@ struct nrg_context {
     size_t stage_cap = 0, stage_head = 0;
     std::deque<StageChunk> stage_inflight;
     std::vector<cudaEvent_t> event_pool;
+    // second stream: the one-block-per-sector eigensolver of the small sectors runs beside
+    // the large-sector pipeline (fork / join events on the caller's stream)
+    cudaStream_t aux = nullptr;
+    cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
     nrg::DevBuf& slot(size_t i) {
         if (store.size() <= i) store.resize(i + 1);
         return store[i];

@@ -265,13 +265,27 @@ int diag_device(nrg_context* ctx, int iteration, Sectors& S, const double* d_Eol
         NRG_CUDA_TRY(cudaEventCreate(&e1));
         NRG_CUDA_TRY(cudaEventRecord(e0, ctx->stream));
     }
-    // sectors of order <= 128: one block each; larger ones: the multi-kernel pipeline
+    // sectors of order <= 128: one block each, on the second stream when large sectors
+    // run beside them; larger ones: the multi-kernel pipeline on the caller's stream
+    const bool fork = nsec > nlarge && nlarge > 0;
+    if (fork) {
+        if (!ctx->aux) {
+            NRG_CUDA_TRY(cudaStreamCreateWithFlags(&ctx->aux, cudaStreamNonBlocking));
+            NRG_CUDA_TRY(cudaEventCreateWithFlags(&ctx->ev_fork, cudaEventDisableTiming));
+            NRG_CUDA_TRY(cudaEventCreateWithFlags(&ctx->ev_join, cudaEventDisableTiming));
+        }
+        NRG_CUDA_TRY(cudaEventRecord(ctx->ev_fork, ctx->stream));
+        NRG_CUDA_TRY(cudaStreamWaitEvent(ctx->aux, ctx->ev_fork, 0));
+    }
     if (nsec > nlarge) {
         NRG_TRY(launch_syev(bsec.as<SyevSector>() + nlarge, nsec - nlarge, max_n, d_V, d_E, bwd.as<double>(),
-                            bwi.as<int>(), ctx->d_status.as<int>(), ctx->stream));
+                            bwi.as<int>(), ctx->d_status.as<int>(), fork ? ctx->aux : ctx->stream));
         ctx->launches++;
     }
-    NRG_TRY(syev_large(ctx, large, d_V, d_E));
+    if (fork) NRG_CUDA_TRY(cudaEventRecord(ctx->ev_join, ctx->aux));
+    const int rl = syev_large(ctx, large, d_V, d_E);
+    if (fork) NRG_CUDA_TRY(cudaStreamWaitEvent(ctx->stream, ctx->ev_join, 0));
+    NRG_TRY(rl);
     if (ctx->profiling) {
         NRG_CUDA_TRY(cudaEventRecord(e1, ctx->stream));
         NRG_CUDA_TRY(cudaEventSynchronize(e1));
