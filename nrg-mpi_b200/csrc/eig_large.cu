@@ -199,34 +199,51 @@ __global__ void __launch_bounds__(TPB) k_tri_finish(const LSec* __restrict__ sec
 // ---------------------------------------------------------------------------------
 // tridiagonalisation by one thread-block cluster per sector
 // ---------------------------------------------------------------------------------
-// The same panel scheme (dlatrd) in one launch: the CL blocks of a cluster split the
+// The same panel scheme (dlatrd) in one launch.  The CL blocks of a cluster split the
 // indices of the sector cyclically (index i belongs to block i % CL, as a row and as a
-// column), keep the panel rows V(i, :), W(i, :) of their own indices in shared memory,
-// and meet at three cluster barriers per column:
-//   A  own rows of column k take the pending panel updates (read as row k of the own
-//      columns, the trailing matrix being stored in full); partial |x|^2 and alpha are
-//      pushed to every block's shared memory; barrier; every block forms the same beta,
-//      tau and scale, and writes the Householder vector for its own rows;
-//   B  partial y = A(:, own) v(own) over the own columns for all rows (coalesced column
-//      reads), partial W^T v, V^T v over the own rows; barrier;
-//   C  own rows sum the partial y of all blocks through distributed shared memory, form
-//      w before the alpha correction, push the partial w.v (and the next pivot row's w);
-//      barrier; the correction is applied and W written.
-// After each panel every block applies A -= V W^T + W V^T to its own columns.  Only
-// blocks of the same cluster touch each other's data, so nothing waits across clusters.
+// column) and keep the panel rows V(i, :), W(i, :) of their own indices in shared
+// memory.  Two cluster barriers per column k:
+//   A  each block updates its rows of column k with the pending panel reflectors (read
+//      as row k of its own columns: the trailing matrix is stored in full) and stores
+//      them into the shared memory of every block of the cluster, with its partial
+//      |x|^2; barrier 1; every block now holds the whole column and forms the same
+//      beta, tau and Householder vector v;
+//   B  y(l) = A(:, l) . v for the own columns l (coalesced column reads), partial
+//      W^T v, V^T v over the own rows and partial y . v are stored into every block;
+//      the owner of row k+1 also sends its panel row and y(k+1); barrier 2; every block
+//      forms t1 = W^T v, t2 = V^T v, w.v = tau (y.v - 2 t1.t2) and
+//      w = tau (y - V t1 - W t2) - (tau/2)(w.v) v for its own rows, and the pivot row's
+//      w for the next column.
+// After each panel every block applies A -= V W^T + W V^T to its own columns.  Blocks of
+// different clusters never touch each other's data.
 constexpr int TT = 512;     // threads per block of the cluster kernel
 constexpr int TRW = 64;     // rows per staged chunk of the trailing update
+constexpr int P2W = 2 * NB + 2;   // partials per block: W^T v | V^T v | y.v
 
 struct TriLayout {
     int MM, PN;
     __host__ __device__ long long doubles(int CL) const {
-        return 2LL * NB * MM + PN + 6LL * NB + 2LL * (CL + 1) + MM + 32 + 2LL * NB * TRW;
+        return 2LL * NB * MM + PN + MM + (long long)CL * P2W + CL + 2 + 2LL * NB + 2LL * NB + P2W + 32 +
+               2LL * NB * TRW;
     }
 };
 
 __device__ __forceinline__ double warp_sum(double v) {
     for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
     return v;
+}
+
+// w = tau (y - sum_q (V_q t1_q + W_q t2_q)) + al v with explicit roundings, so that every
+// block computes the pivot row's w bit-identically to its owner
+__device__ __forceinline__ double w_entry(double y, const double* Vr, const double* Wr, int stride,
+                                          const double* t1, const double* t2, int j, double tau,
+                                          double al, double v) {
+    double s = y;
+    for (int q = 0; q < j; ++q) {
+        s = fma(-Vr[q * stride], t1[q], s);
+        s = fma(-Wr[q * stride], t2[q], s);
+    }
+    return fma(al, v, __dmul_rn(tau, s));
 }
 
 template <int CL>
@@ -239,34 +256,31 @@ __global__ void __launch_bounds__(TT, 1) k_tri_cluster(const LSec* __restrict__ 
     LView L = lview(sec, eigbuf, wsd, wsi);
     const int n = L.n, MM = lay.MM;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    constexpr int NW = TT / 32;
     double* VO = sm;                       // NB x MM: V(own row m, q) at q*MM + m
     double* WO = VO + (size_t)NB * MM;     // NB x MM
-    double* ppart = WO + (size_t)NB * MM;  // partial y, by row
-    double* tpart = ppart + lay.PN;        // 2 NB: partial W^T v | V^T v
-    double* tsum = tpart + 2 * NB;         // 2 NB: totals
-    double* piv = tsum + 2 * NB;           // 2 NB: W(k, q) | V(k, q) of the pivot row
-    double* redA = piv + 2 * NB;           // CL partial |x|^2, then alpha
-    double* redC = redA + CL + 1;          // CL partial w.v, then w of the next pivot row
-    double* ys = redC + CL + 1;            // MM
-    double* red = ys + MM;                 // 32
+    double* cv = WO + (size_t)NB * MM;     // column k (rows > k), then v, by row
+    double* ys = cv + lay.PN;              // y of the own columns
+    double* P2 = ys + MM;                  // CL x P2W partials, by source block
+    double* redA = P2 + CL * P2W;          // CL partial |x|^2
+    double* Y1 = redA + CL;                // y(k+1) from its owner (2 slots)
+    double* pivn = Y1 + 2;                 // 2 NB: V(k+1, q) | W(k+1, q) from its owner
+    double* piv = pivn + 2 * NB;           // 2 NB: W(k, q) | V(k, q) of the current pivot row
+    double* tsum = piv + 2 * NB;           // t1 | t2 | y.v
+    double* red = tsum + P2W;              // 32
     double* stV = red + 32;                // NB x TRW staged rows of V (transposed)
     double* stW = stV + NB * TRW;          // NB x TRW
     double* Vg = L.VW;
     double* Wg = L.VW + (size_t)NB * n;
     double* A = L.A;
-    const int cnt = (n - rank + CL - 1) / CL;               // own indices rank + CL*m, m < cnt
-    auto first_own = [&](int i0) { return (i0 - rank + CL - 1) / CL; };   // i0 >= 0
+    const int cnt = (n - rank + CL - 1) / CL;                           // own indices rank + CL*m
+    auto first_own = [&](int i0) { return (i0 - rank + CL - 1) / CL; };  // i0 >= 0
 
     for (int p = 0; p < n - 1; p += NB) {
         const int last = min(p + NB - 1, n - 2);
         for (int k = p; k <= last; ++k) {
             const int j = k - p;
-            // ---- A ----
-            if (tid + 1 < j) {   // q < j - 1 from the panel in global memory; q = j - 1 came with barrier C
-                piv[tid] = __ldcg(Wg + k + (size_t)tid * n);
-                piv[NB + tid] = __ldcg(Vg + k + (size_t)tid * n);
-            }
-            __syncthreads();
+            // ---- A: own rows of column k, broadcast ----
             const int m = first_own(k) + tid;
             const bool act = m < cnt;
             const int i = rank + CL * m;
@@ -276,94 +290,103 @@ __global__ void __launch_bounds__(TT, 1) k_tri_cluster(const LSec* __restrict__ 
                 double s = 0.0;
                 for (int q = 0; q < j; ++q) s += VO[q * MM + m] * piv[q] + WO[q * MM + m] * piv[NB + q];
                 c -= s;
-                if (i >= k + 2) ss = c * c;
                 if (i == k) L.D[k] = c;
+                if (i >= k + 2) ss = c * c;
+                if (i >= k + 1)
+                    for (int r = 0; r < CL; ++r) cluster.map_shared_rank(cv, r)[i] = c;
             }
             const double ssb = block_sum(ss, red);
             if (tid < CL) cluster.map_shared_rank(redA, tid)[rank] = ssb;
-            if (act && i == k + 1)
-                for (int r = 0; r < CL; ++r) cluster.map_shared_rank(redA, r)[CL] = c;
             cluster.sync();
             double xn2 = 0.0;
             for (int r = 0; r < CL; ++r) xn2 += redA[r];
-            const double alpha = redA[CL];
+            const double alpha = cv[k + 1];
             double beta = alpha, tau = 0.0, scal = 0.0;
             if (xn2 != 0.0) {
                 beta = -copysign(sqrt(alpha * alpha + xn2), alpha);
                 tau = (beta - alpha) / beta;
                 scal = 1.0 / (alpha - beta);
             }
+            for (int r = k + 1 + tid; r < n; r += TT)
+                cv[r] = (r == k + 1) ? 1.0 : (xn2 == 0.0 ? 0.0 : cv[r] * scal);
+            __syncthreads();
             if (act && i >= k + 1) {
-                const double v = (i == k + 1) ? 1.0 : (xn2 == 0.0 ? 0.0 : c * scal);
+                const double v = cv[i];
                 VO[j * MM + m] = v;
                 Vg[(size_t)i + (size_t)j * n] = v;
                 if (i > k + 1) A[(size_t)i + (size_t)k * n] = v;
             }
             if (rank == 0 && tid == 0) { L.E[k] = beta; L.TAU[k] = tau; }
-            __syncthreads();
-            // ---- B ----
+            // ---- B: y of the own columns, partials ----
             const int mB = first_own(k + 1);
-            const double* vj = VO + j * MM;
-            for (int r = k + 1 + tid; r < n; r += TT) {
+            for (int mm = mB + warp; mm < cnt; mm += NW) {
+                const double* col = A + (size_t)(rank + CL * mm) * n;
                 double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
-                int mm = mB;
-                for (; mm + 3 < cnt; mm += 4) {
-                    const size_t l = (size_t)(rank + CL * mm);
-                    s0 = fma(A[r + l * n], vj[mm], s0);
-                    s1 = fma(A[r + (l + CL) * n], vj[mm + 1], s1);
-                    s2 = fma(A[r + (l + 2 * CL) * n], vj[mm + 2], s2);
-                    s3 = fma(A[r + (l + 3 * CL) * n], vj[mm + 3], s3);
+                int r = k + 1 + lane;
+                for (; r + 96 < n; r += 128) {
+                    s0 = fma(col[r], cv[r], s0);
+                    s1 = fma(col[r + 32], cv[r + 32], s1);
+                    s2 = fma(col[r + 64], cv[r + 64], s2);
+                    s3 = fma(col[r + 96], cv[r + 96], s3);
                 }
-                for (; mm < cnt; ++mm) s0 = fma(A[r + (size_t)(rank + CL * mm) * n], vj[mm], s0);
-                ppart[r] = (s0 + s1) + (s2 + s3);
+                for (; r < n; r += 32) s0 = fma(col[r], cv[r], s0);
+                const double y = warp_sum((s0 + s1) + (s2 + s3));
+                if (lane == 0) ys[mm] = y;
             }
-            for (int o = warp; o < 2 * j; o += TT / 32) {
-                const double* col = (o < j) ? WO + o * MM : VO + (o - j) * MM;
+            __syncthreads();   // ys and VO(:, j) complete
+            const double* vj = VO + j * MM;
+            for (int o = warp; o < 2 * j; o += NW) {
+                const double* colp = (o < j) ? WO + o * MM : VO + (o - j) * MM;
                 double s = 0.0;
-                for (int mm = mB + lane; mm < cnt; mm += 32) s = fma(col[mm], vj[mm], s);
+                for (int mm = mB + lane; mm < cnt; mm += 32) s = fma(colp[mm], vj[mm], s);
                 s = warp_sum(s);
-                if (lane == 0) tpart[o] = s;
+                if (lane < CL) cluster.map_shared_rank(P2, lane)[rank * P2W + (o < j ? o : NB + (o - j))] = s;
             }
+            const int mc = mB + tid;
+            const bool own_c = mc < cnt;
+            double yvp = own_c ? ys[mc] * vj[mc] : 0.0;
+            const bool pivot_owner = (rank == (k + 1) % CL);
+            if (pivot_owner && k + 1 <= last) {   // the next column's pivot row
+                for (int e = tid; e < 2 * j * CL; e += TT) {
+                    const int q = e / CL, r = e % CL;
+                    const double val = q < j ? VO[q * MM + mB] : WO[(q - j) * MM + mB];
+                    cluster.map_shared_rank(pivn, r)[q < j ? q : NB + (q - j)] = val;
+                }
+                if (tid < CL) cluster.map_shared_rank(Y1, tid)[0] = ys[mB];
+            }
+            yvp = block_sum(yvp, red);
+            if (tid < CL) cluster.map_shared_rank(P2, tid)[rank * P2W + 2 * NB] = yvp;
             cluster.sync();
-            // ---- C ----
-            for (int base = mB; base < cnt; base += TT / CL) {
-                const int mm = base + tid / CL, r = tid % CL;
-                double v = 0.0;
-                if (mm < cnt) v = cluster.map_shared_rank(ppart, r)[rank + CL * mm];
-                for (int o = CL / 2; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-                if (mm < cnt && r == 0) ys[mm] = v;
-            }
-            for (int base = 0; base < 2 * j * CL; base += TT) {
-                const int e = base + tid, o = e / CL, r = e % CL;
-                double v = 0.0;
-                if (o < 2 * j) v = cluster.map_shared_rank(tpart, r)[o];
-                for (int h = CL / 2; h > 0; h >>= 1) v += __shfl_xor_sync(0xffffffffu, v, h);
-                if (o < 2 * j && r == 0) tsum[o < j ? o : NB + (o - j)] = v;
+            // ---- C: totals, w of the own rows and of the next pivot row ----
+            if (tid < 2 * j) {
+                const int o = tid < j ? tid : NB + (tid - j);
+                double s = 0.0;
+                for (int r = 0; r < CL; ++r) s += P2[r * P2W + o];
+                tsum[o] = s;
+            } else if (tid == TT - 1) {
+                double s = 0.0;
+                for (int r = 0; r < CL; ++r) s += P2[r * P2W + 2 * NB];
+                tsum[2 * NB] = s;
             }
             __syncthreads();
-            const int mc = mB + tid;
-            double part = 0.0;
-            if (mc < cnt) {
-                double s = ys[mc];
-                for (int q = 0; q < j; ++q) s -= VO[q * MM + mc] * tsum[q] + WO[q * MM + mc] * tsum[NB + q];
-                s *= tau;
-                WO[j * MM + mc] = s;
-                part = s * vj[mc];
-                if (rank + CL * mc == k + 1)
-                    for (int r = 0; r < CL; ++r) cluster.map_shared_rank(redC, r)[CL] = s;
-            }
-            const double pb = block_sum(part, red);
-            if (tid < CL) cluster.map_shared_rank(redC, tid)[rank] = pb;
-            cluster.sync();
-            double wv = 0.0;
-            for (int r = 0; r < CL; ++r) wv += redC[r];
+            double t12 = 0.0;
+            for (int q = 0; q < j; ++q) t12 = fma(tsum[q], tsum[NB + q], t12);
+            const double wv = tau * (tsum[2 * NB] - 2.0 * t12);
             const double al = -0.5 * tau * wv;
-            if (mc < cnt) {
-                const double w = WO[j * MM + mc] + al * vj[mc];
+            if (own_c) {
+                const double w = w_entry(ys[mc], VO + mc, WO + mc, MM, tsum, tsum + NB, j, tau, al, vj[mc]);
                 WO[j * MM + mc] = w;
                 Wg[(size_t)(rank + CL * mc) + (size_t)j * n] = w;
             }
-            if (tid == 0) { piv[j] = redC[CL] + al * 1.0; piv[NB + j] = 1.0; }
+            if (k + 1 <= last) {
+                if (tid < j) {
+                    piv[tid] = pivn[NB + tid];        // W(k+1, q)
+                    piv[NB + tid] = pivn[tid];        // V(k+1, q)
+                } else if (tid == TT - 1) {
+                    piv[j] = w_entry(Y1[0], pivn, pivn + NB, 1, tsum, tsum + NB, j, tau, al, 1.0);
+                    piv[NB + j] = 1.0;
+                }
+            }
             __syncthreads();
         }
         // ---- trailing update of the own columns l >= r0, rows >= r0 ----
@@ -391,7 +414,7 @@ __global__ void __launch_bounds__(TT, 1) k_tri_cluster(const LSec* __restrict__ 
     }
     if ((n - 1) % CL == rank && tid == 0) L.D[n - 1] = A[(size_t)(n - 1) + (size_t)(n - 1) * n];
     if (rank == 0 && tid == 0) L.E[n - 1] = 0.0;
-    cluster.sync();   // no block leaves while another may still read its shared memory
+    cluster.sync();   // no block leaves while another may still write its shared memory
 }
 
 __global__ void k_tri_end(const LSec* __restrict__ secs, double* eigbuf, double* wsd, int* wsi) {

@@ -153,9 +153,14 @@ def test_spikes_per_iteration(driven):
     assert worst <= BIN_TOL, worst
 
 
-def test_large_sector_diagonalization(ctx_factory):
-    # N_keep = 512: sectors of order up to ~200 take the multi-kernel eigensolver
-    inp = small_siam(n_keep=512, n_iterations=9)
+@pytest.mark.parametrize("case", ["nkeep512", "bench_sizes"])
+def test_large_sector_diagonalization(ctx_factory, case):
+    # N_keep = 512: sectors of order up to ~200; the benchmark workload (N_keep = 2048)
+    # reaches order ~700 by its sixth diagonalization: both take the large-sector eigensolver
+    if case == "nkeep512":
+        inp = small_siam(n_keep=512, n_iterations=9)
+    else:
+        inp = model.config(2, n_iterations=7)
     d = write_case(inp)
     st = O.State(d)
     ctx = ctx_factory(model.read_inputs(d))
@@ -174,7 +179,7 @@ def test_large_sector_diagonalization(ctx_factory):
             worst_v = max(worst_v, subspace_err(Bg, Bo, st.eigenvalue[s0:s0 + dd]))
             largest = max(largest, dd)
         O.postprocess(st, it)
-    assert largest > 128
+    assert largest > (600 if case == "bench_sizes" else 128)
     assert worst_e <= EIG_TOL, worst_e
     assert worst_v <= VEC_TOL, worst_v
 
