@@ -261,11 +261,17 @@ def main():
     # end to end through the drop-in entry points with host arrays
     e2e = None
     if not args.no_e2e:
-        ctx.reset_stats()
-        t0 = time.perf_counter()
+        # one untimed run pins the host module arrays (first-use allocation), then K timed
         r2 = ctx.run(spectrum=True, host_drop_in=True)
         torch.cuda.synchronize(dev)
-        dt = time.perf_counter() - t0
+        ctx.reset_stats()
+        if dist is not None:
+            dist.barrier()
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            r2 = ctx.run(spectrum=True, host_drop_in=True)
+        torch.cuda.synchronize(dev)
+        dt = (time.perf_counter() - t0) / args.steps
         st2 = ctx.stats()
         if dist is not None:
             t = torch.tensor([dt], device=dev, dtype=torch.float64)
@@ -274,8 +280,10 @@ def main():
         same = float(max(np.max(np.abs(r2["binPos"][:, 1] - res["binPos"][:, 1])),
                          np.max(np.abs(r2["binNeg"][:, 1] - res["binNeg"][:, 1]))))
         e2e = {"value": n_it * world / dt, "unit": "iterations/s",
-               "h2d_bytes_per_step": int(st2["h2d_bytes"]), "d2h_bytes_per_step": int(st2["d2h_bytes"]),
-               "path": "drop-in entry points with host arrays (Fortran caller's data flow)",
+               "h2d_bytes_per_step": int(st2["h2d_bytes"]) // args.steps,
+               "d2h_bytes_per_step": int(st2["d2h_bytes"]) // args.steps,
+               "path": "drop-in entry points with host arrays (Fortran caller's data flow; module "
+                       "arrays in pinned host memory, allocated in one untimed warm-up run)",
                "max_bin_diff_vs_device_resident": same}
     if rank == 0:
         clocks = clk.summary()

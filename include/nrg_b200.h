@@ -26,6 +26,7 @@
 #ifndef NRG_B200_H
 #define NRG_B200_H
 
+#include <stddef.h>
 #include <stdint.h>
 
 #if defined(__GNUC__)
@@ -234,6 +235,16 @@ NRG_API int nrg_spike_cfs(nrg_context* ctx, int32_t iteration, const nrg_spike_i
 #define NRG_NOALLOC_MAX_ORDER 128
 NRG_API int nrg_block_eigh_noalloc(const double* H, int32_t n, double* eigenvalues,
                                    double* eigenvectors, void* stream);
+
+/* ---- pinned host memory for module arrays ------------------------------------------
+ * No counterpart in the reference (its module arrays are Fortran allocatables).  Page-
+ * locked host memory for the arrays that cross the boundary on every iteration
+ * (eigenvector, invariant_matrix, invariant_matrix_spectrum): copies between it and the
+ * device run at full link speed without an extra staging copy.  Optional: every entry
+ * point accepts arrays from any allocator.  A Fortran caller maps the block with
+ * c_f_pointer.  nrg_host_free(NULL) is a no-op. */
+NRG_API int nrg_host_alloc(size_t bytes, void** out);
+NRG_API int nrg_host_free(void* p);
 
 /* ---- whole run: main.F90:142-252 with everything device resident ---------------------
  * Replays the reference's driver (forward NRG sweep, backward reduced density matrices,

@@ -62,6 +62,7 @@ void nrg_set_error_message(const char* fmt, ...) {
 
 nrg_context::~nrg_context() {
     for (auto& b : store) b.release();
+    for (auto& b : host_store) b.release();
     for (auto& b : scratch.b) b.release();
     for (auto& s : iter_sectors) { s.d_bi.release(); s.d_lst.release(); s.d_lstOff.release(); }
     d_status.release();
@@ -238,6 +239,25 @@ int nrg_context_reset_stats(nrg_context* ctx) {
     ctx->syev_flops = 0.0;
     ctx->h2d = 0;
     ctx->d2h = 0;
+    return NRG_OK;
+}
+
+int nrg_host_alloc(size_t bytes, void** out) {
+    if (!out) return NRG_ERR_INVALID;
+    *out = nullptr;
+    if (bytes == 0) return NRG_OK;
+    cudaError_t e = cudaHostAlloc(out, bytes, cudaHostAllocPortable);
+    if (e != cudaSuccess) {
+        *out = nullptr;
+        nrg_set_error_message("cudaHostAlloc(%zu) failed: %s", bytes, cudaGetErrorString(e));
+        return NRG_ERR_NOMEM;
+    }
+    return NRG_OK;
+}
+
+int nrg_host_free(void* p) {
+    if (!p) return NRG_OK;
+    NRG_CUDA_TRY(cudaFreeHost(p));
     return NRG_OK;
 }
 
@@ -659,7 +679,27 @@ static int spike_common(nrg_context* ctx, int32_t iteration, const nrg_spike_io*
     if (rc == NRG_OK) rc = stage_in(ctx, io->eigenvector, (size_t)S.sizeV, kSlotIO + 9, &dV);
     if (rc == NRG_OK) rc = stage_in(ctx, io->invariant_matrix_spectrum,
                                     (size_t)io->numberOfBasis_old * io->numberOfBasis_old * M.nMat, kSlotIO + 10, &dIMS);
-    if (rc == NRG_OK && cfs) rc = stage_in(ctx, io->reducedDensityMatrix, (size_t)io->sizeOfReducedDensity, kSlotIO + 11, &dR);
+    if (rc == NRG_OK && cfs) {
+        // only the density blocks of this iteration's sectors are staged (one contiguous
+        // range of the caller's array); offsets become relative to the range
+        long long lo = -1, hi = -1;
+        for (int s = 0; s < S.nsub; ++s) {
+            if (it.rdm_off[s] < 0) continue;
+            const long long a = it.rdm_off[s], b = a + (long long)it.kept[s] * it.kept[s];
+            lo = lo < 0 ? a : std::min(lo, a);
+            hi = std::max(hi, b);
+        }
+        if (lo >= 0) {
+            if (hi > (long long)io->sizeOfReducedDensity) {
+                nrg_set_error_message("reduced density blocks beyond sizeOfReducedDensity");
+                rc = NRG_ERR_INVALID;
+            } else {
+                rc = stage_in(ctx, io->reducedDensityMatrix + lo, (size_t)(hi - lo), kSlotIO + 11, &dR);
+                for (int s = 0; s < S.nsub; ++s)
+                    if (it.rdm_off[s] >= 0) it.rdm_off[s] -= lo;
+            }
+        }
+    }
     DevBuf& bE = ctx->slot(kSlotIO + 12);
     if (rc == NRG_OK) rc = bE.ensure(sizeof(double) * std::max(nbf, 1));
     if (rc == NRG_OK && cudaMemcpyAsync(bE.p, Esec.data(), sizeof(double) * nbf, cudaMemcpyHostToDevice, ctx->stream) != cudaSuccess) rc = NRG_ERR_CUDA;

@@ -379,10 +379,18 @@ int run_device(nrg_context* ctx, const nrg_run_input* in, nrg_run_output* out, c
 // host drop-in data flow: the Fortran caller's view
 // ------------------------------------------------------------------------------------
 struct HostRestore {
-    std::vector<double> E, V, ims;
+    std::vector<double> E;
+    const double* V = nullptr;     // eigenvector blocks of the iteration (a pinned module array)
+    const double* ims = nullptr;   // invariant matrices for the spectrum (pinned)
+    long long nV = 0;
     std::vector<int> bo, bi, si;
     int nb = 0, nb_full = 0, nsub = 0;
 };
+
+// host slots of the host-array driver: the module arrays a Fortran caller keeps
+// allocated (invariant matrices ping-pong, one eigenvector and one spectrum-matrix array
+// per iteration for the restore stock, the full stock of eigenvectors)
+constexpr size_t kHostIM = 0, kHostFV = 2, kHostV = 16, kHostIMS = 16 + 4096;
 
 int run_drop_in(nrg_context* ctx, const nrg_run_input* in, nrg_run_output* out, cudaEvent_t* ev) {
     const Model& M = ctx->model;
@@ -390,17 +398,33 @@ int run_drop_in(nrg_context* ctx, const nrg_run_input* in, nrg_run_output* out, 
     const int nIt = nIter - first + 1;
     const bool spectrum = in->spectrum && M.nMat > 0;
     int nb_old = in->numberOfBasis;
+    if (nIt > (int)(kHostIMS - kHostV)) return NRG_ERR_TOO_LARGE;
     std::vector<int> bo(in->basis_output, in->basis_output + (size_t)nb_old * rs);
     std::vector<double> E(in->eigenvalue, in->eigenvalue + nb_old);
-    std::vector<double> IM(in->invariant_matrix, in->invariant_matrix + (size_t)nb_old * nb_old * M.nCM);
-    std::vector<double> IMS;
-    if (spectrum) IMS.assign(in->invariant_matrix_spectrum, in->invariant_matrix_spectrum + (size_t)nb_old * nb_old * M.nMat);
+    double* IM = nullptr;
+    const double* IMS = nullptr;
+    {
+        const size_t nim = (size_t)nb_old * nb_old * M.nCM;
+        HostBuf& h = ctx->hslot(kHostIM);
+        NRG_TRY(h.ensure(sizeof(double) * std::max<size_t>(nim, 1)));
+        std::memcpy(h.p, in->invariant_matrix, sizeof(double) * nim);
+        IM = h.as<double>();
+        if (spectrum) {
+            const size_t nis = (size_t)nb_old * nb_old * M.nMat;
+            HostBuf& g = ctx->hslot(kHostIMS + nIt);
+            NRG_TRY(g.ensure(sizeof(double) * std::max<size_t>(nis, 1)));
+            std::memcpy(g.p, in->invariant_matrix_spectrum, sizeof(double) * nis);
+            IMS = g.as<double>();
+        }
+    }
     std::vector<HostRestore> rest(nIt);
     int startTrancation = nIter + 1;
     bool flag_truncation = false;
     // the "full" stock (postprocess.F90:221-374)
     std::vector<int> fsi, fbi, fbo, map(nIter + 2, 0);
-    std::vector<double> fE, fV;
+    std::vector<double> fE;
+    HostBuf& hFV = ctx->hslot(kHostFV);
+    long long nFV = 0;
     long long pointFBI = 1, pointFBO = 1, pointFS = 1, pointFV = 1, sizeRDM = 0;
     for (int it = first; it <= nIter; ++it) {
         const int idx = it - first;
@@ -410,13 +434,16 @@ int run_drop_in(nrg_context* ctx, const nrg_run_input* in, nrg_run_output* out, 
         const int nsub = (int)(si.size() / rs);
         long long sizeV = 0;
         for (int s = 0; s < nsub; ++s) sizeV += (long long)si[(size_t)s * rs + nVar] * si[(size_t)s * rs + nVar];
-        std::vector<double> Enew(nb), Vnew((size_t)sizeV);
+        std::vector<double> Enew(nb);
+        HostBuf& hV = ctx->hslot(kHostV + idx);
+        NRG_TRY(hV.ensure(sizeof(double) * (size_t)std::max(sizeV, 1LL)));
+        double* Vnew = hV.as<double>();
         std::vector<int> bo_sec((size_t)nb * rs);
         double gse = 0.0;
         nrg_diagonalization_io dio;
         dio.numberOfSubspace = nsub; dio.subspaceInfo = si.data(); dio.numberOfBasis = nb;
         dio.basis_input = bi.data(); dio.numberOfBasis_old = nb_old; dio.eigenvalue_old = E.data();
-        dio.invariant_matrix = IM.data(); dio.eigenvalue = Enew.data(); dio.eigenvector = Vnew.data();
+        dio.invariant_matrix = IM; dio.eigenvalue = Enew.data(); dio.eigenvector = Vnew;
         dio.sizeOfEigenvector = sizeV; dio.basis_output = bo_sec.data(); dio.groundStateEnergy = &gse;
         NRG_TRY(nrg_diagonalization(ctx, it, &dio));
         if (out && out->groundStateEnergy) out->groundStateEnergy[idx] = gse;
@@ -431,25 +458,31 @@ int run_drop_in(nrg_context* ctx, const nrg_run_input* in, nrg_run_output* out, 
         }
         if (out && out->kept) out->kept[idx] = nbk;
         if (out && out->numberOfBasisFull) out->numberOfBasisFull[idx] = nb;
-        std::vector<double> IMn, IMSn;
+        double* IMn = nullptr;
+        double* IMSn = nullptr;
         if (it < nIter) {
-            IMn.assign((size_t)nbk * nbk * M.nCM, 0.0);
+            HostBuf& h = ctx->hslot(kHostIM + ((idx + 1) & 1));
+            NRG_TRY(h.ensure(sizeof(double) * std::max<size_t>((size_t)nbk * nbk * M.nCM, 1)));
+            IMn = h.as<double>();
             nrg_invariant_matrix_io iio;
             iio.numberOfSubspace = nsub; iio.subspaceInfo = si.data(); iio.numberOfBasisFull = nb;
             iio.basis_input = bi.data(); iio.numberOfBasis = nbk; iio.basis_output = bo_re.data();
-            iio.eigenvector = Vnew.data(); iio.sizeOfEigenvector = sizeV; iio.numberOfBasis_old = nb_old;
-            iio.invariant_matrix_spectrum_old = nullptr; iio.invariant_matrix = IMn.data();
+            iio.eigenvector = Vnew; iio.sizeOfEigenvector = sizeV; iio.numberOfBasis_old = nb_old;
+            iio.invariant_matrix_spectrum_old = nullptr; iio.invariant_matrix = IMn;
             NRG_TRY(nrg_invariant_matrix_dgemm(ctx, it, &iio));
             if (spectrum) {
-                IMSn.assign((size_t)nbk * nbk * M.nMat, 0.0);
-                iio.invariant_matrix_spectrum_old = IMS.data();
-                iio.invariant_matrix = IMSn.data();
+                HostBuf& g = ctx->hslot(kHostIMS + idx);
+                NRG_TRY(g.ensure(sizeof(double) * std::max<size_t>((size_t)nbk * nbk * M.nMat, 1)));
+                IMSn = g.as<double>();
+                iio.invariant_matrix_spectrum_old = IMS;
+                iio.invariant_matrix = IMSn;
                 NRG_TRY(nrg_invariant_matrix_for_spectrum_dgemm(ctx, it, &iio));
             }
         }
         if (spectrum) {
             HostRestore& R = rest[idx];
-            R.E = E_re; R.V = Vnew; R.bo = bo_re; R.bi = bi; R.si = si; R.nb = nbk; R.nb_full = nb; R.nsub = nsub;
+            R.E = E_re; R.V = Vnew; R.nV = sizeV; R.bo = bo_re; R.bi = bi; R.si = si; R.nb = nbk; R.nb_full = nb;
+            R.nsub = nsub;
             if (it < nIter) R.ims = IMSn;
             if (it >= startTrancation) {
                 map[it + 1] = (int)pointFS;
@@ -475,7 +508,9 @@ int run_drop_in(nrg_context* ctx, const nrg_run_input* in, nrg_run_output* out, 
                     fsi.push_back(0);
                     sizeRDM += (long long)k * k;
                     const long long c0 = (long long)si[(size_t)s * rs + nVar + 1] - 1;
-                    fV.insert(fV.end(), Vnew.begin() + c0, Vnew.begin() + c0 + (long long)d * k);
+                    NRG_TRY(hFV.ensure(sizeof(double) * (size_t)(nFV + (long long)d * k), true));
+                    std::memcpy(hFV.as<double>() + nFV, Vnew + c0, sizeof(double) * (size_t)d * k);
+                    nFV += (long long)d * k;
                     pointFV += (long long)d * k;
                     ++pointFS;
                 }
@@ -485,8 +520,8 @@ int run_drop_in(nrg_context* ctx, const nrg_run_input* in, nrg_run_output* out, 
         }
         E.swap(E_re);
         bo.swap(bo_re);
-        IM.swap(IMn);
-        IMS.swap(IMSn);
+        IM = IMn;
+        IMS = IMSn;
         nb_old = nbk;
     }
     NRG_CUDA_TRY(cudaEventRecord(ev[1], ctx->stream));
@@ -516,7 +551,7 @@ int run_drop_in(nrg_context* ctx, const nrg_run_input* in, nrg_run_output* out, 
         rio.elementNumFullSubspace = elementNum; rio.fullSubspaceInfo = fsi.data();
         rio.fullBasisInput = fbi.data(); rio.numFullBasisInput = (int64_t)(fbi.size() / rs);
         rio.fullBasisOutput = fbo.data(); rio.numFullBasisOutput = (int64_t)(fbo.size() / rs);
-        rio.fullEigenvector = fV.data(); rio.numFullEigenvector = (int64_t)fV.size();
+        rio.fullEigenvector = hFV.as<double>(); rio.numFullEigenvector = (int64_t)nFV;
         rio.reducedDensityMatrix = rdm.data(); rio.sizeOfReducedDensity = (int64_t)rdm.size();
         rio.pointReducedDensity = &point;
         std::vector<double> tr(std::max(nIter - startTrancation, 1));
@@ -536,8 +571,8 @@ int run_drop_in(nrg_context* ctx, const nrg_run_input* in, nrg_run_output* out, 
             std::memset(&sio, 0, sizeof(sio));
             sio.numberOfSubspace = R.nsub; sio.subspaceInfo = R.si.data(); sio.numberOfBasis = R.nb;
             sio.numberOfBasisFull = R.nb_full; sio.basis_input = R.bi.data(); sio.basis_output = R.bo.data();
-            sio.eigenvalue = R.E.data(); sio.eigenvector = R.V.data(); sio.sizeOfEigenvector = (int64_t)R.V.size();
-            sio.numberOfBasis_old = P.nb; sio.invariant_matrix_spectrum = P.ims.data();
+            sio.eigenvalue = R.E.data(); sio.eigenvector = R.V; sio.sizeOfEigenvector = (int64_t)R.nV;
+            sio.numberOfBasis_old = P.nb; sio.invariant_matrix_spectrum = P.ims;
             sio.fullSubspaceInfo = fsi.data(); sio.mapFullSubspaceInfo = map.data();
             sio.elementNumFullSubspace = elementNum; sio.reducedDensityMatrix = rdm.data();
             sio.sizeOfReducedDensity = (int64_t)rdm.size(); sio.numberOfBin = nbin;

@@ -17,6 +17,7 @@
 #include <cooperative_groups.h>
 
 #include <algorithm>
+#include <cstdlib>
 #include <cstring>
 #include <vector>
 
@@ -319,19 +320,35 @@ __global__ void __launch_bounds__(TT, 1) k_tri_cluster(const LSec* __restrict__ 
             if (rank == 0 && tid == 0) { L.E[k] = beta; L.TAU[k] = tau; }
             // ---- B: y of the own columns, partials ----
             const int mB = first_own(k + 1);
-            for (int mm = mB + warp; mm < cnt; mm += NW) {
-                const double* col = A + (size_t)(rank + CL * mm) * n;
-                double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
-                int r = k + 1 + lane;
-                for (; r + 96 < n; r += 128) {
-                    s0 = fma(col[r], cv[r], s0);
-                    s1 = fma(col[r + 32], cv[r + 32], s1);
-                    s2 = fma(col[r + 64], cv[r + 64], s2);
-                    s3 = fma(col[r + 96], cv[r + 96], s3);
+            // a warp takes two columns at a time, 8 rows per lane per batch: 16 independent
+            // loads in flight per lane keep the L2 stream busy
+            for (int c0 = mB + 2 * warp; c0 < cnt; c0 += 2 * NW) {
+                const bool two = c0 + 1 < cnt;
+                const double* ca = A + (size_t)(rank + CL * c0) * n;
+                const double* cb = two ? ca + (size_t)CL * n : ca;
+                double sa = 0.0, sb = 0.0;
+                for (int r0 = k + 1; r0 < n; r0 += 256) {
+                    double xa[8], xb[8], xv[8];
+#pragma unroll
+                    for (int u = 0; u < 8; ++u) {
+                        const int r = r0 + lane + 32 * u;
+                        const bool in = r < n;
+                        xa[u] = in ? ca[r] : 0.0;
+                        xb[u] = in ? cb[r] : 0.0;
+                        xv[u] = in ? cv[r] : 0.0;
+                    }
+#pragma unroll
+                    for (int u = 0; u < 8; ++u) {
+                        sa = fma(xa[u], xv[u], sa);
+                        sb = fma(xb[u], xv[u], sb);
+                    }
                 }
-                for (; r < n; r += 32) s0 = fma(col[r], cv[r], s0);
-                const double y = warp_sum((s0 + s1) + (s2 + s3));
-                if (lane == 0) ys[mm] = y;
+                sa = warp_sum(sa);
+                sb = warp_sum(sb);
+                if (lane == 0) {
+                    ys[c0] = sa;
+                    if (two) ys[c0 + 1] = sb;
+                }
             }
             __syncthreads();   // ys and VO(:, j) complete
             const double* vj = VO + j * MM;
@@ -620,9 +637,9 @@ namespace nrg {
 // ---------------------------------------------------------------------------------
 // One cluster of kTriCL blocks per sector when the own panel rows fit in shared memory
 // and the device can place such a cluster; *done = false leaves the multi-kernel path.
-static int tri_cluster(nrg_context* ctx, const LSec* dsec, int ns, int maxn, double* d_V, double* wsd,
-                       int* wsi, bool* done) {
-    constexpr int CL = kTriCL;
+template <int CL>
+static int tri_cluster_cl(nrg_context* ctx, const LSec* dsec, int ns, int maxn, double* d_V, double* wsd,
+                          int* wsi, bool* done) {
     *done = false;
     TriLayout lay;
     lay.MM = (maxn + CL - 1) / CL;
@@ -634,6 +651,7 @@ static int tri_cluster(nrg_context* ctx, const LSec* dsec, int ns, int maxn, dou
     NRG_CUDA_TRY(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
     if (smem > (size_t)optin) return NRG_OK;
     NRG_CUDA_TRY(cudaFuncSetAttribute(k_tri_cluster<CL>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    if (CL > 8) NRG_CUDA_TRY(cudaFuncSetAttribute(k_tri_cluster<CL>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3((unsigned)(CL * ns));
     cfg.blockDim = dim3(TT);
@@ -655,6 +673,24 @@ static int tri_cluster(nrg_context* ctx, const LSec* dsec, int ns, int maxn, dou
     ctx->launches++;
     *done = true;
     return NRG_OK;
+}
+
+// Cluster size of the one-launch tridiagonalisation: 8 blocks per sector by default; the
+// environment variable NRG_TRI_CLUSTER selects 4, 8 or 16, or 0 for the multi-kernel path.
+static int tri_cluster(nrg_context* ctx, const LSec* dsec, int ns, int maxn, double* d_V, double* wsd,
+                       int* wsi, bool* done) {
+    static const int cl = [] {
+        const char* e = getenv("NRG_TRI_CLUSTER");
+        const int v = e ? atoi(e) : kTriCL;
+        return (v == 0 || v == 4 || v == 8 || v == 16) ? v : kTriCL;
+    }();
+    *done = false;
+    switch (cl) {
+        case 4: return tri_cluster_cl<4>(ctx, dsec, ns, maxn, d_V, wsd, wsi, done);
+        case 8: return tri_cluster_cl<8>(ctx, dsec, ns, maxn, d_V, wsd, wsi, done);
+        case 16: return tri_cluster_cl<16>(ctx, dsec, ns, maxn, d_V, wsd, wsi, done);
+        default: return NRG_OK;
+    }
 }
 
 int syev_large(nrg_context* ctx, const std::vector<SyevSector>& in, double* d_V, double* d_E) {

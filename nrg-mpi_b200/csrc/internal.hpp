@@ -21,6 +21,16 @@ struct DevBuf {
     template <class T> T* as() const { return static_cast<T*>(p); }
 };
 
+// grow-only pinned host buffer (module arrays of the host-array driver); keep = true
+// preserves the contents when the buffer grows
+struct HostBuf {
+    void* p = nullptr;
+    size_t bytes = 0;
+    int ensure(size_t want, bool keep = false);
+    void release();
+    template <class T> T* as() const { return static_cast<T*>(p); }
+};
+
 // ------------------------------------------------------------------------------------
 // model tables (host copies + device copies + derived lookup tables)
 // ------------------------------------------------------------------------------------
@@ -112,6 +122,12 @@ struct nrg_context {
     nrg::DevBuf& slot(size_t i) {
         if (store.size() <= i) store.resize(i + 1);
         return store[i];
+    }
+    // pinned host arrays of the host-array driver, reused across runs
+    std::deque<nrg::HostBuf> host_store;
+    nrg::HostBuf& hslot(size_t i) {
+        if (host_store.size() <= i) host_store.resize(i + 1);
+        return host_store[i];
     }
     ~nrg_context();
 };

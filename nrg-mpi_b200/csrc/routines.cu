@@ -34,6 +34,29 @@ void DevBuf::release() {
     bytes = 0;
 }
 
+int HostBuf::ensure(size_t want, bool keep) {
+    if (want <= bytes && p) return NRG_OK;
+    size_t sz = want < 4096 ? 4096 : want;
+    if (keep) sz = std::max(sz, bytes + bytes / 2);
+    sz = (sz + 4095) & ~size_t(4095);
+    void* q = nullptr;
+    cudaError_t e = cudaHostAlloc(&q, sz, cudaHostAllocPortable);
+    if (e != cudaSuccess) {
+        nrg_set_error_message("cudaHostAlloc(%zu) failed: %s", sz, cudaGetErrorString(e));
+        return NRG_ERR_NOMEM;
+    }
+    if (keep && p && bytes) std::memcpy(q, p, bytes);
+    if (p) cudaFreeHost(p);
+    p = q;
+    bytes = sz;
+    return NRG_OK;
+}
+void HostBuf::release() {
+    if (p) cudaFreeHost(p);
+    p = nullptr;
+    bytes = 0;
+}
+
 // ------------------------------------------------------------------------------------
 // Model
 // ------------------------------------------------------------------------------------

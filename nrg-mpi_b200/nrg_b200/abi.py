@@ -44,6 +44,7 @@ EXPORTS = [
     "nrg_invariant_matrix_for_spectrum_dgemm", "nrg_reduced_density_matrix",
     "nrg_spike_zero_temperature", "nrg_spike_cfs", "nrg_run", "nrg_context_get_stats",
     "nrg_context_reset_stats", "nrg_context_set_profiling", "nrg_block_eigh_noalloc",
+    "nrg_host_alloc", "nrg_host_free",
 ]
 
 
