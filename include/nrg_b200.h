@@ -110,6 +110,10 @@ typedef struct nrg_stats {
     double syev_flops;       /* algorithmic flops of those launches                   */
     int64_t h2d_bytes;       /* host-to-device bytes moved by the library             */
     int64_t d2h_bytes;       /* device-to-host bytes moved by the library             */
+    int64_t tri_launches;    /* cluster tridiagonalisation launches (profiling on)    */
+    double tri_ms;           /* their summed device time                              */
+    double tri_flops;        /* their algorithmic flops, sum over sectors of 4/3 n^3  */
+    double tri_bytes;        /* their algorithmic matrix reads, sum of 8 n^3 / 3      */
 } nrg_stats;
 NRG_API int nrg_context_get_stats(const nrg_context* ctx, nrg_stats* out);
 NRG_API int nrg_context_reset_stats(nrg_context* ctx);

@@ -229,6 +229,10 @@ int nrg_context_get_stats(const nrg_context* ctx, nrg_stats* out) {
     out->syev_flops = ctx->syev_flops;
     out->h2d_bytes = ctx->h2d;
     out->d2h_bytes = ctx->d2h;
+    out->tri_launches = ctx->tri_launches;
+    out->tri_ms = ctx->tri_ms;
+    out->tri_flops = ctx->tri_flops;
+    out->tri_bytes = ctx->tri_bytes;
     return NRG_OK;
 }
 
@@ -239,6 +243,8 @@ int nrg_context_reset_stats(nrg_context* ctx) {
     ctx->syev_flops = 0.0;
     ctx->h2d = 0;
     ctx->d2h = 0;
+    ctx->tri_launches = 0;
+    ctx->tri_ms = ctx->tri_flops = ctx->tri_bytes = 0.0;
     return NRG_OK;
 }
 

@@ -37,11 +37,16 @@ struct LSec {
     int n, pad;
 };
 
-long long lws_doubles(long long n) { return 3 * n * n + 2LL * NB * n + n + 16 * n + 64; }
+// workspace per sector: Z, U, Qt (n x n each), the panel V | W (n x 2 NB), y, the D&C
+// vectors (16 n + 64), then the back-transformation's T factors and explicit reflector
+// panels ((n + NBB)^2 bounds both)
+long long lws_doubles(long long n) {
+    return 3 * n * n + 2LL * NB * n + n + 16 * n + 64 + (n + NBB) * (n + NBB);
+}
 long long lws_ints(long long n) { return 12 * n + 64; }
 
 struct LView {
-    double *A, *Z, *U, *Qt, *VW, *y, *vec, *D, *E, *TAU;
+    double *A, *Z, *U, *Qt, *VW, *y, *vec, *D, *E, *TAU, *R;
     int* I;
     Scratch S;
     int n;
@@ -62,6 +67,7 @@ __device__ LView lview(const LSec& s, double* eigbuf, double* wsd, int* wsi) {
     v.D = v.vec;
     v.E = v.vec + n;
     v.TAU = v.vec + 2 * n;
+    v.R = v.vec + 16 * n + 64;
     v.I = wsi + s.i_off;
     v.S = scratch_at(v.vec, v.I, s.n);
     return v;
@@ -618,6 +624,176 @@ __global__ void k_bt_tfactor(const LSec* __restrict__ secs, int q, double* eigbu
     for (int e = threadIdx.x; e < NBB * NBB; e += blockDim.x) L.Qt[NBB * NBB + e] = Ts[e];
 }
 
+// ---- back-transformation in one pass per column block --------------------------------
+// Panel q holds reflectors jb = 64 q .. jb + b - 1 (rows r0 = jb + 1 .. n - 1).  In R:
+// the triangular factors T_q (NBB x NBB each) first, then the explicit panels
+// V_q (mr x NBB, column-major, zero beyond b).
+__device__ __forceinline__ long long bt_panel_off(int n, int q) {
+    const long long npan = (n - 2) / NBB + 1;
+    const long long before = (long long)q * (n - 1) - (long long)NBB * q * (q - 1) / 2;   // sum of mr
+    return npan * NBB * NBB + (long long)NBB * before;
+}
+
+// explicit V_q, its Gram matrix and T_q (dlarft, forward, columnwise) for every panel of
+// every sector at once: one block per (panel, sector)
+__global__ void __launch_bounds__(256) k_bt_prep(const LSec* __restrict__ secs, double* eigbuf, double* wsd,
+                                                 int* wsi) {
+    extern __shared__ double bsm[];
+    double* Vs = bsm;                  // chunk of the panel, Vs[c * 65 + r]
+    double* G = Vs + NBB * 65;         // NBB x NBB, column-major
+    double* Ts = G + NBB * NBB;        // NBB x NBB, column-major
+    const LSec sec = secs[blockIdx.y];
+    const int n = sec.n, nr = n - 1, q = blockIdx.x, jb = q * NBB;
+    if (jb >= nr) return;
+    LView L = lview(sec, eigbuf, wsd, wsi);
+    const int b = min(NBB, nr - jb), r0 = jb + 1, mr = n - r0;
+    double* Rp = L.R + bt_panel_off(n, q);
+    double* Tq = L.R + (size_t)q * NBB * NBB;
+    const int tid = threadIdx.x, ti = tid & 15, tj = tid >> 4;
+    double g[4][4];
+#pragma unroll
+    for (int a = 0; a < 4; ++a)
+#pragma unroll
+        for (int c = 0; c < 4; ++c) g[a][c] = 0.0;
+    for (int i0 = 0; i0 < mr; i0 += 64) {
+        const int rows = min(64, mr - i0);
+        for (int e = tid; e < 64 * NBB; e += 256) {
+            const int r = e & 63, c = e >> 6;
+            const int row = r0 + i0 + r, k = jb + c;
+            double v = 0.0;
+            if (r < rows && c < b) v = (row == k + 1) ? 1.0 : (row > k + 1 ? L.A[(size_t)row + (size_t)k * n] : 0.0);
+            Vs[c * 65 + r] = v;
+            if (r < rows) Rp[(size_t)(i0 + r) + (size_t)c * mr] = v;
+        }
+        __syncthreads();
+        for (int r = 0; r < rows; ++r) {
+            double x[4], y[4];
+#pragma unroll
+            for (int a = 0; a < 4; ++a) {
+                x[a] = Vs[(ti * 4 + a) * 65 + r];
+                y[a] = Vs[(tj * 4 + a) * 65 + r];
+            }
+#pragma unroll
+            for (int a = 0; a < 4; ++a)
+#pragma unroll
+                for (int c = 0; c < 4; ++c) g[a][c] = fma(x[a], y[c], g[a][c]);
+        }
+        __syncthreads();
+    }
+#pragma unroll
+    for (int a = 0; a < 4; ++a)
+#pragma unroll
+        for (int c = 0; c < 4; ++c) G[(ti * 4 + a) + (tj * 4 + c) * NBB] = g[a][c];
+    for (int e = tid; e < NBB * NBB; e += 256) Ts[e] = 0.0;
+    __syncthreads();
+    for (int c = 0; c < b; ++c) {
+        const double tc = L.TAU[jb + c];
+        double acc = 0.0;
+        if (tid < c)
+            for (int qq = tid; qq < c; ++qq) acc += Ts[tid + qq * NBB] * (-tc * G[qq + c * NBB]);
+        __syncthreads();
+        if (tid < c) Ts[tid + c * NBB] = acc;
+        if (tid == 0) Ts[c + c * NBB] = tc;
+        __syncthreads();
+    }
+    for (int e = tid; e < NBB * NBB; e += 256) Tq[e] = Ts[e];
+}
+
+// Z(:, c0 .. c0+CBK-1) <- H_0 ... H_{n-2} Z(:, ...) panel by panel (last panel first), the
+// column block resident in shared memory; the result and the eigenvalues go to the output
+template <int CBK>
+__global__ void __launch_bounds__(256, 1) k_bt_apply(const LSec* __restrict__ secs, int nsec, double* eigbuf,
+                                                     double* evals, double* wsd, int* wsi) {
+    constexpr int JPT = CBK / 4;       // columns per thread
+    extern __shared__ double asm_[];
+    int bid = blockIdx.x, s = 0;
+    for (; s < nsec; ++s) {
+        const int nbk = (secs[s].n + CBK - 1) / CBK;
+        if (bid < nbk) break;
+        bid -= nbk;
+    }
+    if (s >= nsec) return;
+    const LSec sec = secs[s];
+    LView L = lview(sec, eigbuf, wsd, wsi);
+    const int n = L.n, nr = n - 1, c0 = bid * CBK, nc = min(CBK, n - c0);
+    double* Zs = asm_;                      // Zs[j * n + row]
+    double* Vs = Zs + (size_t)n * CBK;      // Vs[c * 65 + r]
+    double* Ws = Vs + NBB * 65;             // Ws[c * CBK + j]
+    double* W2 = Ws + NBB * CBK;
+    double* Ts = W2 + NBB * CBK;            // T column-major
+    const int tid = threadIdx.x, cl = tid & 63, jg = tid >> 6;
+    for (int j = 0; j < CBK; ++j)
+        for (int row = tid; row < n; row += 256)
+            Zs[(size_t)j * n + row] = j < nc ? L.Z[(size_t)row + (size_t)(c0 + j) * n] : 0.0;
+    const int qmax = (n - 2) / NBB;
+    for (int q = qmax; q >= 0; --q) {
+        const int jb = q * NBB, b = min(NBB, nr - jb), r0 = jb + 1, mr = n - r0;
+        (void)b;
+        const double* Rp = L.R + bt_panel_off(n, q);
+        const double* Tq = L.R + (size_t)q * NBB * NBB;
+        for (int e = tid; e < NBB * NBB; e += 256) Ts[e] = Tq[e];
+        // W = V^T Z(r0:, :)
+        double acc[JPT];
+#pragma unroll
+        for (int u = 0; u < JPT; ++u) acc[u] = 0.0;
+        for (int i0 = 0; i0 < mr; i0 += 64) {
+            const int rows = min(64, mr - i0);
+            __syncthreads();
+            for (int e = tid; e < 64 * NBB; e += 256) {
+                const int r = e & 63, c = e >> 6;
+                Vs[c * 65 + r] = r < rows ? Rp[(size_t)(i0 + r) + (size_t)c * mr] : 0.0;
+            }
+            __syncthreads();
+            const double* zr = Zs + r0 + i0;
+            for (int r = 0; r < rows; ++r) {
+                const double v = Vs[cl * 65 + r];
+#pragma unroll
+                for (int u = 0; u < JPT; ++u) acc[u] = fma(v, zr[(size_t)(jg * JPT + u) * n + r], acc[u]);
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < JPT; ++u) Ws[cl * CBK + jg * JPT + u] = acc[u];
+        __syncthreads();
+        // W2 = T W (T upper triangular)
+#pragma unroll
+        for (int u = 0; u < JPT; ++u) acc[u] = 0.0;
+        for (int c2 = cl; c2 < NBB; ++c2) {
+            const double t = Ts[cl + c2 * NBB];
+#pragma unroll
+            for (int u = 0; u < JPT; ++u) acc[u] = fma(t, Ws[c2 * CBK + jg * JPT + u], acc[u]);
+        }
+#pragma unroll
+        for (int u = 0; u < JPT; ++u) W2[cl * CBK + jg * JPT + u] = acc[u];
+        // Z(r0:, :) -= V W2
+        for (int i0 = 0; i0 < mr; i0 += 64) {
+            const int rows = min(64, mr - i0);
+            __syncthreads();
+            for (int e = tid; e < 64 * NBB; e += 256) {
+                const int r = e & 63, c = e >> 6;
+                Vs[c * 65 + r] = r < rows ? Rp[(size_t)(i0 + r) + (size_t)c * mr] : 0.0;
+            }
+            __syncthreads();
+            if (cl < rows) {
+#pragma unroll
+                for (int u = 0; u < JPT; ++u) acc[u] = 0.0;
+                for (int c = 0; c < NBB; ++c) {
+                    const double v = Vs[c * 65 + cl];
+#pragma unroll
+                    for (int u = 0; u < JPT; ++u) acc[u] = fma(v, W2[c * CBK + jg * JPT + u], acc[u]);
+                }
+                double* zr = Zs + r0 + i0 + cl;
+#pragma unroll
+                for (int u = 0; u < JPT; ++u) zr[(size_t)(jg * JPT + u) * n] -= acc[u];
+            }
+        }
+        __syncthreads();
+    }
+    for (int j = 0; j < nc; ++j)
+        for (int row = tid; row < n; row += 256)
+            L.A[(size_t)row + (size_t)(c0 + j) * n] = Zs[(size_t)j * n + row];
+    for (int j = tid; j < nc; j += 256) evals[sec.e_off + c0 + j] = L.D[c0 + j];
+}
+
 __global__ void k_large_out(const LSec* __restrict__ secs, double* eigbuf, double* evals, double* wsd, int* wsi) {
     const LSec sec = secs[blockIdx.y];
     LView L = lview(sec, eigbuf, wsd, wsi);
@@ -741,7 +917,30 @@ int syev_large(nrg_context* ctx, const std::vector<SyevSector>& in, double* d_V,
 
     // ---- 1. tridiagonalisation ----
     bool clustered = false;
+    cudaEvent_t te[2] = {nullptr, nullptr};
+    if (ctx->profiling) {
+        NRG_CUDA_TRY(cudaEventCreate(&te[0]));
+        NRG_CUDA_TRY(cudaEventCreate(&te[1]));
+        NRG_CUDA_TRY(cudaEventRecord(te[0], st));
+    }
     NRG_TRY(tri_cluster(ctx, dsec, ns, maxn, d_V, wsd, wsi, &clustered));
+    if (ctx->profiling) {
+        NRG_CUDA_TRY(cudaEventRecord(te[1], st));
+        NRG_CUDA_TRY(cudaEventSynchronize(te[1]));
+        float ms = 0.f;
+        NRG_CUDA_TRY(cudaEventElapsedTime(&ms, te[0], te[1]));
+        cudaEventDestroy(te[0]);
+        cudaEventDestroy(te[1]);
+        if (clustered) {
+            ctx->tri_launches++;
+            ctx->tri_ms += ms;
+            for (int x = 0; x < ns; ++x) {
+                const double n = secs[x].n;
+                ctx->tri_flops += 4.0 / 3.0 * n * n * n;
+                ctx->tri_bytes += 8.0 * n * n * n / 3.0;
+            }
+        }
+    }
     for (int p = 0; !clustered && p < maxn - 1; p += NB) {
         for (int j = 0; j < NB; ++j) {
             const int k = p + j;
@@ -846,7 +1045,37 @@ int syev_large(nrg_context* ctx, const std::vector<SyevSector>& in, double* d_V,
         NRG_CUDA_TRY(cudaGetLastError());
     }
 
-    // ---- 3. back-transformation, panels of NBB reflectors, last panel first ----
+    // ---- 3. back-transformation ----
+    // one pass per column block with the block resident in shared memory, when it fits
+    {
+        int dev = 0, optin = 0;
+        NRG_CUDA_TRY(cudaGetDevice(&dev));
+        NRG_CUDA_TRY(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+        auto apply_smem = [&](int c) {
+            return sizeof(double) * ((size_t)maxn * c + NBB * 65 + 2 * NBB * c + NBB * NBB);
+        };
+        const size_t prep_smem = sizeof(double) * (NBB * 65 + 2 * NBB * NBB);
+        const int cbk = apply_smem(16) <= (size_t)optin ? 16 : (apply_smem(8) <= (size_t)optin ? 8 : 0);
+        if (cbk > 0) {
+            const int npan = (maxn - 2) / NBB + 1;
+            NRG_CUDA_TRY(cudaFuncSetAttribute(k_bt_prep, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)prep_smem));
+            k_bt_prep<<<dim3(npan, ns), 256, prep_smem, st>>>(dsec, d_V, wsd, wsi);
+            int nblk = 0;
+            for (int x = 0; x < ns; ++x) nblk += (secs[x].n + cbk - 1) / cbk;
+            const size_t sm = apply_smem(cbk);
+            if (cbk == 16) {
+                NRG_CUDA_TRY(cudaFuncSetAttribute(k_bt_apply<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+                k_bt_apply<16><<<nblk, 256, sm, st>>>(dsec, ns, d_V, d_E, wsd, wsi);
+            } else {
+                NRG_CUDA_TRY(cudaFuncSetAttribute(k_bt_apply<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+                k_bt_apply<8><<<nblk, 256, sm, st>>>(dsec, ns, d_V, d_E, wsd, wsi);
+            }
+            ctx->launches += 2;
+            NRG_CUDA_TRY(cudaGetLastError());
+            return NRG_OK;
+        }
+    }
+    // otherwise panels of NBB reflectors on grouped GEMMs, last panel first
     const int qmax = (maxn - 2) / NBB;   // panels cover reflectors 0 .. n-2
     const size_t tf_smem = sizeof(double) * 2 * NBB * NBB;
     NRG_CUDA_TRY(cudaFuncSetAttribute(k_bt_tfactor, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tf_smem));

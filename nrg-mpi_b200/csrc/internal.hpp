@@ -105,6 +105,8 @@ struct nrg_context {
     long long syev_launches = 0;
     double syev_ms = 0.0, syev_flops = 0.0;
     long long h2d = 0, d2h = 0;
+    long long tri_launches = 0;
+    double tri_ms = 0.0, tri_flops = 0.0, tri_bytes = 0.0;
     // driver-owned persistent storage, reused across runs
     std::deque<nrg::DevBuf> store;
     std::vector<nrg::Sectors> iter_sectors;

@@ -140,7 +140,9 @@ class RunOutput(ctypes.Structure):
 
 class Stats(ctypes.Structure):
     _fields_ = [("launches", c_int64), ("syev_launches", c_int64), ("syev_ms", c_double),
-                ("syev_flops", c_double), ("h2d_bytes", c_int64), ("d2h_bytes", c_int64)]
+                ("syev_flops", c_double), ("h2d_bytes", c_int64), ("d2h_bytes", c_int64),
+                ("tri_launches", c_int64), ("tri_ms", c_double), ("tri_flops", c_double),
+                ("tri_bytes", c_double)]
 
 
 _lib = None
