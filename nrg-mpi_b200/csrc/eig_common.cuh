@@ -80,20 +80,29 @@ struct SeqLanes {
     __device__ double sum(double v) const { return v; }
     __device__ double prod(double v) const { return v; }
 };
-struct WarpLanes {
-    int lane;
-    __device__ int first() const { return lane; }
-    __device__ int step() const { return 32; }
-    __device__ bool leader() const { return lane == 0; }
+// G aligned lanes of a warp (G = 2, 4, ..., 32) share one item; the shuffles name only
+// the group's lanes, so groups of one warp may leave their loops at different times
+template <int G>
+struct GroupLanes {
+    int lane;   // lane index in the warp
+    __device__ int first() const { return lane & (G - 1); }
+    __device__ int step() const { return G; }
+    __device__ bool leader() const { return (lane & (G - 1)) == 0; }
+    __device__ unsigned mask() const {
+        return G == 32 ? 0xffffffffu : (((1u << G) - 1u) << (lane & ~(G - 1)));
+    }
     __device__ double sum(double v) const {
-        for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+        for (int o = G / 2; o > 0; o >>= 1) v += __shfl_xor_sync(mask(), v, o);
         return v;
     }
     __device__ double prod(double v) const {
-        for (int o = 16; o > 0; o >>= 1) v *= __shfl_xor_sync(0xffffffffu, v, o);
+        for (int o = G / 2; o > 0; o >>= 1) v *= __shfl_xor_sync(mask(), v, o);
         return v;
     }
 };
+using WarpLanes = GroupLanes<32>;
+// lanes per item inside the one-block merges
+constexpr int kMergeLanes = 4;
 
 // Root j of 1 + rho * sum_i zz_i^2 / (dd_i - lambda) = 0 (rho > 0, dd ascending, zz != 0),
 // returned as lambda = dd[org] + tau with org the pole nearer to the root, so that every
@@ -129,9 +138,9 @@ __device__ void secular_root(R r, int K, const double* dd, const double* zz, dou
     for (int it = 0; it < 100; ++it) {
         double psi = 0.0, dpsi = 0.0, phi = 0.0, dphi = 0.0;
         for (int i = r.first(); i < K; i += r.step()) {
-            const double del = (dd[i] - base) - t;
-            const double q = zz[i] * zz[i] / del;
-            if (i <= j) { psi += q; dpsi += q / del; } else { phi += q; dphi += q / del; }
+            const double rdel = 1.0 / ((dd[i] - base) - t);
+            const double q = zz[i] * zz[i] * rdel;
+            if (i <= j) { psi += q; dpsi += q * rdel; } else { phi += q; dphi += q * rdel; }
         }
         psi = r.sum(psi); dpsi = r.sum(dpsi); phi = r.sum(phi); dphi = r.sum(dphi);
         psi *= rho; dpsi *= rho; phi *= rho; dphi *= rho;
@@ -393,13 +402,14 @@ __device__ void dc_merge(G g, int a, int mid, int b, int n, double* Z, double* D
                          double* gsm, int* status) {
     const int t = g.rank(), T = g.size();
     const int nn = b - a;
+    const GroupLanes<kMergeLanes> gl{(int)(threadIdx.x & 31)};
     merge_prep(g, a, mid, b, n, Z, D, E, S, red);
     g.sync();
-    merge_roots(t, T, a, mid, E, S, status);
+    merge_roots(t / kMergeLanes, T / kMergeLanes, a, mid, E, S, status, gl);
     g.sync();
-    merge_zhat(t, T, a, mid, E, S);
+    merge_zhat(t / kMergeLanes, T / kMergeLanes, a, mid, E, S, gl);
     g.sync();
-    merge_ucols(t, T, a, n, S, U);
+    merge_ucols(t / kMergeLanes, T / kMergeLanes, a, n, S, U, gl);
     merge_vals(t, T, a, b, S);
     g.sync();
     merge_rank(t, T, a, b, S);

@@ -224,14 +224,14 @@ __global__ void __launch_bounds__(TPB) k_tri_finish(const LSec* __restrict__ sec
 // After each panel every block applies A -= V W^T + W V^T to its own columns.  Blocks of
 // different clusters never touch each other's data.
 constexpr int TT = 512;     // threads per block of the cluster kernel
-constexpr int TRW = 64;     // rows per staged chunk of the trailing update
+constexpr int TRW = 128;    // rows per staged chunk of the trailing update
 constexpr int P2W = 2 * NB + 2;   // partials per block: W^T v | V^T v | y.v
 
 struct TriLayout {
-    int MM, PN;
+    int MM, PN, NRB;   // own indices per block, rows (even), row batches of 256
     __host__ __device__ long long doubles(int CL) const {
         return 2LL * NB * MM + PN + MM + (long long)CL * P2W + CL + 2 + 2LL * NB + 2LL * NB + P2W + 32 +
-               2LL * NB * TRW;
+               2LL * NB * TRW + (long long)NRB * MM;
     }
 };
 
@@ -277,6 +277,7 @@ __global__ void __launch_bounds__(TT, 1) k_tri_cluster(const LSec* __restrict__ 
     double* red = tsum + P2W;              // 32
     double* stV = red + 32;                // NB x TRW staged rows of V (transposed)
     double* stW = stV + NB * TRW;          // NB x TRW
+    double* ysp = stW + NB * TRW;          // NRB x MM partial y per row batch
     double* Vg = L.VW;
     double* Wg = L.VW + (size_t)NB * n;
     double* A = L.A;
@@ -326,34 +327,42 @@ __global__ void __launch_bounds__(TT, 1) k_tri_cluster(const LSec* __restrict__ 
             if (rank == 0 && tid == 0) { L.E[k] = beta; L.TAU[k] = tau; }
             // ---- B: y of the own columns, partials ----
             const int mB = first_own(k + 1);
-            // a warp takes two columns at a time, 8 rows per lane per batch: 16 independent
-            // loads in flight per lane keep the L2 stream busy
-            for (int c0 = mB + 2 * warp; c0 < cnt; c0 += 2 * NW) {
-                const bool two = c0 + 1 < cnt;
-                const double* ca = A + (size_t)(rank + CL * c0) * n;
-                const double* cb = two ? ca + (size_t)CL * n : ca;
-                double sa = 0.0, sb = 0.0;
-                for (int r0 = k + 1; r0 < n; r0 += 256) {
-                    double xa[8], xb[8], xv[8];
+            // work items of four own columns x 256 rows, one warp each, 32 independent loads
+            // per lane; partial sums per row batch, added in a fixed order
+            {
+                const int nq = (cnt - mB + 3) / 4, nrb = (n - k - 1 + 255) / 256;
+                for (int item = warp; item < nq * nrb; item += NW) {
+                    const int g = item % nq, rb = item / nq, m0 = mB + 4 * g;
+                    const double* col[4];
+#pragma unroll
+                    for (int c = 0; c < 4; ++c) col[c] = A + (size_t)(rank + CL * min(m0 + c, cnt - 1)) * n;
+                    const int rbase = k + 1 + rb * 256;
+                    double x[4][8], xv[8];
 #pragma unroll
                     for (int u = 0; u < 8; ++u) {
-                        const int r = r0 + lane + 32 * u;
+                        const int r = rbase + lane + 32 * u;
                         const bool in = r < n;
-                        xa[u] = in ? ca[r] : 0.0;
-                        xb[u] = in ? cb[r] : 0.0;
                         xv[u] = in ? cv[r] : 0.0;
-                    }
 #pragma unroll
-                    for (int u = 0; u < 8; ++u) {
-                        sa = fma(xa[u], xv[u], sa);
-                        sb = fma(xb[u], xv[u], sb);
+                        for (int c = 0; c < 4; ++c) x[c][u] = in ? col[c][r] : 0.0;
                     }
+                    double sc[4] = {0.0, 0.0, 0.0, 0.0};
+#pragma unroll
+                    for (int u = 0; u < 8; ++u)
+#pragma unroll
+                        for (int c = 0; c < 4; ++c) sc[c] = fma(x[c][u], xv[u], sc[c]);
+#pragma unroll
+                    for (int c = 0; c < 4; ++c) sc[c] = warp_sum(sc[c]);
+                    if (lane == 0)
+#pragma unroll
+                        for (int c = 0; c < 4; ++c)
+                            if (m0 + c < cnt) ysp[rb * MM + m0 + c] = sc[c];
                 }
-                sa = warp_sum(sa);
-                sb = warp_sum(sb);
-                if (lane == 0) {
-                    ys[c0] = sa;
-                    if (two) ys[c0 + 1] = sb;
+                __syncthreads();
+                for (int m2 = mB + tid; m2 < cnt; m2 += TT) {
+                    double sy = 0.0;
+                    for (int rb = 0; rb < nrb; ++rb) sy += ysp[rb * MM + m2];
+                    ys[m2] = sy;
                 }
             }
             __syncthreads();   // ys and VO(:, j) complete
@@ -416,6 +425,8 @@ __global__ void __launch_bounds__(TT, 1) k_tri_cluster(const LSec* __restrict__ 
         const int r0 = last + 1, jc = last - p + 1;
         cluster.sync();
         const int mR = first_own(r0);
+        // register tiles of 4 rows (tr + 32 u) x 4 own columns (4 tc + c), K = 2 jc
+        const int tr = tid & 31, tc = tid >> 5;
         for (int ib = r0; ib < n; ib += TRW) {
             for (int e = tid; e < jc * TRW; e += TT) {
                 const int q = e / TRW, r = e % TRW, row = ib + r;
@@ -423,15 +434,46 @@ __global__ void __launch_bounds__(TT, 1) k_tri_cluster(const LSec* __restrict__ 
                 stW[q * TRW + r] = row < n ? __ldcg(Wg + row + (size_t)q * n) : 0.0;
             }
             __syncthreads();
-            const int r = tid % TRW, g = tid / TRW, row = ib + r;
-            if (row < n)
-                for (int mm = mR + g; mm < cnt; mm += TT / TRW) {
-                    const size_t l = (size_t)(rank + CL * mm);
-                    double s = 0.0;
-                    for (int q = 0; q < jc; ++q)
-                        s += stV[q * TRW + r] * WO[q * MM + mm] + stW[q * TRW + r] * VO[q * MM + mm];
-                    A[row + l * n] -= s;
+            for (int mc = mR; mc < cnt; mc += 4 * (TT / 32)) {
+                const int m0 = mc + 4 * tc;
+                if (m0 < cnt) {
+                    int mcol[4];
+#pragma unroll
+                    for (int c = 0; c < 4; ++c) mcol[c] = min(m0 + c, cnt - 1);
+                    double acc[4][4];
+#pragma unroll
+                    for (int u = 0; u < 4; ++u)
+#pragma unroll
+                        for (int c = 0; c < 4; ++c) acc[u][c] = 0.0;
+                    for (int q = 0; q < jc; ++q) {
+                        double av[4], aw[4], bw[4], bv[4];
+#pragma unroll
+                        for (int u = 0; u < 4; ++u) {
+                            av[u] = stV[q * TRW + tr + 32 * u];
+                            aw[u] = stW[q * TRW + tr + 32 * u];
+                        }
+#pragma unroll
+                        for (int c = 0; c < 4; ++c) {
+                            bw[c] = WO[q * MM + mcol[c]];
+                            bv[c] = VO[q * MM + mcol[c]];
+                        }
+#pragma unroll
+                        for (int u = 0; u < 4; ++u)
+#pragma unroll
+                            for (int c = 0; c < 4; ++c) acc[u][c] = fma(av[u], bw[c], fma(aw[u], bv[c], acc[u][c]));
+                    }
+#pragma unroll
+                    for (int c = 0; c < 4; ++c) {
+                        if (m0 + c >= cnt) continue;
+                        double* colp = A + (size_t)(rank + CL * (m0 + c)) * n;
+#pragma unroll
+                        for (int u = 0; u < 4; ++u) {
+                            const int row = ib + tr + 32 * u;
+                            if (row < n) colp[row] -= acc[u][c];
+                        }
+                    }
                 }
+            }
             __syncthreads();
         }
     }
@@ -820,6 +862,7 @@ static int tri_cluster_cl(nrg_context* ctx, const LSec* dsec, int ns, int maxn, 
     TriLayout lay;
     lay.MM = (maxn + CL - 1) / CL;
     lay.PN = maxn + (maxn & 1);
+    lay.NRB = (maxn + 255) / 256;
     if (lay.MM > TT) return NRG_OK;
     const size_t smem = sizeof(double) * (size_t)lay.doubles(CL);
     int dev = 0, optin = 0;
