@@ -146,44 +146,103 @@ __global__ void k_im_gather(const ImGatherProb* __restrict__ probs, const long l
 }
 
 // spike weights w = S * Y (or S^2/pf at T=0) at energies sgn*(E_k - cE*E_l)*scale,
-// binned like binningSpike (module.F90:1210-1254); raw sums per (matrix, sign)
-__global__ void k_spikes(const SpikeProb* __restrict__ probs, const long long* __restrict__ prefix, int nprob,
-                         const double* __restrict__ W, const double* __restrict__ E, int nbin,
-                         double* __restrict__ binPos, double* __restrict__ binNeg,
-                         double* __restrict__ tot, long long total) {
-    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < total;
-         e += (long long)gridDim.x * blockDim.x) {
-        int lo = 0, hi = nprob - 1;
-        while (lo < hi) {
-            const int mid = (lo + hi + 1) >> 1;
-            if (prefix[mid] <= e) lo = mid; else hi = mid - 1;
+// binned like binningSpike (module.F90:1210-1254); raw sums per (matrix, sign).
+// One block per tile of 32 k x 64 l spikes of one problem: the tile's bins are first
+// accumulated in a shared-memory window (when they span at most kSpkWin bins), then
+// added to the global bins once per touched bin; the raw sum takes one add per block.
+constexpr int kSpkTK = 32, kSpkTL = 64, kSpkWin = 4096;
+
+__global__ void __launch_bounds__(256) k_spikes(const SpikeProb* __restrict__ probs,
+                                                const long long* __restrict__ tilePrefix, int nprob,
+                                                const double* __restrict__ W, const double* __restrict__ E,
+                                                int nbin, double* __restrict__ binPos, double* __restrict__ binNeg,
+                                                double* __restrict__ tot) {
+    __shared__ double hist[kSpkWin];
+    __shared__ double rs[8];
+    __shared__ int rmin[8], rmax[8];
+    const long long bid = blockIdx.x;
+    int lo = 0, hi = nprob - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (tilePrefix[mid] <= bid) lo = mid; else hi = mid - 1;
+    }
+    const SpikeProb pr = probs[lo];
+    const long long tix = bid - tilePrefix[lo];
+    const int ntk = (pr.kk + kSpkTK - 1) / kSpkTK;
+    const int tk = (int)(tix % ntk), tl = (int)(tix / ntk);
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int k1 = tk * kSpkTK + lane;
+    const int lb = tl * kSpkTL + warp;
+    const double ek = k1 < pr.kk ? E[pr.ek_off + k1] : 0.0;
+    int ia[8], ib[8];
+    double wa[8], wv[8];
+    double wsum = 0.0;
+    int bmin = 0x7fffffff, bmax = -1;
+#pragma unroll
+    for (int u = 0; u < 8; ++u) {
+        const int l = lb + 8 * u;
+        ia[u] = -1;
+        ib[u] = -1;
+        wa[u] = 0.0;
+        wv[u] = 0.0;
+        if (k1 < pr.kk && l < pr.nl) {
+            const long long loc = (long long)k1 + (long long)l * pr.kk;
+            const double sv = W[pr.s_off + loc];
+            const double w = (pr.y_off >= 0) ? sv * W[pr.y_off + loc] : sv * sv * pr.invpf;
+            const double el = E[pr.el_off + (long long)l * pr.lstride];
+            const double en = pr.sgn * ((ek - pr.cE * el) * pr.scale);
+            wsum += w;
+            // binningSpike
+            const double position = (log10(fabs(en)) - (-15.0)) * 1000.0 + 1.0;
+            long long pref = (long long)position;   // int(): truncation toward zero
+            int i1 = 0;
+            if (position <= 0.0) i1 = 1;
+            else if (position >= (double)nbin) i1 = nbin;
+            if (pref <= 0) pref = 1;
+            if (i1 > 0) {
+                ia[u] = i1;
+                wa[u] = w;
+            } else {
+                const double wb = position - (double)pref;
+                ia[u] = (int)pref;
+                wa[u] = w * (1.0 - wb);
+                ib[u] = (int)pref + 1;
+                wv[u] = w * wb;
+            }
+            bmin = min(bmin, ia[u]);
+            bmax = max(bmax, ib[u] >= 0 ? ib[u] : ia[u]);
         }
-        const SpikeProb pr = probs[lo];
-        const long long loc = e - prefix[lo];
-        const int k1 = (int)(loc % pr.kk), l = (int)(loc / pr.kk);
-        const double s = W[pr.s_off + loc];
-        double w;
-        if (pr.y_off >= 0) w = s * W[pr.y_off + loc];
-        else w = s * s * pr.invpf;
-        const double ek = E[pr.ek_off + k1];
-        const double el = E[pr.el_off + (long long)l * pr.lstride];
-        const double en = pr.sgn * ((ek - pr.cE * el) * pr.scale);
-        double* cont = pr.toPos ? binPos : binNeg;
-        atomicAdd(&tot[2 * pr.m + (pr.toPos ? 1 : 0)], w);
-        // binningSpike
-        const double position = (log10(fabs(en)) - (-15.0)) * 1000.0 + 1.0;
-        long long pref = (long long)position;   // int(): truncation toward zero
-        int i1 = 0;
-        if (position <= 0.0) i1 = 1;
-        else if (position >= (double)nbin) i1 = nbin;
-        if (pref <= 0) pref = 1;
-        const size_t base = (size_t)pr.m * nbin - 1;
-        if (i1 > 0) {
-            atomicAdd(&cont[base + i1], w);
-        } else {
-            const double wb = position - (double)pref;
-            atomicAdd(&cont[base + pref], w * (1.0 - wb));
-            atomicAdd(&cont[base + pref + 1], w * wb);
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        wsum += __shfl_xor_sync(0xffffffffu, wsum, o);
+        bmin = min(bmin, __shfl_xor_sync(0xffffffffu, bmin, o));
+        bmax = max(bmax, __shfl_xor_sync(0xffffffffu, bmax, o));
+    }
+    if (lane == 0) { rs[warp] = wsum; rmin[warp] = bmin; rmax[warp] = bmax; }
+    __syncthreads();
+    double ws = 0.0;
+    int wmin = 0x7fffffff, wmax = -1;
+    for (int q = 0; q < 8; ++q) { ws += rs[q]; wmin = min(wmin, rmin[q]); wmax = max(wmax, rmax[q]); }
+    if (tid == 0 && wmax >= 0) atomicAdd(&tot[2 * pr.m + (pr.toPos ? 1 : 0)], ws);
+    if (wmax < 0) return;
+    double* cont = (pr.toPos ? binPos : binNeg) + ((size_t)pr.m * nbin - 1);
+    const int win = wmax - wmin + 1;
+    if (win <= kSpkWin) {
+        for (int i = tid; i < win; i += 256) hist[i] = 0.0;
+        __syncthreads();
+#pragma unroll
+        for (int u = 0; u < 8; ++u) {
+            if (ia[u] >= 0) atomicAdd(&hist[ia[u] - wmin], wa[u]);
+            if (ib[u] >= 0) atomicAdd(&hist[ib[u] - wmin], wv[u]);
+        }
+        __syncthreads();
+        for (int i = tid; i < win; i += 256)
+            if (hist[i] != 0.0) atomicAdd(&cont[wmin + i], hist[i]);
+    } else {
+#pragma unroll
+        for (int u = 0; u < 8; ++u) {
+            if (ia[u] >= 0) atomicAdd(&cont[ia[u]], wa[u]);
+            if (ib[u] >= 0) atomicAdd(&cont[ib[u]], wv[u]);
         }
     }
 }
@@ -311,16 +370,20 @@ int run_spikes(nrg_context* ctx, std::vector<SpikeProb>& probs, const double* d_
     if (np == 0) return NRG_OK;
     std::vector<long long> prefix(np);
     long long total = 0;
-    for (int p = 0; p < np; ++p) { prefix[p] = total; total += (long long)probs[p].kk * probs[p].nl; }
+    for (int p = 0; p < np; ++p) {
+        prefix[p] = total;
+        total += (long long)((probs[p].kk + kSpkTK - 1) / kSpkTK) * ((probs[p].nl + kSpkTL - 1) / kSpkTL);
+    }
     if (total == 0) return NRG_OK;
+    if (total > 0x7fffffffLL) return NRG_ERR_TOO_LARGE;
     DevBuf& dp = ctx->scratch.b[18];
     DevBuf& dq = ctx->scratch.b[19];
     NRG_TRY(dp.ensure(sizeof(SpikeProb) * np));
     NRG_TRY(dq.ensure(sizeof(long long) * np));
     NRG_TRY(h2d_async(ctx, dp.p, probs.data(), sizeof(SpikeProb) * np));
     NRG_TRY(h2d_async(ctx, dq.p, prefix.data(), sizeof(long long) * np));
-    k_spikes<<<grid_for(total, 256), 256, 0, ctx->stream>>>(dp.as<SpikeProb>(), dq.as<long long>(), np, d_work,
-                                                          d_E, nbin, d_binPos, d_binNeg, d_tot, total);
+    k_spikes<<<(unsigned)total, 256, 0, ctx->stream>>>(dp.as<SpikeProb>(), dq.as<long long>(), np, d_work, d_E, nbin,
+                                                     d_binPos, d_binNeg, d_tot);
     ctx->launches++;
     NRG_CUDA_TRY(cudaGetLastError());
     return NRG_OK;
