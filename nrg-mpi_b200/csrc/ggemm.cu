@@ -10,23 +10,34 @@
 //   B(k,j) = B[ki(k)*b_sk + ji(j)*b_sj]          ki = b_ki ? b_ki[k] : k, ji likewise
 //   C(i,j) = C[ci(i)*c_si + cj(j)*c_sj]          ci = c_ri ? c_ri[i] : i, cj likewise
 //
-// 64x64 output tiles, 256 threads with 4x4 register tiles, k slabs of 16 staged in
-// shared memory, double buffered.  Loads are coalesced along whichever index of each
-// operand has unit stride.
+// 64x64 output tiles, 128 threads (four warps of 32x32), FP64 tensor-core MMA
+// (mma.sync m8n8k4 f64); k slabs of 16 staged in shared memory, the next slab's global
+// loads held in registers while the current slab is multiplied.  Loads are coalesced
+// along whichever index of each operand has unit stride.
 #include "internal.hpp"
 
 namespace nrg {
 namespace {
 
-constexpr int TM = 64, TN = 64, TK = 16, NT = 256;
-constexpr int LDS = TM + 1;
+constexpr int TM = 64, TN = 64, TK = 16, NT = 128;
+constexpr int LDA = TM + 4, LDB = TN + 4;   // [k][i] and [k][j] rows, padded against bank conflicts
 
-__device__ __forceinline__ void load_slab(const GemmProblem& P, int i0, int j0, int k0, double* As,
-                                          double* Bs, bool a_kfast, bool b_kfast) {
+__device__ __forceinline__ void dmma(double& d0, double& d1, double a, double b) {
+    asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};\n"
+                 : "+d"(d0), "+d"(d1)
+                 : "d"(a), "d"(b));
+}
+
+struct Slab {
+    double a[(TM * TK) / NT], b[(TN * TK) / NT];
+};
+
+__device__ __forceinline__ void fetch_slab(const GemmProblem& P, int i0, int j0, int k0, Slab& r, bool a_kfast,
+                                           bool b_kfast) {
     const int tid = threadIdx.x;
 #pragma unroll
-    for (int r = 0; r < (TM * TK) / NT; ++r) {
-        const int e = tid + r * NT;
+    for (int u = 0; u < (TM * TK) / NT; ++u) {
+        const int e = tid + u * NT;
         int ii, kk;
         if (a_kfast) { kk = e % TK; ii = e / TK; } else { ii = e % TM; kk = e / TM; }
         const int gi = i0 + ii, gk = k0 + kk;
@@ -36,11 +47,11 @@ __device__ __forceinline__ void load_slab(const GemmProblem& P, int i0, int j0, 
             const long long ki = P.a_ki ? P.a_ki[gk] : gk;
             v = P.A[ri * P.a_si + ki * P.a_sk];
         }
-        As[kk * LDS + ii] = v;
+        r.a[u] = v;
     }
 #pragma unroll
-    for (int r = 0; r < (TN * TK) / NT; ++r) {
-        const int e = tid + r * NT;
+    for (int u = 0; u < (TN * TK) / NT; ++u) {
+        const int e = tid + u * NT;
         int jj, kk;
         if (b_kfast) { kk = e % TK; jj = e / TK; } else { jj = e % TN; kk = e / TN; }
         const int gj = j0 + jj, gk = k0 + kk;
@@ -50,14 +61,32 @@ __device__ __forceinline__ void load_slab(const GemmProblem& P, int i0, int j0, 
             const long long ji = P.b_ji ? P.b_ji[gj] : gj;
             v = P.B[ki * P.b_sk + ji * P.b_sj];
         }
-        Bs[kk * LDS + jj] = v;
+        r.b[u] = v;
+    }
+}
+
+__device__ __forceinline__ void store_slab(const Slab& r, double* As, double* Bs, bool a_kfast, bool b_kfast) {
+    const int tid = threadIdx.x;
+#pragma unroll
+    for (int u = 0; u < (TM * TK) / NT; ++u) {
+        const int e = tid + u * NT;
+        int ii, kk;
+        if (a_kfast) { kk = e % TK; ii = e / TK; } else { ii = e % TM; kk = e / TM; }
+        As[kk * LDA + ii] = r.a[u];
+    }
+#pragma unroll
+    for (int u = 0; u < (TN * TK) / NT; ++u) {
+        const int e = tid + u * NT;
+        int jj, kk;
+        if (b_kfast) { kk = e % TK; jj = e / TK; } else { jj = e % TN; kk = e / TN; }
+        Bs[kk * LDB + jj] = r.b[u];
     }
 }
 
 __global__ void __launch_bounds__(NT) k_ggemm(const GemmProblem* __restrict__ probs,
                                               const int* __restrict__ tilePrefix, int nprob) {
-    __shared__ double As[2][TK * LDS];
-    __shared__ double Bs[2][TK * LDS];
+    __shared__ double As[2][TK * LDA];
+    __shared__ double Bs[2][TK * LDB];
     const int bid = blockIdx.x;
     int lo = 0, hi = nprob - 1;
     while (lo < hi) {
@@ -76,47 +105,57 @@ __global__ void __launch_bounds__(NT) k_ggemm(const GemmProblem* __restrict__ pr
     }
     const bool a_kfast = (P.a_sk == 1 && P.a_si != 1);
     const bool b_kfast = (P.b_sk == 1 && P.b_sj != 1);
-    const int tx = threadIdx.x % 16, ty = threadIdx.x / 16;
-    double acc[4][4];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int wi = (warp >> 1) * 32, wj = (warp & 1) * 32;   // warp tile origin
+    const int g = lane >> 2, q4 = lane & 3;
+    double acc[4][4][2];
 #pragma unroll
     for (int r = 0; r < 4; ++r)
 #pragma unroll
-        for (int c = 0; c < 4; ++c) acc[r][c] = 0.0;
+        for (int c = 0; c < 4; ++c) acc[r][c][0] = acc[r][c][1] = 0.0;
     const int nslab = (P.K + TK - 1) / TK;
-    if (nslab > 0) load_slab(P, i0, j0, 0, As[0], Bs[0], a_kfast, b_kfast);
+    Slab reg;
+    if (nslab > 0) {
+        fetch_slab(P, i0, j0, 0, reg, a_kfast, b_kfast);
+        store_slab(reg, As[0], Bs[0], a_kfast, b_kfast);
+    }
     __syncthreads();
     for (int s = 0; s < nslab; ++s) {
         const int cur = s & 1;
-        if (s + 1 < nslab) load_slab(P, i0, j0, (s + 1) * TK, As[cur ^ 1], Bs[cur ^ 1], a_kfast, b_kfast);
+        if (s + 1 < nslab) fetch_slab(P, i0, j0, (s + 1) * TK, reg, a_kfast, b_kfast);
         const double* as = As[cur];
         const double* bs = Bs[cur];
 #pragma unroll
-        for (int kk = 0; kk < TK; ++kk) {
-            double a[4], b[4];
+        for (int ks = 0; ks < TK; ks += 4) {
+            double af[4], bf[4];
 #pragma unroll
-            for (int r = 0; r < 4; ++r) a[r] = as[kk * LDS + ty * 4 + r];
+            for (int r = 0; r < 4; ++r) af[r] = as[(ks + q4) * LDA + wi + r * 8 + g];
 #pragma unroll
-            for (int c = 0; c < 4; ++c) b[c] = bs[kk * LDS + tx + 16 * c];
+            for (int c = 0; c < 4; ++c) bf[c] = bs[(ks + q4) * LDB + wj + c * 8 + g];
 #pragma unroll
             for (int r = 0; r < 4; ++r)
 #pragma unroll
-                for (int c = 0; c < 4; ++c) acc[r][c] = fma(a[r], b[c], acc[r][c]);
+                for (int c = 0; c < 4; ++c) dmma(acc[r][c][0], acc[r][c][1], af[r], bf[c]);
         }
+        if (s + 1 < nslab) store_slab(reg, As[cur ^ 1], Bs[cur ^ 1], a_kfast, b_kfast);
         __syncthreads();
     }
 #pragma unroll
     for (int r = 0; r < 4; ++r) {
-        const int gi = i0 + ty * 4 + r;
+        const int gi = i0 + wi + r * 8 + g;
         if (gi >= P.M) continue;
         const long long ci = P.c_ri ? P.c_ri[gi] : gi;
 #pragma unroll
         for (int c = 0; c < 4; ++c) {
-            const int gj = j0 + tx + 16 * c;
-            if (gj >= P.N) continue;
-            const long long cj = P.c_ji ? P.c_ji[gj] : gj;
-            double* out = P.C + ci * P.c_si + cj * P.c_sj;
-            const double v = P.alpha * acc[r][c];
-            *out = (P.beta == 0.0) ? v : P.beta * *out + v;
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                const int gj = j0 + wj + c * 8 + 2 * q4 + h;
+                if (gj >= P.N) continue;
+                const long long cj = P.c_ji ? P.c_ji[gj] : gj;
+                double* out = P.C + ci * P.c_si + cj * P.c_sj;
+                const double v = P.alpha * acc[r][c][h];
+                *out = (P.beta == 0.0) ? v : P.beta * *out + v;
+            }
         }
     }
 }
