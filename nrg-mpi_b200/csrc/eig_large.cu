@@ -221,8 +221,11 @@ __global__ void __launch_bounds__(TPB) k_tri_finish(const LSec* __restrict__ sec
 //      forms t1 = W^T v, t2 = V^T v, w.v = tau (y.v - 2 t1.t2) and
 //      w = tau (y - V t1 - W t2) - (tau/2)(w.v) v for its own rows, and the pivot row's
 //      w for the next column.
-// After each panel every block applies A -= V W^T + W V^T to its own columns.  Blocks of
-// different clusters never touch each other's data.
+// After each panel every block writes its panel rows of V and W, the reflectors and the
+// panel's D, E and tau to global memory (inside the panel they stay in shared memory: a
+// global store pending at a cluster barrier makes the barrier wait for it) and applies
+// A -= V W^T + W V^T to its own columns.  Blocks of different clusters never touch each
+// other's data.
 constexpr int TT = 512;     // threads per block of the cluster kernel
 constexpr int TRW = 128;    // rows per staged chunk of the trailing update
 constexpr int P2W = 2 * NB + 2;   // partials per block: W^T v | V^T v | y.v
@@ -230,8 +233,10 @@ constexpr int P2W = 2 * NB + 2;   // partials per block: W^T v | V^T v | y.v
 struct TriLayout {
     int MM, PN, NRB;   // own indices per block, rows (even), row batches of 256
     __host__ __device__ long long doubles(int CL) const {
+        // the panel rows AR share their space with the staging of the trailing update
+        const long long stage = (long long)NB * MM > 2LL * NB * TRW ? (long long)NB * MM : 2LL * NB * TRW;
         return 2LL * NB * MM + PN + MM + (long long)CL * P2W + CL + 2 + 2LL * NB + 2LL * NB + P2W + 32 +
-               2LL * NB * TRW + (long long)NRB * MM;
+               stage + (long long)NRB * MM + 3LL * NB;
     }
 };
 
@@ -241,16 +246,16 @@ __device__ __forceinline__ double warp_sum(double v) {
 }
 
 // w = tau (y - sum_q (V_q t1_q + W_q t2_q)) + al v with explicit roundings, so that every
-// block computes the pivot row's w bit-identically to its owner
+// block computes the pivot row's w bit-identically to its owner (two partial sums)
 __device__ __forceinline__ double w_entry(double y, const double* Vr, const double* Wr, int stride,
                                           const double* t1, const double* t2, int j, double tau,
                                           double al, double v) {
-    double s = y;
+    double s = y, s2 = 0.0;
     for (int q = 0; q < j; ++q) {
         s = fma(-Vr[q * stride], t1[q], s);
-        s = fma(-Wr[q * stride], t2[q], s);
+        s2 = fma(-Wr[q * stride], t2[q], s2);
     }
-    return fma(al, v, __dmul_rn(tau, s));
+    return fma(al, v, __dmul_rn(tau, __dadd_rn(s, s2)));
 }
 
 template <int CL>
@@ -275,9 +280,11 @@ __global__ void __launch_bounds__(TT, 1) k_tri_cluster(const LSec* __restrict__ 
     double* piv = pivn + 2 * NB;           // 2 NB: W(k, q) | V(k, q) of the current pivot row
     double* tsum = piv + 2 * NB;           // t1 | t2 | y.v
     double* red = tsum + P2W;              // 32
-    double* stV = red + 32;                // NB x TRW staged rows of V (transposed)
-    double* stW = stV + NB * TRW;          // NB x TRW
-    double* ysp = stW + NB * TRW;          // NRB x MM partial y per row batch
+    double* AR = red + 32;                 // NB x MM: A(p + q, own column m), during the columns
+    double* stV = AR;                      // NB x TRW staged rows of V (transposed), during the
+    double* stW = stV + NB * TRW;          // trailing update; NB x TRW
+    double* ysp = AR + ((size_t)NB * MM > 2 * NB * TRW ? (size_t)NB * MM : 2 * NB * TRW);   // NRB x MM
+    double* pan = ysp + (size_t)lay.NRB * MM;   // D | E | tau of the panel's columns
     double* Vg = L.VW;
     double* Wg = L.VW + (size_t)NB * n;
     double* A = L.A;
@@ -286,6 +293,17 @@ __global__ void __launch_bounds__(TT, 1) k_tri_cluster(const LSec* __restrict__ 
 
     for (int p = 0; p < n - 1; p += NB) {
         const int last = min(p + NB - 1, n - 2);
+        const int jn = last - p + 1;
+        // rows p..last of the own columns: the panel's columns read them as rows (the
+        // trailing matrix is stored in full) and nothing writes them during the panel
+        {
+            const int m0 = first_own(p);
+            for (int e = tid; e < jn * (cnt - m0); e += TT) {
+                const int q = e % jn, m = m0 + e / jn;
+                AR[q * MM + m] = __ldcg(A + (size_t)(p + q) + (size_t)(rank + CL * m) * n);
+            }
+            __syncthreads();
+        }
         for (int k = p; k <= last; ++k) {
             const int j = k - p;
             // ---- A: own rows of column k, broadcast ----
@@ -294,11 +312,20 @@ __global__ void __launch_bounds__(TT, 1) k_tri_cluster(const LSec* __restrict__ 
             const int i = rank + CL * m;
             double c = 0.0, ss = 0.0;
             if (act) {
-                c = A[(size_t)k + (size_t)i * n];
-                double s = 0.0;
-                for (int q = 0; q < j; ++q) s += VO[q * MM + m] * piv[q] + WO[q * MM + m] * piv[NB + q];
-                c -= s;
-                if (i == k) L.D[k] = c;
+                double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
+                int q = 0;
+                for (; q + 1 < j; q += 2) {
+                    s0 = fma(VO[q * MM + m], piv[q], s0);
+                    s1 = fma(WO[q * MM + m], piv[NB + q], s1);
+                    s2 = fma(VO[(q + 1) * MM + m], piv[q + 1], s2);
+                    s3 = fma(WO[(q + 1) * MM + m], piv[NB + q + 1], s3);
+                }
+                if (q < j) {
+                    s0 = fma(VO[q * MM + m], piv[q], s0);
+                    s1 = fma(WO[q * MM + m], piv[NB + q], s1);
+                }
+                c = AR[j * MM + m] - ((s0 + s2) + (s1 + s3));
+                if (i == k) pan[j] = c;
                 if (i >= k + 2) ss = c * c;
                 if (i >= k + 1)
                     for (int r = 0; r < CL; ++r) cluster.map_shared_rank(cv, r)[i] = c;
@@ -315,34 +342,46 @@ __global__ void __launch_bounds__(TT, 1) k_tri_cluster(const LSec* __restrict__ 
                 tau = (beta - alpha) / beta;
                 scal = 1.0 / (alpha - beta);
             }
-            for (int r = k + 1 + tid; r < n; r += TT)
-                cv[r] = (r == k + 1) ? 1.0 : (xn2 == 0.0 ? 0.0 : cv[r] * scal);
+            // v(k+1) = 1 is implied: cv(k+1) keeps alpha, which every thread reads above
+            for (int r = k + 2 + tid; r < n; r += TT) cv[r] = xn2 == 0.0 ? 0.0 : cv[r] * scal;
+            if (act && i >= k + 1) VO[j * MM + m] = (i == k + 1) ? 1.0 : (xn2 == 0.0 ? 0.0 : c * scal);
+            if (tid == 0) { pan[NB + j] = beta; pan[2 * NB + j] = tau; }
             __syncthreads();
-            if (act && i >= k + 1) {
-                const double v = cv[i];
-                VO[j * MM + m] = v;
-                Vg[(size_t)i + (size_t)j * n] = v;
-                if (i > k + 1) A[(size_t)i + (size_t)k * n] = v;
-            }
-            if (rank == 0 && tid == 0) { L.E[k] = beta; L.TAU[k] = tau; }
-            // ---- B: y of the own columns, partials ----
+            // ---- B: partial W^T v, V^T v over the own rows, the next pivot row, then y of
+            // the own columns and partial y.v ----
             const int mB = first_own(k + 1);
-            // work items of four own columns x 256 rows, one warp each, 32 independent loads
-            // per lane; partial sums per row batch, added in a fixed order
+            const int nq = (cnt - mB + 3) / 4, nrb = (n - k - 1 + 255) / 256, nitems = nq * nrb;
+            const double* vj = VO + j * MM;
+            for (int o = warp; o < 2 * j; o += NW) {
+                const double* colp = (o < j) ? WO + o * MM : VO + (o - j) * MM;
+                double s = 0.0;
+                for (int mm = mB + lane; mm < cnt; mm += 32) s = fma(colp[mm], vj[mm], s);
+                s = warp_sum(s);
+                if (lane < CL) cluster.map_shared_rank(P2, lane)[rank * P2W + (o < j ? o : NB + (o - j))] = s;
+            }
+            const bool pivot_owner = (rank == (k + 1) % CL);
+            if (pivot_owner && k + 1 <= last) {
+                for (int e = tid; e < 2 * j * CL; e += TT) {
+                    const int q = e / CL, r = e % CL;
+                    const double val = q < j ? VO[q * MM + mB] : WO[(q - j) * MM + mB];
+                    cluster.map_shared_rank(pivn, r)[q < j ? q : NB + (q - j)] = val;
+                }
+            }
+            // y = A v in work items of four own columns x 256 rows, one warp each, 32
+            // independent loads per lane; partial sums per row batch, added in a fixed order
             {
-                const int nq = (cnt - mB + 3) / 4, nrb = (n - k - 1 + 255) / 256;
-                for (int item = warp; item < nq * nrb; item += NW) {
+                for (int item = warp; item < nitems; item += NW) {
                     const int g = item % nq, rb = item / nq, m0 = mB + 4 * g;
+                    const int rbase = k + 1 + rb * 256;
                     const double* col[4];
 #pragma unroll
                     for (int c = 0; c < 4; ++c) col[c] = A + (size_t)(rank + CL * min(m0 + c, cnt - 1)) * n;
-                    const int rbase = k + 1 + rb * 256;
                     double x[4][8], xv[8];
 #pragma unroll
                     for (int u = 0; u < 8; ++u) {
                         const int r = rbase + lane + 32 * u;
                         const bool in = r < n;
-                        xv[u] = in ? cv[r] : 0.0;
+                        xv[u] = in ? (r == k + 1 ? 1.0 : cv[r]) : 0.0;
 #pragma unroll
                         for (int c = 0; c < 4; ++c) x[c][u] = in ? col[c][r] : 0.0;
                     }
@@ -359,32 +398,17 @@ __global__ void __launch_bounds__(TT, 1) k_tri_cluster(const LSec* __restrict__ 
                             if (m0 + c < cnt) ysp[rb * MM + m0 + c] = sc[c];
                 }
                 __syncthreads();
-                for (int m2 = mB + tid; m2 < cnt; m2 += TT) {
-                    double sy = 0.0;
-                    for (int rb = 0; rb < nrb; ++rb) sy += ysp[rb * MM + m2];
-                    ys[m2] = sy;
-                }
-            }
-            __syncthreads();   // ys and VO(:, j) complete
-            const double* vj = VO + j * MM;
-            for (int o = warp; o < 2 * j; o += NW) {
-                const double* colp = (o < j) ? WO + o * MM : VO + (o - j) * MM;
-                double s = 0.0;
-                for (int mm = mB + lane; mm < cnt; mm += 32) s = fma(colp[mm], vj[mm], s);
-                s = warp_sum(s);
-                if (lane < CL) cluster.map_shared_rank(P2, lane)[rank * P2W + (o < j ? o : NB + (o - j))] = s;
             }
             const int mc = mB + tid;
             const bool own_c = mc < cnt;
-            double yvp = own_c ? ys[mc] * vj[mc] : 0.0;
-            const bool pivot_owner = (rank == (k + 1) % CL);
-            if (pivot_owner && k + 1 <= last) {   // the next column's pivot row
-                for (int e = tid; e < 2 * j * CL; e += TT) {
-                    const int q = e / CL, r = e % CL;
-                    const double val = q < j ? VO[q * MM + mB] : WO[(q - j) * MM + mB];
-                    cluster.map_shared_rank(pivn, r)[q < j ? q : NB + (q - j)] = val;
-                }
-                if (tid < CL) cluster.map_shared_rank(Y1, tid)[0] = ys[mB];
+            double yvp = 0.0;
+            if (own_c) {
+                double sy = 0.0;
+                for (int rb = 0; rb < nrb; ++rb) sy += ysp[rb * MM + mc];
+                ys[mc] = sy;
+                yvp = sy * vj[mc];
+                if (tid == 0 && pivot_owner && k + 1 <= last)
+                    for (int r = 0; r < CL; ++r) cluster.map_shared_rank(Y1, r)[0] = sy;
             }
             yvp = block_sum(yvp, red);
             if (tid < CL) cluster.map_shared_rank(P2, tid)[rank * P2W + 2 * NB] = yvp;
@@ -401,15 +425,15 @@ __global__ void __launch_bounds__(TT, 1) k_tri_cluster(const LSec* __restrict__ 
                 tsum[2 * NB] = s;
             }
             __syncthreads();
-            double t12 = 0.0;
-            for (int q = 0; q < j; ++q) t12 = fma(tsum[q], tsum[NB + q], t12);
-            const double wv = tau * (tsum[2 * NB] - 2.0 * t12);
-            const double al = -0.5 * tau * wv;
-            if (own_c) {
-                const double w = w_entry(ys[mc], VO + mc, WO + mc, MM, tsum, tsum + NB, j, tau, al, vj[mc]);
-                WO[j * MM + mc] = w;
-                Wg[(size_t)(rank + CL * mc) + (size_t)j * n] = w;
+            double t12 = 0.0, t12b = 0.0;
+            for (int q = 0; q + 1 < j; q += 2) {
+                t12 = fma(tsum[q], tsum[NB + q], t12);
+                t12b = fma(tsum[q + 1], tsum[NB + q + 1], t12b);
             }
+            if (j & 1) t12 = fma(tsum[j - 1], tsum[NB + j - 1], t12);
+            const double wv = tau * (tsum[2 * NB] - 2.0 * (t12 + t12b));
+            const double al = -0.5 * tau * wv;
+            if (own_c) WO[j * MM + mc] = w_entry(ys[mc], VO + mc, WO + mc, MM, tsum, tsum + NB, j, tau, al, vj[mc]);
             if (k + 1 <= last) {
                 if (tid < j) {
                     piv[tid] = pivn[NB + tid];        // W(k+1, q)
@@ -420,6 +444,25 @@ __global__ void __launch_bounds__(TT, 1) k_tri_cluster(const LSec* __restrict__ 
                 }
             }
             __syncthreads();
+        }
+        // ---- the panel's V, W, reflectors (into A below the subdiagonal), D, E and tau go
+        // to global memory once per panel: a global store pending at a cluster barrier
+        // makes the barrier wait for it ----
+        const int m1 = first_own(p + 1), nm1 = cnt - m1;
+        for (int e = tid; e < jn * nm1; e += TT) {
+            const int mm = m1 + e % nm1, q = e / nm1;
+            const int i = rank + CL * mm, kq = p + q;
+            if (i >= kq + 1) {
+                const double v = VO[q * MM + mm];
+                Vg[(size_t)i + (size_t)q * n] = v;
+                Wg[(size_t)i + (size_t)q * n] = WO[q * MM + mm];
+                if (i > kq + 1) A[(size_t)i + (size_t)kq * n] = v;
+            }
+        }
+        if (tid < jn) {
+            const int kq = p + tid;
+            if (kq % CL == rank) L.D[kq] = pan[tid];
+            if (rank == 0) { L.E[kq] = pan[NB + tid]; L.TAU[kq] = pan[2 * NB + tid]; }
         }
         // ---- trailing update of the own columns l >= r0, rows >= r0 ----
         const int r0 = last + 1, jc = last - p + 1;
