@@ -78,6 +78,14 @@ nrg_context::~nrg_context() {
     if (ev_fork) cudaEventDestroy(ev_fork);
     if (ev_join) cudaEventDestroy(ev_join);
     if (aux) cudaStreamDestroy(aux);
+    if (ev_join2) cudaEventDestroy(ev_join2);
+    if (aux2) cudaStreamDestroy(aux2);
+    if (ev_join_hi) cudaEventDestroy(ev_join_hi);
+    if (aux_hi) cudaStreamDestroy(aux_hi);
+    for (auto& t : pending_tri) {
+        cudaEventDestroy(t.a);
+        cudaEventDestroy(t.b);
+    }
     if (stage_host) cudaFreeHost(stage_host);
 }
 

@@ -20,6 +20,7 @@ namespace {
 constexpr int kThreads = 512;
 constexpr int kNB = 32;           // reflectors per back-transform panel
 constexpr int kSmemTri = 128;     // orders tridiagonalised in shared memory
+constexpr int kDcCap = 128;       // orders whose divide and conquer vectors live in shared memory
 
 // Householder tridiagonalisation of the n x n block A (leading dim lda, full storage kept
 // symmetric); reflector k is stored below the subdiagonal of column k with an implicit 1.
@@ -181,7 +182,8 @@ __global__ void __launch_bounds__(kThreads) k_syev(const SyevSector* __restrict_
     double* vs = sm + 32 + gsz;
     const int vlen = n > kNB * kNB ? n : kNB * kNB;
     double* ps = vs + vlen;
-    double* As = vs + 2 * vlen + kNB * kNB;
+    double* dcs = vs + 2 * vlen + kNB * kNB;          // D and the merge vectors (orders <= kDcCap)
+    double* As = dcs + kDcSmemDoubles * kDcCap;
 
     // ---- 1. tridiagonalisation ----
     if (smem_tri && n <= kSmemTri) {
@@ -194,7 +196,13 @@ __global__ void __launch_bounds__(kThreads) k_syev(const SyevSector* __restrict_
         tridiagonalise(A, n, n, Dd, Ee, TAU, vs, ps, red);
     }
 
-    // ---- 2. divide and conquer on (Dd, Ee) -> eigenvalues in Dd, vectors in Z ----
+    // ---- 2. divide and conquer on (Dd, Ee) -> eigenvalues in Dm, vectors in Z ----
+    double* Dm = Dd;
+    Scratch Sm = S;
+    if (n <= kDcCap) {
+        Dm = dcs;
+        Sm = scratch_smem(dcs, kDcCap);
+    }
     for (long long e = tid; e < sq; e += T) Z[e] = 0.0;
     __syncthreads();
     for (int i = tid; i < n; i += T) {
@@ -202,10 +210,8 @@ __global__ void __launch_bounds__(kThreads) k_syev(const SyevSector* __restrict_
         double dv = Dd[i];
         if (i > 0) dv -= fabs(Ee[i - 1]);
         if (i < n - 1) dv -= fabs(Ee[i]);
-        S.vals[i] = dv;
+        Dm[i] = dv;
     }
-    __syncthreads();
-    for (int i = tid; i < n; i += T) Dd[i] = S.vals[i];
     __syncthreads();
     const int warp = tid >> 5, lane = tid & 31, nwarps = T >> 5;
     for (int s = 1; s < n; s *= 2) {
@@ -214,13 +220,13 @@ __global__ void __launch_bounds__(kThreads) k_syev(const SyevSector* __restrict_
             int mi = 0;
             for (int a = 0; a + s < n; a += 2 * s, ++mi) {
                 if (mi % nwarps != warp) continue;
-                dc_merge(wg, a, a + s, min(a + 2 * s, n), n, Z, Dd, Ee, S, U, Qt, red, gsm, status);
+                dc_merge(wg, a, a + s, min(a + 2 * s, n), n, Z, Dm, Ee, Sm, U, Qt, red, gsm, status);
             }
             __syncthreads();
         } else {
             BlockG bg;
             for (int a = 0; a + s < n; a += 2 * s)
-                dc_merge(bg, a, a + s, min(a + 2 * s, n), n, Z, Dd, Ee, S, U, Qt, red, gsm, status);
+                dc_merge(bg, a, a + s, min(a + 2 * s, n), n, Z, Dm, Ee, Sm, U, Qt, red, gsm, status);
         }
     }
     __syncthreads();
@@ -228,7 +234,7 @@ __global__ void __launch_bounds__(kThreads) k_syev(const SyevSector* __restrict_
     // ---- 3. back-transformation ----
     back_transform(A, n, TAU, Z, U, Qt, vs, vs + kNB * kNB, gsm);
 
-    for (int i = tid; i < n; i += T) ev[i] = Dd[i];
+    for (int i = tid; i < n; i += T) ev[i] = Dm[i];
     for (long long e = tid; e < sq; e += T) A[e] = Z[e];
 }
 
@@ -240,7 +246,7 @@ int launch_syev(const SyevSector* d_secs, int nsec, int max_n, double* eigbuf, d
     const int gsz = 16 * (4 * (kThreads / 16) + 1) + 16 * 65;
     const size_t vlen = (size_t)(max_n > kNB * kNB ? max_n : kNB * kNB);
     const int smem_tri = max_n <= kSmemTri ? 1 : 0;
-    size_t smem = sizeof(double) * (32 + gsz + 2 * vlen + kNB * kNB +
+    size_t smem = sizeof(double) * (32 + gsz + 2 * vlen + kNB * kNB + kDcSmemDoubles * kDcCap +
                                     (smem_tri ? (size_t)max_n * max_n : 0));
     if (smem > 227 * 1024) {
         nrg_set_error_message("sector of order %d exceeds the shared-memory plan", max_n);

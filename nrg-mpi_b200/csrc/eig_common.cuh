@@ -70,6 +70,22 @@ __device__ Scratch scratch_at(double* vec, int* I, int n) {
     return S;
 }
 
+// The same vectors for a range of at most cap rows in shared memory, indexed from the
+// start of the range: cap doubles for D, then 10 cap doubles and 10 cap ints (16 cap
+// doubles in all, from dsm).  The merges' serial and iterative parts (deflation scan,
+// secular roots, ranks) then wait on shared memory instead of L2.
+constexpr int kDcSmemDoubles = 16;
+__device__ Scratch scratch_smem(double* dsm, int cap) {
+    Scratch S;
+    double* v = dsm + cap;
+    int* I = reinterpret_cast<int*>(dsm + 11 * cap);
+    S.z = v; S.ds = v + cap; S.zs = v + 2 * cap; S.dd = v + 3 * cap; S.zz = v + 4 * cap;
+    S.tau = v + 5 * cap; S.zh = v + 6 * cap; S.vals = v + 7 * cap; S.rc = v + 8 * cap; S.rs = v + 9 * cap;
+    S.perm = I; S.nd = I + cap; S.df = I + 2 * cap; S.org = I + 3 * cap; S.pos = I + 4 * cap;
+    S.ra = I + 5 * cap; S.rb = I + 6 * cap; S.mk = I + 7 * cap; S.mr = I + 8 * cap; S.mf = I + 9 * cap;
+    return S;
+}
+
 // How the O(K) sums of one secular root, one zhat entry or one rank-one eigenvector are
 // split: one thread runs the whole sum, or the 32 lanes of a warp take every 32nd term
 // and combine them with a butterfly (every lane ends with the same value).
@@ -248,15 +264,18 @@ __device__ void merge_prep(G g, int a, int mid, int b, int n, double* Z, const d
         int K = 0, ndf = 0, nrot = 0, jlam = -1;
         double* ds = S.ds + a;
         double* zs = S.zs + a;
+        double zl = 0.0, dl = 0.0;   // z and d of the pending entry jlam
         for (int j = 0; j < nn; ++j) {
-            if (rho * fabs(zs[j]) <= tol) { S.df[a + ndf++] = j; continue; }
-            if (jlam < 0) { jlam = j; continue; }
-            double s_ = zs[jlam], c_ = zs[j];
-            const double tau = hypot(c_, s_);
-            const double tt = ds[j] - ds[jlam];
-            c_ /= tau;
-            s_ = -s_ / tau;
-            if (fabs(tt * c_ * s_) <= tol) {
+            const double zj = zs[j], dj = ds[j];
+            if (rho * fabs(zj) <= tol) { S.df[a + ndf++] = j; continue; }
+            if (jlam < 0) { jlam = j; zl = zj; dl = dj; continue; }
+            // close poles: |(d_j - d_l) c s| <= tol with c = z_j / tau, s = -z_l / tau,
+            // tau^2 = z_j^2 + z_l^2, tested without the square root and the divisions
+            // (the rotation itself is rare)
+            const double tt = dj - dl;
+            if (fabs(tt) * fabs(zj * zl) <= tol * fma(zj, zj, zl * zl)) {
+                const double tau = hypot(zj, zl);
+                const double c_ = zj / tau, s_ = -zl / tau;
                 zs[j] = tau;
                 zs[jlam] = 0.0;
                 S.ra[a + nrot] = S.perm[a + jlam];
@@ -264,14 +283,19 @@ __device__ void merge_prep(G g, int a, int mid, int b, int n, double* Z, const d
                 S.rc[a + nrot] = c_;
                 S.rs[a + nrot] = s_;
                 ++nrot;
-                const double tn = ds[jlam] * c_ * c_ + ds[j] * s_ * s_;
-                ds[j] = ds[jlam] * s_ * s_ + ds[j] * c_ * c_;
+                const double tn = dl * c_ * c_ + dj * s_ * s_;
+                const double dn = dl * s_ * s_ + dj * c_ * c_;
+                ds[j] = dn;
                 ds[jlam] = tn;
                 S.df[a + ndf++] = jlam;
                 jlam = j;
+                zl = tau;
+                dl = dn;
             } else {
                 S.nd[a + K++] = jlam;
                 jlam = j;
+                zl = zj;
+                dl = dj;
             }
         }
         if (jlam >= 0) S.nd[a + K++] = jlam;

@@ -31,6 +31,7 @@ constexpr int DC_LOW = 128;   // merges of up to this many rows run inside one b
 constexpr int TPB = 256;
 constexpr int CB = 32;        // columns per block in the symmetric matrix-vector product
 constexpr int kTriCL = 8;     // blocks per cluster of the one-launch tridiagonalisation
+constexpr int kDcGsz = 16 * (4 * (512 / 16) + 1) + 16 * 65;   // in-block GEMM staging of k_dc_low
 
 struct LSec {
     long long a_off, e_off, w_off, i_off;
@@ -551,9 +552,17 @@ __global__ void __launch_bounds__(512) k_dc_low(const LSec* __restrict__ secs, i
     if (sidx >= nsec) return;
     LView L = lview(secs[sidx], eigbuf, wsd, wsi);
     const int n = L.n, tid = threadIdx.x, T = blockDim.x;
-    const int c0 = bid * DC_LOW, c1 = min(c0 + DC_LOW, n);
+    const int c0 = bid * DC_LOW, c1 = min(c0 + DC_LOW, n), nl = c1 - c0;
     double* red = sm;
     double* gsm = sm + 32;
+    // D of the range and the merge vectors in shared memory; the merges work in indices
+    // local to the range (Z, U, Qt through pointers to the range's diagonal block)
+    double* Dl = gsm + kDcGsz;
+    const Scratch Sl = scratch_smem(Dl, DC_LOW);
+    double* Zl = L.Z + c0 + (size_t)c0 * n;
+    double* Ul = L.U + c0 + (size_t)c0 * n;
+    double* Ql = L.Qt + c0 + (size_t)c0 * n;
+    const double* El = L.E + c0;
     // columns c0 .. c1-1 of Z start as the identity
     const long long ne = (long long)n * (c1 - c0);
     for (long long e = tid; e < ne; e += T) {
@@ -565,25 +574,27 @@ __global__ void __launch_bounds__(512) k_dc_low(const LSec* __restrict__ secs, i
         double dv = L.D[i];
         if (i > 0) dv -= fabs(L.E[i - 1]);
         if (i < n - 1) dv -= fabs(L.E[i]);
-        L.D[i] = dv;
+        Dl[i - c0] = dv;
     }
     __syncthreads();
     const int warp = tid >> 5, lane = tid & 31, nwarps = T >> 5;
-    for (int s = 1; 2 * s <= DC_LOW && c0 + s < c1; s *= 2) {
+    for (int s = 1; 2 * s <= DC_LOW && s < nl; s *= 2) {
         if (2 * s <= 32) {
             WarpG wg{lane};
             int mi = 0;
-            for (int a = c0; a + s < c1; a += 2 * s, ++mi) {
+            for (int a = 0; a + s < nl; a += 2 * s, ++mi) {
                 if (mi % nwarps != warp) continue;
-                dc_merge(wg, a, a + s, min(a + 2 * s, c1), n, L.Z, L.D, L.E, L.S, L.U, L.Qt, red, gsm, status);
+                dc_merge(wg, a, a + s, min(a + 2 * s, nl), n, Zl, Dl, El, Sl, Ul, Ql, red, gsm, status);
             }
             __syncthreads();
         } else {
             BlockG bg;
-            for (int a = c0; a + s < c1; a += 2 * s)
-                dc_merge(bg, a, a + s, min(a + 2 * s, c1), n, L.Z, L.D, L.E, L.S, L.U, L.Qt, red, gsm, status);
+            for (int a = 0; a + s < nl; a += 2 * s)
+                dc_merge(bg, a, a + s, min(a + 2 * s, nl), n, Zl, Dl, El, Sl, Ul, Ql, red, gsm, status);
         }
     }
+    __syncthreads();
+    for (int i = tid; i < nl; i += T) L.D[c0 + i] = Dl[i];
 }
 
 struct Merge {
@@ -955,7 +966,7 @@ static int tri_cluster(nrg_context* ctx, const LSec* dsec, int ns, int maxn, dou
     }
 }
 
-int syev_large(nrg_context* ctx, const std::vector<SyevSector>& in, double* d_V, double* d_E) {
+int syev_large(nrg_context* ctx, const std::vector<SyevSector>& in, double* d_V, double* d_E, int slot_base) {
     const int ns = (int)in.size();
     if (ns == 0) return NRG_OK;
     cudaStream_t st = ctx->stream;
@@ -973,11 +984,12 @@ int syev_large(nrg_context* ctx, const std::vector<SyevSector>& in, double* d_V,
         wi += lws_ints(in[s].n);
         maxn = std::max(maxn, in[s].n);
     }
-    DevBuf& bsec = ctx->scratch.b[24];
-    DevBuf& bwd = ctx->scratch.b[25];
-    DevBuf& bwi = ctx->scratch.b[26];
-    DevBuf& bidx = ctx->scratch.b[27];
-    DevBuf& bmrg = ctx->scratch.b[28];
+    DevBuf& bsec = ctx->scratch.b[slot_base];
+    DevBuf& bwd = ctx->scratch.b[slot_base + 1];
+    DevBuf& bwi = ctx->scratch.b[slot_base + 2];
+    DevBuf& bidx = ctx->scratch.b[slot_base + 3];
+    DevBuf& bmrg = ctx->scratch.b[slot_base + 4];
+    const int gslot = slot_base + 5;   // grouped GEMM problem lists (two slots)
     NRG_TRY(bsec.ensure(sizeof(LSec) * ns));
     NRG_TRY(bwd.ensure(sizeof(double) * (size_t)wd));
     NRG_TRY(bwi.ensure(sizeof(int) * (size_t)wi));
@@ -1012,19 +1024,17 @@ int syev_large(nrg_context* ctx, const std::vector<SyevSector>& in, double* d_V,
     NRG_TRY(tri_cluster(ctx, dsec, ns, maxn, d_V, wsd, wsi, &clustered));
     if (ctx->profiling) {
         NRG_CUDA_TRY(cudaEventRecord(te[1], st));
-        NRG_CUDA_TRY(cudaEventSynchronize(te[1]));
-        float ms = 0.f;
-        NRG_CUDA_TRY(cudaEventElapsedTime(&ms, te[0], te[1]));
-        cudaEventDestroy(te[0]);
-        cudaEventDestroy(te[1]);
         if (clustered) {
-            ctx->tri_launches++;
-            ctx->tri_ms += ms;
+            nrg_context::PendingTimer t{te[0], te[1], 0.0, 0.0};
             for (int x = 0; x < ns; ++x) {
                 const double n = secs[x].n;
-                ctx->tri_flops += 4.0 / 3.0 * n * n * n;
-                ctx->tri_bytes += 8.0 * n * n * n / 3.0;
+                t.flops += 4.0 / 3.0 * n * n * n;
+                t.bytes += 8.0 * n * n * n / 3.0;
             }
+            ctx->pending_tri.push_back(t);
+        } else {
+            cudaEventDestroy(te[0]);
+            cudaEventDestroy(te[1]);
         }
     }
     for (int p = 0; !clustered && p < maxn - 1; p += NB) {
@@ -1058,7 +1068,7 @@ int syev_large(nrg_context* ctx, const std::vector<SyevSector>& in, double* d_V,
             P.C = d_V + secs[s].a_off + r0 + (long long)r0 * n; P.c_si = 1; P.c_sj = n;
             probs.push_back(P);
         }
-        NRG_TRY(launch_ggemm(ctx, probs, 29));
+        NRG_TRY(launch_ggemm(ctx, probs, gslot));
     }
     if (!clustered) {
         k_tri_end<<<ns, 32, 0, st>>>(dsec, d_V, wsd, wsi);
@@ -1067,8 +1077,7 @@ int syev_large(nrg_context* ctx, const std::vector<SyevSector>& in, double* d_V,
 
     // ---- 2. divide and conquer ----
     {
-        const int gsz = 16 * (4 * (512 / 16) + 1) + 16 * 65;
-        const size_t smem = sizeof(double) * (32 + gsz);
+        const size_t smem = sizeof(double) * (32 + kDcGsz + kDcSmemDoubles * DC_LOW);
         int nchunk = 0;
         for (int x = 0; x < ns; ++x) nchunk += (secs[x].n + DC_LOW - 1) / DC_LOW;
         k_dc_low<<<nchunk, 512, smem, st>>>(dsec, ns, d_V, wsd, wsi, ctx->d_status.as<int>());
@@ -1124,7 +1133,7 @@ int syev_large(nrg_context* ctx, const std::vector<SyevSector>& in, double* d_V,
             P.C = W + 2 * sq + m.a; P.c_si = 1; P.c_sj = n; P.c_ji = I + 6LL * n + m.a;  // Qt(:, a+pos[j])
             probs.push_back(P);
         }
-        NRG_TRY(launch_ggemm(ctx, probs, 29));
+        NRG_TRY(launch_ggemm(ctx, probs, gslot));
         k_dc_phase<<<blk[kMapWide], TPB, 0, st>>>(dsec, dms, nm, 5, d_V, wsd, wsi, ctx->d_status.as<int>());
         k_dc_phase<<<blk[kMapWide], TPB, 0, st>>>(dsec, dms, nm, 6, d_V, wsd, wsi, ctx->d_status.as<int>());
         ctx->launches += 2;
@@ -1195,7 +1204,7 @@ int syev_large(nrg_context* ctx, const std::vector<SyevSector>& in, double* d_V,
             Q.C = G + 2 * NBB * NBB; Q.c_si = 1; Q.c_sj = b;            // Wt (b x n)
             g1.push_back(Q);
         }
-        NRG_TRY(launch_ggemm(ctx, g1, 29));
+        NRG_TRY(launch_ggemm(ctx, g1, gslot));
         k_bt_tfactor<<<ns, NBB, tf_smem, st>>>(dsec, q, d_V, wsd, wsi);
         ctx->launches++;
         std::vector<GemmProblem> g2, g3;
@@ -1223,8 +1232,8 @@ int syev_large(nrg_context* ctx, const std::vector<SyevSector>& in, double* d_V,
             Q.C = W + r0; Q.c_si = 1; Q.c_sj = n;
             g3.push_back(Q);
         }
-        NRG_TRY(launch_ggemm(ctx, g2, 29));
-        NRG_TRY(launch_ggemm(ctx, g3, 29));
+        NRG_TRY(launch_ggemm(ctx, g2, gslot));
+        NRG_TRY(launch_ggemm(ctx, g3, gslot));
     }
     k_large_out<<<dim3(32, ns), TPB, 0, st>>>(dsec, d_V, d_E, wsd, wsi);
     ctx->launches++;

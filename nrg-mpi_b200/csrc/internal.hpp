@@ -121,6 +121,14 @@ struct nrg_context {
     // the large-sector pipeline (fork / join events on the caller's stream)
     cudaStream_t aux = nullptr;
     cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+    // third stream: the large sectors below the largest size class run their pipeline
+    // beside the largest sectors' (whose tridiagonalisation sets the critical path)
+    cudaStream_t aux2 = nullptr, aux_hi = nullptr;   // aux_hi: greatest priority, the largest sectors
+    cudaEvent_t ev_join2 = nullptr, ev_join_hi = nullptr;
+    // tridiagonalisation timers (profiling on), read once the eigensolver has joined so
+    // that timing does not stall the launch queue
+    struct PendingTimer { cudaEvent_t a, b; double flops, bytes; };
+    std::vector<PendingTimer> pending_tri;
     nrg::DevBuf& slot(size_t i) {
         if (store.size() <= i) store.resize(i + 1);
         return store[i];
@@ -158,7 +166,8 @@ int launch_ggemm(nrg_context* ctx, std::vector<GemmProblem>& probs, int scratch_
 
 // eigensolver for sectors of order > 128 across the whole GPU (eig_large.cu); the
 // descriptors use a_off / e_off / n only
-int syev_large(nrg_context* ctx, const std::vector<SyevSector>& secs, double* d_V, double* d_E);
+// (scratch slots slot_base .. slot_base + 6; on ctx->stream)
+int syev_large(nrg_context* ctx, const std::vector<SyevSector>& secs, double* d_V, double* d_E, int slot_base);
 constexpr int kLargeSector = 128;
 
 // ---- kernels (kernels.cu) ------------------------------------------------------------

@@ -288,26 +288,58 @@ int diag_device(nrg_context* ctx, int iteration, Sectors& S, const double* d_Eol
         NRG_CUDA_TRY(cudaEventCreate(&e1));
         NRG_CUDA_TRY(cudaEventRecord(e0, ctx->stream));
     }
-    // sectors of order <= 128: one block each, on the second stream when large sectors
-    // run beside them; larger ones: the multi-kernel pipeline on the caller's stream
-    const bool fork = nsec > nlarge && nlarge > 0;
-    if (fork) {
+    // Three independent groups: the largest large sectors (order >= 4/5 of the largest)
+    // on a stream of the greatest priority, the other sectors of order > 128 on a third
+    // stream, and the sectors of order <= 128 (one block each) on the second stream.  The
+    // largest sectors' pipeline sets the critical path; the blocks of the other groups
+    // fill the SMs it leaves idle.
+    std::vector<SyevSector> g1, g2;
+    for (const auto& q : large) (5 * q.n >= 4 * large[0].n ? g1 : g2).push_back(q);
+    const bool fork_small = nsec > nlarge && nlarge > 0;
+    const bool fork_large = !g2.empty();
+    if (fork_small || fork_large) {
         if (!ctx->aux) {
+            int lo = 0, hi = 0;
+            NRG_CUDA_TRY(cudaDeviceGetStreamPriorityRange(&lo, &hi));
             NRG_CUDA_TRY(cudaStreamCreateWithFlags(&ctx->aux, cudaStreamNonBlocking));
+            NRG_CUDA_TRY(cudaStreamCreateWithFlags(&ctx->aux2, cudaStreamNonBlocking));
+            NRG_CUDA_TRY(cudaStreamCreateWithPriority(&ctx->aux_hi, cudaStreamNonBlocking, hi));
             NRG_CUDA_TRY(cudaEventCreateWithFlags(&ctx->ev_fork, cudaEventDisableTiming));
             NRG_CUDA_TRY(cudaEventCreateWithFlags(&ctx->ev_join, cudaEventDisableTiming));
+            NRG_CUDA_TRY(cudaEventCreateWithFlags(&ctx->ev_join2, cudaEventDisableTiming));
+            NRG_CUDA_TRY(cudaEventCreateWithFlags(&ctx->ev_join_hi, cudaEventDisableTiming));
         }
         NRG_CUDA_TRY(cudaEventRecord(ctx->ev_fork, ctx->stream));
-        NRG_CUDA_TRY(cudaStreamWaitEvent(ctx->aux, ctx->ev_fork, 0));
     }
-    if (nsec > nlarge) {
-        NRG_TRY(launch_syev(bsec.as<SyevSector>() + nlarge, nsec - nlarge, max_n, d_V, d_E, bwd.as<double>(),
-                            bwi.as<int>(), ctx->d_status.as<int>(), fork ? ctx->aux : ctx->stream));
+    int rl = NRG_OK;
+    if (fork_large) {
+        NRG_CUDA_TRY(cudaStreamWaitEvent(ctx->aux_hi, ctx->ev_fork, 0));
+        cudaStream_t caller = ctx->stream;
+        ctx->stream = ctx->aux_hi;
+        rl = syev_large(ctx, g1, d_V, d_E, 24);
+        ctx->stream = caller;
+        NRG_CUDA_TRY(cudaEventRecord(ctx->ev_join_hi, ctx->aux_hi));
+    } else {
+        rl = syev_large(ctx, g1, d_V, d_E, 24);
+    }
+    if (fork_small) NRG_CUDA_TRY(cudaStreamWaitEvent(ctx->aux, ctx->ev_fork, 0));
+    if (nsec > nlarge && rl == NRG_OK) {
+        rl = launch_syev(bsec.as<SyevSector>() + nlarge, nsec - nlarge, max_n, d_V, d_E, bwd.as<double>(),
+                         bwi.as<int>(), ctx->d_status.as<int>(), fork_small ? ctx->aux : ctx->stream);
         ctx->launches++;
     }
-    if (fork) NRG_CUDA_TRY(cudaEventRecord(ctx->ev_join, ctx->aux));
-    const int rl = syev_large(ctx, large, d_V, d_E);
-    if (fork) NRG_CUDA_TRY(cudaStreamWaitEvent(ctx->stream, ctx->ev_join, 0));
+    if (fork_small) NRG_CUDA_TRY(cudaEventRecord(ctx->ev_join, ctx->aux));
+    if (fork_large) {
+        NRG_CUDA_TRY(cudaStreamWaitEvent(ctx->aux2, ctx->ev_fork, 0));
+        cudaStream_t caller = ctx->stream;
+        ctx->stream = ctx->aux2;
+        if (rl == NRG_OK) rl = syev_large(ctx, g2, d_V, d_E, 31);
+        ctx->stream = caller;
+        NRG_CUDA_TRY(cudaEventRecord(ctx->ev_join2, ctx->aux2));
+        NRG_CUDA_TRY(cudaStreamWaitEvent(ctx->stream, ctx->ev_join2, 0));
+        NRG_CUDA_TRY(cudaStreamWaitEvent(ctx->stream, ctx->ev_join_hi, 0));
+    }
+    if (fork_small) NRG_CUDA_TRY(cudaStreamWaitEvent(ctx->stream, ctx->ev_join, 0));
     NRG_TRY(rl);
     if (ctx->profiling) {
         NRG_CUDA_TRY(cudaEventRecord(e1, ctx->stream));
@@ -318,6 +350,17 @@ int diag_device(nrg_context* ctx, int iteration, Sectors& S, const double* d_Eol
         cudaEventDestroy(e1);
         ctx->syev_ms += ms;
         ctx->syev_launches++;
+        for (auto& t : ctx->pending_tri) {
+            float tm = 0.f;
+            NRG_CUDA_TRY(cudaEventElapsedTime(&tm, t.a, t.b));
+            cudaEventDestroy(t.a);
+            cudaEventDestroy(t.b);
+            ctx->tri_launches++;
+            ctx->tri_ms += tm;
+            ctx->tri_flops += t.flops;
+            ctx->tri_bytes += t.bytes;
+        }
+        ctx->pending_tri.clear();
         double f = 0.0;
         for (int s = 0; s < nsec; ++s) f += (4.0 / 3.0 + 2.0) * double(S.dim[s]) * S.dim[s] * S.dim[s];
         ctx->syev_flops += f;
