@@ -178,8 +178,7 @@ __global__ void __launch_bounds__(kThreads) k_syev(const SyevSector* __restrict_
 
     double* red = sm;
     double* gsm = sm + 32;
-    const int gsz = 16 * (4 * (T / 16) + 1) + 16 * 65;
-    double* vs = sm + 32 + gsz;
+    double* vs = sm + 32 + nrg::kCtaGemmSmem;
     const int vlen = n > kNB * kNB ? n : kNB * kNB;
     double* ps = vs + vlen;
     double* dcs = vs + 2 * vlen + kNB * kNB;          // D and the merge vectors (orders <= kDcCap)
@@ -243,10 +242,9 @@ __global__ void __launch_bounds__(kThreads) k_syev(const SyevSector* __restrict_
 int launch_syev(const SyevSector* d_secs, int nsec, int max_n, double* eigbuf, double* evals,
                 double* wsd, int* wsi, int* d_status, cudaStream_t st) {
     if (nsec == 0) return NRG_OK;
-    const int gsz = 16 * (4 * (kThreads / 16) + 1) + 16 * 65;
     const size_t vlen = (size_t)(max_n > kNB * kNB ? max_n : kNB * kNB);
     const int smem_tri = max_n <= kSmemTri ? 1 : 0;
-    size_t smem = sizeof(double) * (32 + gsz + 2 * vlen + kNB * kNB + kDcSmemDoubles * kDcCap +
+    size_t smem = sizeof(double) * (32 + nrg::kCtaGemmSmem + 2 * vlen + kNB * kNB + kDcSmemDoubles * kDcCap +
                                     (smem_tri ? (size_t)max_n * max_n : 0));
     if (smem > 227 * 1024) {
         nrg_set_error_message("sector of order %d exceeds the shared-memory plan", max_n);

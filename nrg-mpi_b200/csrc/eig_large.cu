@@ -31,7 +31,6 @@ constexpr int DC_LOW = 128;   // merges of up to this many rows run inside one b
 constexpr int TPB = 256;
 constexpr int CB = 32;        // columns per block in the symmetric matrix-vector product
 constexpr int kTriCL = 8;     // blocks per cluster of the one-launch tridiagonalisation
-constexpr int kDcGsz = 16 * (4 * (512 / 16) + 1) + 16 * 65;   // in-block GEMM staging of k_dc_low
 
 struct LSec {
     long long a_off, e_off, w_off, i_off;
@@ -557,7 +556,7 @@ __global__ void __launch_bounds__(512) k_dc_low(const LSec* __restrict__ secs, i
     double* gsm = sm + 32;
     // D of the range and the merge vectors in shared memory; the merges work in indices
     // local to the range (Z, U, Qt through pointers to the range's diagonal block)
-    double* Dl = gsm + kDcGsz;
+    double* Dl = gsm + nrg::kCtaGemmSmem;
     const Scratch Sl = scratch_smem(Dl, DC_LOW);
     double* Zl = L.Z + c0 + (size_t)c0 * n;
     double* Ul = L.U + c0 + (size_t)c0 * n;
@@ -1077,7 +1076,7 @@ int syev_large(nrg_context* ctx, const std::vector<SyevSector>& in, double* d_V,
 
     // ---- 2. divide and conquer ----
     {
-        const size_t smem = sizeof(double) * (32 + kDcGsz + kDcSmemDoubles * DC_LOW);
+        const size_t smem = sizeof(double) * (32 + nrg::kCtaGemmSmem + kDcSmemDoubles * DC_LOW);
         int nchunk = 0;
         for (int x = 0; x < ns; ++x) nchunk += (secs[x].n + DC_LOW - 1) / DC_LOW;
         k_dc_low<<<nchunk, 512, smem, st>>>(dsec, ns, d_V, wsd, wsi, ctx->d_status.as<int>());
