@@ -118,6 +118,11 @@ typedef struct nrg_stats {
 NRG_API int nrg_context_get_stats(const nrg_context* ctx, nrg_stats* out);
 NRG_API int nrg_context_reset_stats(nrg_context* ctx);
 NRG_API int nrg_context_set_profiling(nrg_context* ctx, int on);
+/* Frees the device and pinned host storage a context keeps between runs (eigenvector
+ * store, invariant matrices, workspaces); the model stays set and the next run
+ * allocates again.  (No reference counterpart: the reference deallocates its module
+ * arrays when the program ends.) */
+NRG_API int nrg_context_release_storage(nrg_context* ctx);
 NRG_API const char* nrg_last_error(void);
 NRG_API const char* nrg_status_string(int status);
 NRG_API int nrg_version(void);
@@ -284,6 +289,23 @@ typedef struct nrg_run_output {
                                              (device events)                            */
 } nrg_run_output;
 NRG_API int nrg_run(nrg_context* ctx, const nrg_run_input* in, nrg_run_output* out);
+
+/* ---- many independent impurity instances on one device ------------------------------
+ * The reference runs one impurity per MPI job; loadbalance.F90:102-186
+ * (loadbalanceDiagonalization2) spreads the sectors of one iteration over the ranks by a
+ * greedy d^3 cost.  On one B200 a single instance leaves most SMs idle (its work is a
+ * chain of latency-bound sector solves), so independent instances (parameter sweeps)
+ * run side by side: count instances, each a context with its model set (distinct
+ * contexts, all on one device), as nrg_run calls on up to `concurrency` host threads
+ * (concurrency < 1: one per instance), each instance on its own CUDA stream (a context
+ * whose stream is NULL gets a non-blocking stream for the call).  Instances start in
+ * array order; callers sort them by estimated cost, largest first.  statuses[i]
+ * (optional) receives each instance's status; the return value is the status of the
+ * first failing instance (all instances run to the end), or NRG_OK. */
+#define NRG_BATCH_RELEASE 1   /* flags: release each context's storage when its instance ends,
+                                 so that device memory holds only the instances in flight */
+NRG_API int nrg_run_batch(nrg_context* const* ctxs, const nrg_run_input* in, nrg_run_output* out,
+                          int32_t count, int32_t concurrency, int32_t flags, int32_t* statuses);
 
 #ifdef __cplusplus
 }

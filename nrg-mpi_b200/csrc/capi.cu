@@ -275,6 +275,20 @@ int nrg_host_free(void* p) {
     return NRG_OK;
 }
 
+int nrg_context_release_storage(nrg_context* ctx) {
+    if (!ctx) return NRG_ERR_INVALID;
+    NRG_CUDA_TRY(cudaSetDevice(ctx->device));
+    NRG_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+    for (auto& b : ctx->store) b.release();
+    ctx->store.clear();
+    for (auto& b : ctx->host_store) b.release();
+    ctx->host_store.clear();
+    for (auto& b : ctx->scratch.b) b.release();
+    for (auto& s : ctx->iter_sectors) { s.d_bi.release(); s.d_lst.release(); s.d_lstOff.release(); }
+    ctx->iter_sectors.clear();
+    return NRG_OK;
+}
+
 int nrg_context_set_profiling(nrg_context* ctx, int on) {
     if (!ctx) return NRG_ERR_INVALID;
     ctx->profiling = on != 0;

@@ -13,9 +13,13 @@
 #include "internal.hpp"
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstring>
+#include <mutex>
 #include <numeric>
+#include <string>
+#include <thread>
 #include <vector>
 
 using namespace nrg;
@@ -597,9 +601,91 @@ int run_drop_in(nrg_context* ctx, const nrg_run_input* in, nrg_run_output* out, 
     return NRG_OK;
 }
 
+int run_one(nrg_context* ctx, const nrg_run_input* in, nrg_run_output* out);
+
 }  // namespace
 
 extern "C" int nrg_run(nrg_context* ctx, const nrg_run_input* in, nrg_run_output* out) {
+    return run_one(ctx, in, out);
+}
+
+extern "C" int nrg_run_batch(nrg_context* const* ctxs, const nrg_run_input* in, nrg_run_output* out,
+                             int32_t count, int32_t concurrency, int32_t flags, int32_t* statuses) {
+    if (count < 0 || (count > 0 && (!ctxs || !in || !out))) {
+        nrg_set_error_message("nrg_run_batch: NULL arrays or negative count");
+        return NRG_ERR_INVALID;
+    }
+    for (int i = 0; i < count; ++i)
+        for (int j = 0; j < i; ++j)
+            if (ctxs[i] == ctxs[j]) {
+                nrg_set_error_message("nrg_run_batch: instance %d repeats the context of instance %d", i, j);
+                return NRG_ERR_INVALID;
+            }
+    const int nthr = std::max(1, std::min<int>(concurrency < 1 ? count : concurrency, count));
+    std::vector<int> st(count, NRG_OK);
+    std::atomic<int> next{0};
+    std::mutex mu;
+    int first_bad = -1;
+    std::string first_msg;
+    auto worker = [&]() {
+        for (;;) {
+            const int i = next.fetch_add(1);
+            if (i >= count) return;
+            nrg_context* c = ctxs[i];
+            int rc = NRG_OK;
+            cudaStream_t own = nullptr;
+            if (!c) {
+                nrg_set_error_message("nrg_run_batch: instance %d has no context", i);
+                rc = NRG_ERR_INVALID;
+            } else if (cudaSetDevice(c->device) != cudaSuccess) {
+                cudaGetLastError();
+                nrg_set_error_message("nrg_run_batch: cudaSetDevice(%d) failed", c->device);
+                rc = NRG_ERR_CUDA;
+            } else if (!c->stream) {
+                // the legacy default stream would serialise the instances
+                if (cudaStreamCreateWithFlags(&own, cudaStreamNonBlocking) != cudaSuccess) {
+                    cudaGetLastError();
+                    nrg_set_error_message("nrg_run_batch: stream creation failed");
+                    rc = NRG_ERR_CUDA;
+                } else {
+                    c->stream = own;
+                }
+            }
+            if (rc == NRG_OK) rc = run_one(c, in + i, out + i);
+            if (c && (flags & NRG_BATCH_RELEASE)) {
+                const int rr = nrg_context_release_storage(c);
+                if (rc == NRG_OK) rc = rr;
+            }
+            if (own) {
+                cudaStreamSynchronize(own);
+                c->stream = nullptr;
+                cudaStreamDestroy(own);
+            }
+            st[i] = rc;
+            if (rc != NRG_OK) {
+                std::lock_guard<std::mutex> lk(mu);
+                if (first_bad < 0 || i < first_bad) {
+                    first_bad = i;
+                    first_msg = nrg_last_error();
+                }
+            }
+        }
+    };
+    std::vector<std::thread> pool;
+    for (int t = 1; t < nthr; ++t) pool.emplace_back(worker);
+    worker();
+    for (auto& t : pool) t.join();
+    if (statuses)
+        for (int i = 0; i < count; ++i) statuses[i] = st[i];
+    if (first_bad >= 0) {
+        nrg_set_error_message("instance %d: %s", first_bad, first_msg.c_str());
+        return st[first_bad];
+    }
+    return NRG_OK;
+}
+
+namespace {
+int run_one(nrg_context* ctx, const nrg_run_input* in, nrg_run_output* out) {
     if (!ctx || !in) return NRG_ERR_INVALID;
     if (!ctx->model.set) { nrg_set_error_message("nrg_context_set_model has not been called"); return NRG_ERR_STATE; }
     NRG_CUDA_TRY(cudaSetDevice(ctx->device));
@@ -620,3 +706,4 @@ extern "C" int nrg_run(nrg_context* ctx, const nrg_run_input* in, nrg_run_output
     for (auto& e : ev) cudaEventDestroy(e);
     return rc;
 }
+}  // namespace

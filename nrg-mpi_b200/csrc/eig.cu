@@ -14,6 +14,7 @@
 // Eigenvalues come out ascending with their eigenvectors in the same column order, as
 // dsyev returns them.
 #include "eig_common.cuh"
+#include "internal.hpp"
 
 namespace {
 
@@ -250,11 +251,7 @@ int launch_syev(const SyevSector* d_secs, int nsec, int max_n, double* eigbuf, d
         nrg_set_error_message("sector of order %d exceeds the shared-memory plan", max_n);
         return NRG_ERR_TOO_LARGE;
     }
-    static size_t configured = 0;
-    if (smem > 48 * 1024 && smem > configured) {
-        NRG_CUDA_TRY(cudaFuncSetAttribute(k_syev, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        configured = smem;
-    }
+    if (smem > 48 * 1024) NRG_TRY(nrg::raise_smem_limit((const void*)k_syev, smem));
     k_syev<<<nsec, kThreads, smem, st>>>(d_secs, eigbuf, evals, wsd, wsi, d_status, smem_tri);
     NRG_CUDA_TRY(cudaGetLastError());
     return NRG_OK;

@@ -922,7 +922,7 @@ static int tri_cluster_cl(nrg_context* ctx, const LSec* dsec, int ns, int maxn, 
     NRG_CUDA_TRY(cudaGetDevice(&dev));
     NRG_CUDA_TRY(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
     if (smem > (size_t)optin) return NRG_OK;
-    NRG_CUDA_TRY(cudaFuncSetAttribute(k_tri_cluster<CL>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    NRG_TRY(raise_smem_limit((const void*)k_tri_cluster<CL>, smem));
     if (CL > 8) NRG_CUDA_TRY(cudaFuncSetAttribute(k_tri_cluster<CL>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3((unsigned)(CL * ns));
@@ -1010,7 +1010,7 @@ int syev_large(nrg_context* ctx, const std::vector<SyevSector>& in, double* d_V,
     const int* didx = bidx.as<int>();
     const size_t symv_smem = sizeof(double) * (size_t)maxn;
     if (symv_smem > 48 * 1024)
-        NRG_CUDA_TRY(cudaFuncSetAttribute(k_tri_symv, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)symv_smem));
+        NRG_TRY(raise_smem_limit((const void*)k_tri_symv, symv_smem));
 
     // ---- 1. tridiagonalisation ----
     bool clustered = false;
@@ -1152,16 +1152,16 @@ int syev_large(nrg_context* ctx, const std::vector<SyevSector>& in, double* d_V,
         const int cbk = apply_smem(16) <= (size_t)optin ? 16 : (apply_smem(8) <= (size_t)optin ? 8 : 0);
         if (cbk > 0) {
             const int npan = (maxn - 2) / NBB + 1;
-            NRG_CUDA_TRY(cudaFuncSetAttribute(k_bt_prep, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)prep_smem));
+            NRG_TRY(raise_smem_limit((const void*)k_bt_prep, prep_smem));
             k_bt_prep<<<dim3(npan, ns), 256, prep_smem, st>>>(dsec, d_V, wsd, wsi);
             int nblk = 0;
             for (int x = 0; x < ns; ++x) nblk += (secs[x].n + cbk - 1) / cbk;
             const size_t sm = apply_smem(cbk);
             if (cbk == 16) {
-                NRG_CUDA_TRY(cudaFuncSetAttribute(k_bt_apply<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+                NRG_TRY(raise_smem_limit((const void*)k_bt_apply<16>, sm));
                 k_bt_apply<16><<<nblk, 256, sm, st>>>(dsec, ns, d_V, d_E, wsd, wsi);
             } else {
-                NRG_CUDA_TRY(cudaFuncSetAttribute(k_bt_apply<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+                NRG_TRY(raise_smem_limit((const void*)k_bt_apply<8>, sm));
                 k_bt_apply<8><<<nblk, 256, sm, st>>>(dsec, ns, d_V, d_E, wsd, wsi);
             }
             ctx->launches += 2;
@@ -1172,7 +1172,7 @@ int syev_large(nrg_context* ctx, const std::vector<SyevSector>& in, double* d_V,
     // otherwise panels of NBB reflectors on grouped GEMMs, last panel first
     const int qmax = (maxn - 2) / NBB;   // panels cover reflectors 0 .. n-2
     const size_t tf_smem = sizeof(double) * 2 * NBB * NBB;
-    NRG_CUDA_TRY(cudaFuncSetAttribute(k_bt_tfactor, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tf_smem));
+    NRG_TRY(raise_smem_limit((const void*)k_bt_tfactor, tf_smem));
     for (int q = qmax; q >= 0; --q) {
         std::vector<int> act;
         for (int s = 0; s < ns; ++s)

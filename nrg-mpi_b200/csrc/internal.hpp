@@ -144,6 +144,11 @@ struct nrg_context {
 
 namespace nrg {
 
+// raises a kernel's dynamic shared-memory limit on the current device to at least bytes
+// and never lowers it: the attribute belongs to the kernel, not to a stream, and host
+// threads running independent contexts launch the same kernels with different sizes
+int raise_smem_limit(const void* func, size_t bytes);
+
 // stream-ordered upload of a small host array through the pinned staging ring (the host
 // array may be reused as soon as the call returns)
 int h2d_async(nrg_context* ctx, void* dst, const void* src, size_t bytes);

@@ -2,6 +2,9 @@
 // and the device-resident driver (driver.cu).
 #include "internal.hpp"
 
+#include <map>
+#include <mutex>
+
 #include <algorithm>
 #include <cmath>
 #include <cstring>
@@ -161,6 +164,20 @@ int Sectors::upload(nrg_context* ctx) {
     NRG_TRY(h2d_async(ctx, d_bi.p, bi.data(), sizeof(int) * bi.size()));
     NRG_TRY(h2d_async(ctx, d_lst.p, lst.data(), sizeof(int) * lst.size()));
     NRG_TRY(h2d_async(ctx, d_lstOff.p, lstOff.data(), sizeof(int) * lstOff.size()));
+    return NRG_OK;
+}
+
+int raise_smem_limit(const void* func, size_t bytes) {
+    static std::mutex mu;
+    static std::map<std::pair<const void*, int>, size_t> limit;
+    int dev = 0;
+    NRG_CUDA_TRY(cudaGetDevice(&dev));
+    std::lock_guard<std::mutex> lk(mu);
+    size_t& cur = limit[{func, dev}];
+    if (bytes > cur) {
+        NRG_CUDA_TRY(cudaFuncSetAttribute(func, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
+        cur = bytes;
+    }
     return NRG_OK;
 }
 

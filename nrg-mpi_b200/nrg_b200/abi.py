@@ -44,7 +44,7 @@ EXPORTS = [
     "nrg_invariant_matrix_for_spectrum_dgemm", "nrg_reduced_density_matrix",
     "nrg_spike_zero_temperature", "nrg_spike_cfs", "nrg_run", "nrg_context_get_stats",
     "nrg_context_reset_stats", "nrg_context_set_profiling", "nrg_block_eigh_noalloc",
-    "nrg_host_alloc", "nrg_host_free",
+    "nrg_host_alloc", "nrg_host_free", "nrg_run_batch", "nrg_context_release_storage",
 ]
 
 
@@ -172,6 +172,9 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
     lib.nrg_spike_zero_temperature.argtypes = [c_void_p, c_int32, POINTER(SpikeIO)]
     lib.nrg_spike_cfs.argtypes = [c_void_p, c_int32, POINTER(SpikeIO)]
     lib.nrg_run.argtypes = [c_void_p, POINTER(RunInput), POINTER(RunOutput)]
+    lib.nrg_run_batch.argtypes = [POINTER(c_void_p), POINTER(RunInput), POINTER(RunOutput), c_int32, c_int32,
+                                  c_int32, POINTER(c_int32)]
+    lib.nrg_context_release_storage.argtypes = [c_void_p]
     lib.nrg_context_get_stats.argtypes = [c_void_p, POINTER(Stats)]
     lib.nrg_context_reset_stats.argtypes = [c_void_p]
     lib.nrg_context_set_profiling.argtypes = [c_void_p, ctypes.c_int]
@@ -233,6 +236,10 @@ class Context:
 
     def set_stream(self, stream_handle: int):
         self._check(self.lib.nrg_context_set_stream(self._h, c_void_p(stream_handle)), "set_stream")
+
+    def release_storage(self):
+        """Frees the device storage kept between runs (the model stays set)."""
+        self._check(self.lib.nrg_context_release_storage(self._h), "release_storage")
 
     def set_profiling(self, on: bool = True):
         self._check(self.lib.nrg_context_set_profiling(self._h, int(bool(on))), "set_profiling")
@@ -440,38 +447,71 @@ class Context:
         ``host_drop_in=True`` drives every routine through its drop-in entry point with
         host arrays (the Fortran caller's data flow) instead of keeping state on the device.
         """
+        args = self._run_args(spectrum, flow_stride, final_capacity, host_drop_in)
+        self._check(self.lib.nrg_run(self._h, ctypes.byref(args["ri"]), ctypes.byref(args["ro"])), "nrg_run")
+        return self._run_result(args)
+
+    def _run_args(self, spectrum, flow_stride, final_capacity, host_drop_in):
+        """Input and output records of nrg_run for this context (arrays kept alive here)."""
         inp = self.inp
-        rs = inp.numberOfVariation + 3
         nb = inp.numberOfBasis
-        bo = _i32(inp.basis_output)
-        E = np.ascontiguousarray(inp.eigenvalue, dtype=np.float64)
-        im = _f64f(inp.invariant_matrix)
-        ims = _f64f(inp.invariant_matrix_spectrum) if inp.flag_spectrum else None
-        ri = RunInput(nb, _p(bo, c_int32), _p(E, c_double), _p(im, c_double), _p(ims, c_double),
-                      int(bool(spectrum)), int(bool(host_drop_in)))
+        a = dict(bo=_i32(inp.basis_output), E=np.ascontiguousarray(inp.eigenvalue, dtype=np.float64),
+                 im=_f64f(inp.invariant_matrix),
+                 ims=_f64f(inp.invariant_matrix_spectrum) if inp.flag_spectrum else None)
+        a["ri"] = RunInput(nb, _p(a["bo"], c_int32), _p(a["E"], c_double), _p(a["im"], c_double),
+                           _p(a["ims"], c_double), int(bool(spectrum)), int(bool(host_drop_in)))
         nit = inp.numberOfIteration - inp.indexOfFirstIteration + 1
         nmat = max(inp.numberOfMatrix, 1)
         nbin_cap = 20001
-        bp = np.zeros(2 * nbin_cap * nmat)
-        bn = np.zeros(2 * nbin_cap * nmat)
-        kept = np.zeros(nit, dtype=np.int32)
-        nfull = np.zeros(nit, dtype=np.int32)
-        gse = np.zeros(nit)
-        tr = np.full(inp.numberOfIteration + 1, np.nan)
-        flow = np.full(nit * flow_stride, np.nan)
-        fin = np.zeros(max(final_capacity, 1))
-        ph = np.zeros(4)
-        ro = RunOutput(0, _p(bp, c_double), _p(bn, c_double), bp.size, 0, _p(kept, c_int32),
-                       _p(nfull, c_int32), _p(gse, c_double), _p(tr, c_double), _p(flow, c_double),
-                       flow_stride, _p(fin, c_double), final_capacity, _p(ph, c_double))
-        self._check(self.lib.nrg_run(self._h, ctypes.byref(ri), ctypes.byref(ro)), "nrg_run")
+        a.update(bp=np.zeros(2 * nbin_cap * nmat), bn=np.zeros(2 * nbin_cap * nmat),
+                 kept=np.zeros(nit, dtype=np.int32), nfull=np.zeros(nit, dtype=np.int32),
+                 gse=np.zeros(nit), tr=np.full(inp.numberOfIteration + 1, np.nan),
+                 flow=np.full(nit * flow_stride, np.nan), fin=np.zeros(max(final_capacity, 1)),
+                 ph=np.zeros(4), nit=nit, nmat=nmat, spectrum=spectrum, flow_stride=flow_stride,
+                 final_capacity=final_capacity)
+        a["ro"] = RunOutput(0, _p(a["bp"], c_double), _p(a["bn"], c_double), a["bp"].size, 0,
+                            _p(a["kept"], c_int32), _p(a["nfull"], c_int32), _p(a["gse"], c_double),
+                            _p(a["tr"], c_double), _p(a["flow"], c_double), flow_stride,
+                            _p(a["fin"], c_double), final_capacity, _p(a["ph"], c_double))
+        return a
+
+    def _run_result(self, a):
+        ro, nmat = a["ro"], a["nmat"]
         nbin = ro.numberOfBin
-        if spectrum and inp.flag_spectrum and 2 * nbin * nmat > bp.size:
+        if a["spectrum"] and self.inp.flag_spectrum and 2 * nbin * nmat > a["bp"].size:
             raise NrgError(4, "nrg_run", f"bin buffers too small for {nbin} bins")
         nw = nbin * nmat
+        bp, bn = a["bp"], a["bn"]
         binPos = np.stack([bp[:nw], bp[nw:2 * nw]], axis=1)
         binNeg = np.stack([bn[:nw], bn[nw:2 * nw]], axis=1)
-        return dict(numberOfBin=nbin, binPos=binPos, binNeg=binNeg, kept=kept,
-                    numberOfBasisFull=nfull, groundStateEnergy=gse, rdmTrace=tr,
-                    flow=flow.reshape(nit, flow_stride), startTrancation=ro.startTrancation,
-                    finalEigenvalue=fin[:final_capacity], phaseSeconds=ph)
+        return dict(numberOfBin=nbin, binPos=binPos, binNeg=binNeg, kept=a["kept"],
+                    numberOfBasisFull=a["nfull"], groundStateEnergy=a["gse"], rdmTrace=a["tr"],
+                    flow=a["flow"].reshape(a["nit"], a["flow_stride"]), startTrancation=ro.startTrancation,
+                    finalEigenvalue=a["fin"][:a["final_capacity"]], phaseSeconds=a["ph"])
+
+
+def run_batch(contexts, spectrum: bool = True, concurrency: int = 0, flow_stride: int = 8,
+              release: bool = False):
+    """nrg_run_batch: independent instances (distinct contexts on one device) side by side.
+    ``release=True`` frees each context's run storage when its instance ends.
+
+    Returns (results, statuses): one result dict per context and the per-instance
+    statuses; raises NrgError when any instance failed (every instance still ran).
+    """
+    if not contexts:
+        return [], []
+    lib = contexts[0].lib
+    args = [c._run_args(spectrum, flow_stride, 0, False) for c in contexts]
+    n = len(contexts)
+    hs = (c_void_p * n)(*[c._h for c in contexts])
+    ris = (RunInput * n)(*[a["ri"] for a in args])
+    ros = (RunOutput * n)(*[a["ro"] for a in args])
+    st = np.zeros(n, dtype=np.int32)
+    rc = lib.nrg_run_batch(hs, ris, ros, n, int(concurrency), 1 if release else 0, _p(st, c_int32))
+    if rc != 0:
+        raise NrgError(rc, "nrg_run_batch", lib.nrg_last_error().decode(errors="replace"))
+    results = []
+    for i, (c, a) in enumerate(zip(contexts, args)):
+        a["ro"] = ros[i]
+        results.append(c._run_result(a))
+    return results, st.tolist()
