@@ -18,7 +18,13 @@ the backward reduced density matrices and the T=0 CFS spectrum on the reference'
   threads) on a bounded sample of the same sweep.
 * --impl reference: the oracle port timed per NRG iteration of the same sweep (steps are
   full-size iterations), rank 0 only.
-Multi-GPU: the path does not shard (one GPU per NRG instance), so N ranks run N replicas.
+* many_instance: independent impurity models side by side (nrg_run_batch): the 27 draws
+  with N_keep <= 1024 of the seeded 64-SIAM sweep (50 iterations each, T=0 CFS), run one
+  at a time and then 8 in flight; wall clock around each batch with the device
+  synchronised; with N ranks the instances are dealt to the ranks by the greedy cost
+  rule and the slowest rank's time counts.
+Multi-GPU: one NRG instance does not shard (one GPU per instance), so N ranks run N
+replicas of the headline workload; the many-instance sample is partitioned instead.
 """
 import argparse
 import json
@@ -51,6 +57,7 @@ def parse():
     p.add_argument("--impl", default="b200", choices=["b200", "reference"])
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-cpu", action="store_true")
+    p.add_argument("--no-many", action="store_true")
     # profiling helpers: a shorter sweep of the same model (not the headline workload)
     p.add_argument("--iterations", type=int, default=None)
     p.add_argument("--n-keep", type=int, default=None)
@@ -137,6 +144,43 @@ def fp64_peak_tflops(torch, device):
         best = min(best, s.elapsed_time(e) * 1e-3)
     del a, b
     return 2.0 * n ** 3 / best / 1e12
+
+
+def many_instance(torch, dev, rank, world, dist, concurrency=8):
+    """Independent instances side by side: the N_keep <= 1024 draws of the 64-SIAM sweep."""
+    from nrg_b200 import Context, run_batch, sweep
+    sample = [x for x in sweep.sweep_instances() if x.n_keep <= 1024]
+    share = sweep.rank_share(sample, rank, world)
+    ctxs = []
+    try:
+        for x in share:
+            c = Context(dev.index)
+            c.set_model(x.build())
+            ctxs.append(c)
+        run_batch(ctxs, spectrum=True, concurrency=concurrency)   # allocates every context's storage
+        times = {}
+        for conc in (1, concurrency):
+            if dist is not None:
+                dist.barrier()
+            torch.cuda.synchronize(dev)
+            t0 = time.perf_counter()
+            res, _ = run_batch(ctxs, spectrum=True, concurrency=conc)
+            torch.cuda.synchronize(dev)
+            dt = time.perf_counter() - t0
+            if dist is not None:
+                t = torch.tensor([dt], device=dev, dtype=torch.float64)
+                dist.all_reduce(t, op=dist.ReduceOp.MAX)
+                dt = float(t.item())
+            times[conc] = dt
+    finally:
+        for c in ctxs:
+            c.close()
+    its = sum(x.n_iterations for x in sample)
+    return {"workload": f"{len(sample)} SIAMs of the seeded 64-instance draw (seed {sweep.SWEEP_SEED}) with "
+                        "N_keep <= 1024, Lambda=2, 50 NRG iterations each + RDM + T=0 CFS spectrum",
+            "instances": len(sample), "iterations": its, "unit": "iterations/s",
+            "sequential": its / times[1], "batched": its / times[concurrency], "concurrency": concurrency,
+            "ranks": world, "timing": "wall clock around each batch, device synchronised, max over ranks"}
 
 
 def cpu_sample(n_timed=3):
@@ -285,6 +329,7 @@ def main():
                "path": "drop-in entry points with host arrays (Fortran caller's data flow; module "
                        "arrays in pinned host memory, allocated in one untimed warm-up run)",
                "max_bin_diff_vs_device_resident": same}
+    many = None if args.no_many else many_instance(torch, dev, rank, world, dist)
     if rank == 0:
         clocks = clk.summary()
         nbin = res["numberOfBin"]
@@ -322,6 +367,7 @@ def main():
             "clocks": clocks,
             "e2e": e2e,
             "cpu_baseline": cpu,
+            "many_instance": many,
         }
         print(json.dumps(line), flush=True)
     ctx.close()
