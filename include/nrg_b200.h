@@ -287,6 +287,12 @@ typedef struct nrg_run_output {
     int32_t finalCapacity;
     double* phaseSeconds;                 /* out, optional [4]: nrg sweep, rdm, cfs, total
                                              (device events)                            */
+    double* thermo;                       /* out, optional [nIter-first+1]*3: Cn, Sn, Xn of
+                                             calcThermo (module.F90:1931-1982, called at
+                                             postprocess.F90:62) per iteration, computed on
+                                             the device in the device-resident run; NaN in
+                                             the drop-in replay, whose caller computes
+                                             them on the host as the reference does     */
 } nrg_run_output;
 NRG_API int nrg_run(nrg_context* ctx, const nrg_run_input* in, nrg_run_output* out);
 
@@ -302,6 +308,17 @@ NRG_API int nrg_run(nrg_context* ctx, const nrg_run_input* in, nrg_run_output* o
  * array order; callers sort them by estimated cost, largest first.  statuses[i]
  * (optional) receives each instance's status; the return value is the status of the
  * first failing instance (all instances run to the end), or NRG_OK. */
+/* ---- log-Gaussian broadening of a binned spectrum -----------------------------------
+ * No reference counterpart: the reference writes raw bins (binnedSpikePositive/Negative,
+ * main.F90:204-252) and leaves the smoothing to post-processing.  The standard NRG kernel
+ * (Bulla, Costi and Pruschke, Rev. Mod. Phys. 80, 395 (2008), Sec. V.A):
+ *   A[m*nOmega + k] = sum_i w_i exp(-b^2/4) / (b |E_i| sqrt(pi)) exp(-(ln(omega_k/E_i)/b)^2)
+ * over the bins i of matrix type m with omega_k E_i > 0.  bins is a binnedSpike array as
+ * spikeCFS fills it, Fortran (numberOfBin*nMat, 2): energies, then weights; pass the
+ * positive and the negative array in turn.  Host or device pointers. */
+NRG_API int nrg_broaden_log_gaussian(nrg_context* ctx, const double* bins, int32_t numberOfBin, int32_t nMat,
+                                     double b, const double* omega, int32_t nOmega, double* A);
+
 #define NRG_BATCH_RELEASE 1   /* flags: release each context's storage when its instance ends,
                                  so that device memory holds only the instances in flight */
 NRG_API int nrg_run_batch(nrg_context* const* ctxs, const nrg_run_input* in, nrg_run_output* out,

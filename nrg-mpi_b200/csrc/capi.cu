@@ -794,6 +794,28 @@ static int spike_common(nrg_context* ctx, int32_t iteration, const nrg_spike_io*
     return rc;
 }
 
+int nrg_broaden_log_gaussian(nrg_context* ctx, const double* bins, int32_t numberOfBin, int32_t nMat, double b,
+                             const double* omega, int32_t nOmega, double* A) {
+    if (!ctx) { nrg_set_error_message("NULL context"); return NRG_ERR_INVALID; }
+    if (numberOfBin < 1 || nMat < 1 || nOmega < 0 || !(b > 0.0)) {
+        nrg_set_error_message("nrg_broaden_log_gaussian: numberOfBin %d, nMat %d, nOmega %d, b %g", numberOfBin, nMat,
+                              nOmega, b);
+        return NRG_ERR_INVALID;
+    }
+    if (nOmega == 0) return NRG_OK;
+    NRG_CUDA_TRY(cudaSetDevice(ctx->device));
+    const double *dB = nullptr, *dW = nullptr;
+    double* dA = nullptr;
+    const size_t nbt = 2 * (size_t)numberOfBin * nMat;
+    NRG_TRY(stage_in(ctx, bins, nbt, kSlotIO + 15, &dB));
+    NRG_TRY(stage_in(ctx, omega, (size_t)nOmega, kSlotIO + 16, &dW));
+    NRG_TRY(stage_out(ctx, A, (size_t)nOmega * nMat, kSlotIO + 17, &dA));
+    NRG_TRY(run_broaden(ctx, dB, numberOfBin, nMat, b, dW, nOmega, dA));
+    NRG_TRY(finish_out(ctx, A, dA, (size_t)nOmega * nMat));
+    NRG_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+    return NRG_OK;
+}
+
 int nrg_spike_zero_temperature(nrg_context* ctx, int32_t iteration, const nrg_spike_io* io) {
     return spike_common(ctx, iteration, io, false);
 }

@@ -207,6 +207,12 @@ int run_device(nrg_context* ctx, const nrg_run_input* in, nrg_run_output* out, c
     auto slotV = [&](int idx) -> DevBuf& { return ctx->slot(20 + 3 * (size_t)idx); };
     auto slotE = [&](int idx) -> DevBuf& { return ctx->slot(21 + 3 * (size_t)idx); };
     auto slotS = [&](int idx) -> DevBuf& { return ctx->slot(22 + 3 * (size_t)idx); };
+    double* dThermo = nullptr;
+    if (out && out->thermo) {
+        DevBuf& bT = ctx->scratch.b[39];
+        NRG_TRY(bT.ensure(sizeof(double) * 3 * (size_t)nIt));
+        dThermo = bT.as<double>();
+    }
 
     // ---- forward sweep ----
     for (int it = first; it <= nIter; ++it) {
@@ -226,6 +232,7 @@ int run_device(nrg_context* ctx, const nrg_run_input* in, nrg_run_output* out, c
         NRG_TRY(bE.ensure(sizeof(double) * (size_t)nb));
         DiagOut dout;
         NRG_TRY(diag_device(ctx, it, S, dEold, nb_old, dIMold, bV.as<double>(), bE.as<double>(), &dout));
+        if (out && out->thermo) NRG_TRY(run_thermo(ctx, S, bE.as<double>(), dThermo + 3 * (size_t)idx));
         if (out && out->groundStateEnergy) out->groundStateEnergy[idx] = dout.groundStateEnergy;
         R.Esec.resize(nb);
         NRG_CUDA_TRY(cudaMemcpyAsync(R.Esec.data(), bE.p, sizeof(double) * nb, cudaMemcpyDeviceToHost, st));
@@ -364,6 +371,10 @@ int run_device(nrg_context* ctx, const nrg_run_input* in, nrg_run_output* out, c
     NRG_CUDA_TRY(cudaEventRecord(ev[3], st));
     NRG_CUDA_TRY(cudaStreamSynchronize(st));
     NRG_TRY(check_device_status(ctx));
+    if (dThermo) {
+        NRG_CUDA_TRY(cudaMemcpy(out->thermo, dThermo, sizeof(double) * 3 * (size_t)nIt, cudaMemcpyDeviceToHost));
+        ctx->d2h += (long long)sizeof(double) * 3 * nIt;
+    }
     if (out) {
         out->numberOfBin = nbin;
         out->startTrancation = startTrancation;
@@ -398,6 +409,8 @@ constexpr size_t kHostIM = 0, kHostFV = 2, kHostV = 16, kHostIMS = 16 + 4096;
 
 int run_drop_in(nrg_context* ctx, const nrg_run_input* in, nrg_run_output* out, cudaEvent_t* ev) {
     const Model& M = ctx->model;
+    if (out && out->thermo)   // thermodynamics are the caller's part of postprocess here
+        for (int k = 0; k < 3 * (M.nIter - M.first + 1); ++k) out->thermo[k] = std::nan("");
     const int nVar = M.nVar, rs = nVar + 3, rsf = nVar + 6, first = M.first, nIter = M.nIter;
     const int nIt = nIter - first + 1;
     const bool spectrum = in->spectrum && M.nMat > 0;

@@ -200,6 +200,13 @@ int run_spikes(nrg_context* ctx, std::vector<SpikeProb>& probs, const double* d_
                const double* d_E, int nbin, int nMat, double* d_binPos, double* d_binNeg,
                double* d_tot);
 int run_fill(nrg_context* ctx, double* p, long long n, double v);
+// betabar of module.F90:652, a default-real literal (single precision 0.8 widened)
+constexpr double kBetabar = (double)0.8f;
+// calcThermo (module.F90:1931-1982) of one iteration: d_out[0..2] = Cn, Sn, Xn
+int run_thermo(nrg_context* ctx, const Sectors& S, const double* d_E, double* d_out);
+// log-Gaussian broadening of binned spikes onto the frequencies d_omega: d_A[m*nw + k]
+int run_broaden(nrg_context* ctx, const double* d_bins, int nbin, int nMat, double b, const double* d_omega,
+                int nw, double* d_A);
 int run_add(nrg_context* ctx, double* dst, const double* src, long long n);
 int run_sum_bins(nrg_context* ctx, const double* bins, int nbin, int nMat, double* out);
 int run_trace(nrg_context* ctx, const double* rdm, const long long* d_offs, const int* d_dims,

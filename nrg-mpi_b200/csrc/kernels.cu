@@ -247,6 +247,89 @@ __global__ void __launch_bounds__(256) k_spikes(const SpikeProb* __restrict__ pr
     }
 }
 
+// calcThermo (module.F90:1931-1982) on one iteration's eigenvalues in sector order, before
+// truncation (postprocess.F90:62): Z, E = sum bE e^-bE, <Sz^2>, <Sz> with bE = betabar E,
+// then C = sum (bE - E/Z)^2 e^-bE / Z (the fluctuation form), S = E/Z + ln Z and
+// X = <Sz^2> - <Sz>^2.  One block; partial sums per thread, combined in a fixed order.
+// tab: sector start | dimension | 2 Sz, nsub entries each.
+__device__ __forceinline__ void thermo_sum(double* v, int nv, double (*red)[32]) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    for (int q = 0; q < nv; ++q)
+        for (int o = 16; o > 0; o >>= 1) v[q] += __shfl_xor_sync(0xffffffffu, v[q], o);
+    __syncthreads();
+    if (lane == 0)
+        for (int q = 0; q < nv; ++q) red[q][warp] = v[q];
+    __syncthreads();
+    for (int q = 0; q < nv; ++q) {
+        double s = 0.0;
+        for (int w = 0; w < nw; ++w) s += red[q][w];
+        v[q] = s;
+    }
+}
+__global__ void __launch_bounds__(512) k_thermo(const double* __restrict__ E, const int* __restrict__ tab,
+                                                int nsub, double betabar, double* __restrict__ out) {
+    __shared__ double red[4][32];
+    double v[4] = {0.0, 0.0, 0.0, 0.0};
+    for (int s = 0; s < nsub; ++s) {
+        const int s0 = tab[s], d = tab[nsub + s];
+        const double sz = 0.5 * tab[2 * nsub + s];
+        for (int i = threadIdx.x; i < d; i += blockDim.x) {
+            const double bE = betabar * E[s0 + i];
+            const double ex = exp(-bE);
+            v[0] += ex;
+            v[1] += bE * ex;
+            v[2] += ex * sz * sz;
+            v[3] += ex * sz;
+        }
+    }
+    thermo_sum(v, 4, red);
+    const double Z = v[0], em = v[1] / Z;
+    double c[1] = {0.0};
+    for (int s = 0; s < nsub; ++s) {
+        const int s0 = tab[s], d = tab[nsub + s];
+        for (int i = threadIdx.x; i < d; i += blockDim.x) {
+            const double bE = betabar * E[s0 + i];
+            c[0] += (bE - em) * (bE - em) * exp(-bE);
+        }
+    }
+    thermo_sum(c, 1, red);
+    if (threadIdx.x == 0) {
+        out[0] = c[0] / Z;
+        out[1] = em + log(Z);
+        out[2] = v[2] / Z - (v[3] / Z) * (v[3] / Z);
+    }
+}
+
+// log-Gaussian broadening of binned spikes (Bulla, Costi and Pruschke, Rev. Mod. Phys. 80,
+// 395 (2008), Sec. V.A): A(w) = sum_i w_i P(w, E_i) with
+// P(w, E) = exp(-b^2/4) / (b |E| sqrt(pi)) exp(-(ln(w/E)/b)^2) for w E > 0, else 0.
+// bins: Fortran (nbin*nMat, 2) (energies, then weights; column stride ld); one block per
+// (output frequency, matrix type), threads over the bins, partial sums in a fixed order.
+__global__ void __launch_bounds__(256) k_broaden(const double* __restrict__ bins, int nbin, long long ld,
+                                                 double b, const double* __restrict__ omega, int nw,
+                                                 double* __restrict__ A) {
+    __shared__ double red[8];
+    const int k = blockIdx.x % nw, m = blockIdx.x / nw;
+    const double w = omega[k];
+    const double* E = bins + (size_t)m * nbin;
+    const double* W = bins + ld + (size_t)m * nbin;
+    double s = 0.0;
+    for (int i = threadIdx.x; i < nbin; i += blockDim.x) {
+        const double wi = W[i], ei = E[i];
+        if (wi == 0.0 || !(w * ei > 0.0)) continue;
+        const double x = log(w / ei) / b;
+        s += wi * exp(-x * x) / fabs(ei);
+    }
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double t = 0.0;
+        for (int q = 0; q < (int)(blockDim.x >> 5); ++q) t += red[q];
+        A[(size_t)m * nw + k] = t * exp(-0.25 * b * b) / (b * sqrt(3.14159265358979323846));
+    }
+}
+
 __global__ void k_fill(double* p, long long n, double v) {
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) p[i] = v;
 }
@@ -384,6 +467,37 @@ int run_spikes(nrg_context* ctx, std::vector<SpikeProb>& probs, const double* d_
     NRG_TRY(h2d_async(ctx, dq.p, prefix.data(), sizeof(long long) * np));
     k_spikes<<<(unsigned)total, 256, 0, ctx->stream>>>(dp.as<SpikeProb>(), dq.as<long long>(), np, d_work, d_E, nbin,
                                                      d_binPos, d_binNeg, d_tot);
+    ctx->launches++;
+    NRG_CUDA_TRY(cudaGetLastError());
+    return NRG_OK;
+}
+
+int run_thermo(nrg_context* ctx, const Sectors& S, const double* d_E, double* d_out) {
+    const Model& M = ctx->model;
+    const int nsub = S.nsub, nVar = S.nVar;
+    std::vector<int> tab(3 * (size_t)nsub);
+    for (int s = 0; s < nsub; ++s) {
+        int sz = 0;
+        for (int v = M.cb[1]; v <= M.cb[3]; ++v) sz += S.qn[(size_t)s * nVar + v - 1];
+        tab[s] = S.start[s];
+        tab[nsub + s] = S.dim[s];
+        tab[2 * nsub + s] = sz;
+    }
+    DevBuf& b = ctx->scratch.b[38];
+    NRG_TRY(b.ensure(sizeof(int) * tab.size()));
+    NRG_TRY(h2d_async(ctx, b.p, tab.data(), sizeof(int) * tab.size()));
+    k_thermo<<<1, 512, 0, ctx->stream>>>(d_E, b.as<int>(), nsub, kBetabar, d_out);
+    ctx->launches++;
+    NRG_CUDA_TRY(cudaGetLastError());
+    return NRG_OK;
+}
+
+int run_broaden(nrg_context* ctx, const double* d_bins, int nbin, int nMat, double b, const double* d_omega,
+                int nw, double* d_A) {
+    if (nw <= 0 || nMat <= 0) return NRG_OK;
+    const long long blocks = (long long)nw * nMat;
+    if (blocks > 0x7fffffffLL) return NRG_ERR_TOO_LARGE;
+    k_broaden<<<(unsigned)blocks, 256, 0, ctx->stream>>>(d_bins, nbin, (long long)nbin * nMat, b, d_omega, nw, d_A);
     ctx->launches++;
     NRG_CUDA_TRY(cudaGetLastError());
     return NRG_OK;

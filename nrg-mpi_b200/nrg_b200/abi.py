@@ -45,6 +45,7 @@ EXPORTS = [
     "nrg_spike_zero_temperature", "nrg_spike_cfs", "nrg_run", "nrg_context_get_stats",
     "nrg_context_reset_stats", "nrg_context_set_profiling", "nrg_block_eigh_noalloc",
     "nrg_host_alloc", "nrg_host_free", "nrg_run_batch", "nrg_context_release_storage",
+    "nrg_broaden_log_gaussian",
 ]
 
 
@@ -134,7 +135,7 @@ class RunOutput(ctypes.Structure):
         ("binCapacity", c_int64), ("startTrancation", c_int32), ("kept", _pi32),
         ("numberOfBasisFull", _pi32), ("groundStateEnergy", _pf64), ("rdmTrace", _pf64),
         ("flow", _pf64), ("flowStride", c_int32), ("finalEigenvalue", _pf64),
-        ("finalCapacity", c_int32), ("phaseSeconds", _pf64),
+        ("finalCapacity", c_int32), ("phaseSeconds", _pf64), ("thermo", _pf64),
     ]
 
 
@@ -175,6 +176,8 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
     lib.nrg_run_batch.argtypes = [POINTER(c_void_p), POINTER(RunInput), POINTER(RunOutput), c_int32, c_int32,
                                   c_int32, POINTER(c_int32)]
     lib.nrg_context_release_storage.argtypes = [c_void_p]
+    lib.nrg_broaden_log_gaussian.argtypes = [c_void_p, POINTER(c_double), c_int32, c_int32, c_double,
+                                             POINTER(c_double), c_int32, POINTER(c_double)]
     lib.nrg_context_get_stats.argtypes = [c_void_p, POINTER(Stats)]
     lib.nrg_context_reset_stats.argtypes = [c_void_p]
     lib.nrg_context_set_profiling.argtypes = [c_void_p, ctypes.c_int]
@@ -236,6 +239,18 @@ class Context:
 
     def set_stream(self, stream_handle: int):
         self._check(self.lib.nrg_context_set_stream(self._h, c_void_p(stream_handle)), "set_stream")
+
+    def broaden_log_gaussian(self, bins, numberOfBin: int, nMat: int, b: float, omega):
+        """nrg_broaden_log_gaussian: A of shape (nMat, len(omega)) from one binnedSpike array."""
+        bins = np.asfortranarray(bins, dtype=np.float64)
+        if bins.shape != (numberOfBin * nMat, 2):
+            raise NrgError(1, "broaden_log_gaussian", f"bins shape {bins.shape}")
+        om = np.ascontiguousarray(omega, dtype=np.float64)
+        A = np.zeros(nMat * om.size)
+        self._check(self.lib.nrg_broaden_log_gaussian(self._h, _p(bins, c_double), numberOfBin, nMat, float(b),
+                                                      _p(om, c_double), om.size, _p(A, c_double)),
+                    "broaden_log_gaussian")
+        return A.reshape(nMat, om.size)
 
     def release_storage(self):
         """Frees the device storage kept between runs (the model stays set)."""
@@ -467,12 +482,14 @@ class Context:
                  kept=np.zeros(nit, dtype=np.int32), nfull=np.zeros(nit, dtype=np.int32),
                  gse=np.zeros(nit), tr=np.full(inp.numberOfIteration + 1, np.nan),
                  flow=np.full(nit * flow_stride, np.nan), fin=np.zeros(max(final_capacity, 1)),
-                 ph=np.zeros(4), nit=nit, nmat=nmat, spectrum=spectrum, flow_stride=flow_stride,
+                 ph=np.zeros(4), thermo=np.full(3 * nit, np.nan), nit=nit, nmat=nmat,
+                 spectrum=spectrum, flow_stride=flow_stride,
                  final_capacity=final_capacity)
         a["ro"] = RunOutput(0, _p(a["bp"], c_double), _p(a["bn"], c_double), a["bp"].size, 0,
                             _p(a["kept"], c_int32), _p(a["nfull"], c_int32), _p(a["gse"], c_double),
                             _p(a["tr"], c_double), _p(a["flow"], c_double), flow_stride,
-                            _p(a["fin"], c_double), final_capacity, _p(a["ph"], c_double))
+                            _p(a["fin"], c_double), final_capacity, _p(a["ph"], c_double),
+                            _p(a["thermo"], c_double))
         return a
 
     def _run_result(self, a):
@@ -487,7 +504,8 @@ class Context:
         return dict(numberOfBin=nbin, binPos=binPos, binNeg=binNeg, kept=a["kept"],
                     numberOfBasisFull=a["nfull"], groundStateEnergy=a["gse"], rdmTrace=a["tr"],
                     flow=a["flow"].reshape(a["nit"], a["flow_stride"]), startTrancation=ro.startTrancation,
-                    finalEigenvalue=a["fin"][:a["final_capacity"]], phaseSeconds=a["ph"])
+                    finalEigenvalue=a["fin"][:a["final_capacity"]], phaseSeconds=a["ph"],
+                    thermo=a["thermo"].reshape(a["nit"], 3))
 
 
 def run_batch(contexts, spectrum: bool = True, concurrency: int = 0, flow_stride: int = 8,

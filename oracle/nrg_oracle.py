@@ -838,6 +838,34 @@ def bin_spikes(st: State, container: np.ndarray, energy: np.ndarray, weight: np.
         np.add.at(container[:, 1], pr[two] + 1 + off, weight[two] * wb[two])
 
 
+def log_grid(wmin: float = 1e-8, wmax: float = 1.0, per_decade: int = 100) -> np.ndarray:
+    """Positive frequencies wmin .. wmax, per_decade points per decade (both ends kept)."""
+    n = int(round(np.log10(wmax / wmin) * per_decade))
+    return wmin * 10.0 ** (np.arange(n + 1) / per_decade)
+
+
+def broaden_log_gaussian(bins: np.ndarray, nbin: int, nmat: int, b: float, omega: np.ndarray) -> np.ndarray:
+    """Log-Gaussian broadening of binned spikes (Bulla, Costi and Pruschke, Rev. Mod. Phys.
+    80, 395 (2008), Sec. V.A; the reference has none: it writes raw bins):
+    A_m(w) = sum_i w_i exp(-b^2/4) / (b |E_i| sqrt(pi)) exp(-(ln(w/E_i)/b)^2), w E_i > 0.
+    bins: (nbin*nmat, 2) energies and weights as spikeCFS fills them.  Returns (nmat, len(w))."""
+    omega = np.asarray(omega, dtype=np.float64)
+    out = np.zeros((nmat, omega.size))
+    pref = math.exp(-0.25 * b * b) / (b * math.sqrt(math.pi))
+    for m in range(nmat):
+        E = bins[m * nbin:(m + 1) * nbin, 0]
+        W = bins[m * nbin:(m + 1) * nbin, 1]
+        nz = W != 0.0
+        E, W = E[nz], W[nz]
+        for k, w in enumerate(omega):
+            same = w * E > 0.0
+            if not np.any(same):
+                continue
+            x = np.log(w / E[same]) / b
+            out[m, k] = pref * np.sum(W[same] * np.exp(-x * x) / np.abs(E[same]))
+    return out
+
+
 def _find_subspace(si, nVar, qn):
     """findSubspace (module.F90:1256-1284): first match."""
     hit = np.nonzero(np.all(si[:, :nVar] == qn, axis=1))[0]

@@ -9,7 +9,8 @@ Tolerances (written here, checked below):
 * basis_output: bit-exact;
 * invariant matrices, density matrices: <= 1e-12 absolute (entries are O(1));
 * spectral bins: <= 1e-8 absolute per bin (spectra are O(1) in total weight);
-* spectral sum rule: |sum - 1| <= 1e-10.
+* spectral sum rule: |sum - 1| <= 1e-10;
+* thermodynamics (Cn, Sn, Xn per iteration): <= 1e-12 * max(1, |value|).
 """
 import numpy as np
 import pytest
@@ -26,6 +27,7 @@ VEC_TOL = 1e-9
 MAT_TOL = 1e-12
 BIN_TOL = 1e-8
 SUM_TOL = 1e-10
+THERMO_TOL = 1e-12
 
 
 def _drive(ctx_factory, inp):
@@ -226,6 +228,8 @@ def test_device_resident_run_matches_oracle(ctx_factory):
     for k, i in enumerate(its):
         flow = st.flow[i][:8]
         assert np.max(np.abs(res["flow"][k][:len(flow)] - flow)) <= 1e-11
+        ref = np.array(st.thermo[i])
+        assert np.max(np.abs(res["thermo"][k] - ref) / np.maximum(1.0, np.abs(ref))) <= THERMO_TOL
     # the same run through the drop-in entry points with host arrays
     res2 = ctx.run(spectrum=True, host_drop_in=True)
     assert [int(k) for k in res2["kept"]] == [int(k) for k in res["kept"]]
@@ -233,3 +237,21 @@ def test_device_resident_run_matches_oracle(ctx_factory):
     assert np.max(np.abs(res2["binNeg"][:, 1] - st.binNeg[:, 1])) <= BIN_TOL
     for N in range(st.startTrancation, st.nIter):
         assert abs(res2["rdmTrace"][N] - 1.0) <= 1e-12
+
+
+def test_log_gaussian_broadening_matches_oracle(ctx_factory):
+    # the derived view of the CPU-runnable workload: the run's bins broadened onto
+    # 1e-8 .. 1 at 100 points per decade with b = 0.6; 1e-12 relative to the oracle
+    inp = small_siam(n_keep=48, n_iterations=14)
+    d = write_case(inp)
+    st = O.run(d)
+    ctx = ctx_factory(model.read_inputs(d))
+    res = ctx.run(spectrum=True)
+    nbin, nmat = res["numberOfBin"], st.nMat
+    w = O.log_grid(1e-8, 1.0, 100)
+    for bins, om in ((res["binPos"], w), (res["binNeg"], -w)):
+        A = ctx.broaden_log_gaussian(bins, nbin, nmat, 0.6, om)
+        R = O.broaden_log_gaussian(bins, nbin, nmat, 0.6, om)
+        assert A.shape == (nmat, w.size)
+        assert np.max(np.abs(A - R) / np.maximum(np.abs(R), 1e-300 + np.max(np.abs(R)) * 1e-3)) <= 1e-12
+        assert np.all(np.isfinite(A)) and np.all(A >= 0.0)

@@ -132,3 +132,25 @@ def test_exchange_sort_matches_reference_semantics():
                 ref[[i, j]] = ref[[j, i]]
     out = O.exchange_sort(rec.copy(), 2)
     assert np.array_equal(out, ref)
+
+
+def test_log_gaussian_broadening_keeps_the_weight():
+    # one spike of weight 0.7 at E = 2e-4 (and one of weight 0.3 at -5e-3 in the negative
+    # bins): the broadened curve integrates back to the weight (log grid, trapezoid in ln w)
+    nbin = 5
+    pos = np.zeros((nbin, 2))
+    pos[:, 0] = [1e-6, 1e-5, 2e-4, 1e-3, 1e-2]
+    pos[2, 1] = 0.7
+    neg = np.zeros((nbin, 2))
+    neg[:, 0] = -pos[:, 0]
+    neg[4, 1] = 0.3
+    w = O.log_grid(1e-9, 1e2, 400)
+    Ap = O.broaden_log_gaussian(pos, nbin, 1, 0.6, w)[0]
+    An = O.broaden_log_gaussian(neg, nbin, 1, 0.6, -w)[0]
+    lnw = np.log(w)
+    assert abs(np.trapezoid(Ap * w, lnw) - 0.7) <= 1e-6
+    assert abs(np.trapezoid(An * w, lnw) - 0.3) <= 1e-6
+    assert np.all(O.broaden_log_gaussian(pos, nbin, 1, 0.6, -w) == 0.0)
+    # A(w) peaks at E, and w A(w) (the density in ln w) at E exp(b^2/2)
+    assert abs(w[np.argmax(Ap)] / 2e-4 - 1.0) < 0.01
+    assert abs(w[np.argmax(Ap * w)] / (2e-4 * np.exp(0.18)) - 1.0) < 0.01
