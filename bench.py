@@ -11,9 +11,12 @@ the backward reduced density matrices and the T=0 CFS spectrum on the reference'
   stream the library launches on, barrier + synchronize on both sides, max over ranks.
 * e2e: the same metric through the drop-in entry points with host arrays (every routine
   copies its module arrays host->device and back, as a Fortran caller would).
-* roofline: the batched FP64 eigensolver (the dominant kernel), algorithmic flops
-  sum_s (4/3+2) d_s^3 per launch over its event-timed duration, against a cuBLAS DGEMM
-  peak measured here.
+* roofline: k_tri_cluster, the Householder tridiagonalisation of the sectors of order
+  > 128 (the largest share of device time): algorithmic flops sum_s 4/3 d_s^3 per launch
+  over its event-timed launch duration, against a cuBLAS DGEMM peak measured here (the
+  FP64 ceiling; tcgen05 has no FP64 kind); traffic = DRAM bytes per launch from the ncu
+  capture summarised in profiles/.  "eigensolver" gives the same for the whole
+  eigensolver of an iteration (sum_s (4/3+2) d_s^3 over the event-timed window).
 * cpu_baseline: the oracle (numpy/scipy port of the reference path, OpenBLAS on all host
   threads) on a bounded sample of the same sweep.
 * --impl reference: the oracle port timed per NRG iteration of the same sweep (steps are
@@ -47,6 +50,11 @@ WORKLOAD = dict(U=0.2, Gamma=0.02, eps_d=-0.1, Lambda=2.0, n_keep=2048, n_iterat
 WORKLOAD_NAME = ("SIAM flat band Lambda=2.0 U=0.2 Gamma=0.02 eps_d=-0.1 N_keep=2048, "
                  "60 NRG iterations + backward RDM + T=0 CFS spectrum (1000 bins/decade)")
 METRIC = "NRG iterations/s (full sweep + RDM + CFS spectrum, FP64, eig err <= 1e-12)"
+# DRAM bytes (read + write) per k_tri_cluster launch of this workload, from the ncu
+# capture in profiles/k_tri_cluster_siam_nkeep2048.md (average over the two launches of
+# one iteration)
+TRI_TRAFFIC_BYTES = 12.03e6
+TRI_TRAFFIC_SOURCE = "profiles/k_tri_cluster_siam_nkeep2048.md"
 
 
 def parse():
@@ -339,6 +347,9 @@ def main():
         syev_avg_s = stats["syev_ms"] * 1e-3 / max(stats["syev_launches"], 1)
         flops_per_launch = stats["syev_flops"] / max(stats["syev_launches"], 1)
         achieved = flops_per_launch / syev_avg_s / 1e12 if syev_avg_s > 0 else None
+        tri_avg_s = stats["tri_ms"] * 1e-3 / max(stats["tri_launches"], 1)
+        tri_flops = stats["tri_flops"] / max(stats["tri_launches"], 1)
+        tri_ach = tri_flops / tri_avg_s / 1e12 if tri_avg_s > 0 else None
         cpu = None
         if not args.no_cpu:
             v, dt, i0, i1 = cpu_sample()
@@ -357,13 +368,22 @@ def main():
             "spectrum_seconds": float(ph[2]),
             "sum_rule": sums,
             "gpu_launches": int(launches),
-            "roofline": {"kernel": "k_syev (batched FP64 tridiagonalisation + divide and conquer + back-transform)",
+            "roofline": {"kernel": "k_tri_cluster (FP64 Householder tridiagonalisation of the sectors of "
+                                   "order > 128, one 8-block cluster per sector)",
                          "bound": "tensor", "pipe": "fp64",
-                         "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
-                         "frac": (achieved / peak) if (achieved and peak) else None,
-                         "peak_source": "cuBLAS DGEMM 8192^3 measured in this run (MEASURED_PEAKS.json has no FP64 figure)",
-                         "flops_per_launch": flops_per_launch, "avg_launch_ms": syev_avg_s * 1e3,
-                         "launches": int(stats["syev_launches"]), "traffic": None},
+                         "achieved": tri_ach, "peak": peak, "unit": "TFLOP/s",
+                         "frac": (tri_ach / peak) if (tri_ach and peak) else None,
+                         "peak_source": "cuBLAS DGEMM 8192^3 measured in this run (MEASURED_PEAKS.json has no "
+                                        "FP64 figure)",
+                         "flops_per_launch": tri_flops, "avg_launch_ms": tri_avg_s * 1e3,
+                         "launches": int(stats["tri_launches"]),
+                         "traffic": TRI_TRAFFIC_BYTES, "traffic_source": TRI_TRAFFIC_SOURCE},
+            "eigensolver": {"what": "all sectors of one iteration: tridiagonalisation, divide and conquer, "
+                                    "back-transformation (three streams)",
+                            "achieved": achieved, "unit": "TFLOP/s", "peak": peak,
+                            "frac": (achieved / peak) if (achieved and peak) else None,
+                            "flops_per_launch": flops_per_launch, "avg_window_ms": syev_avg_s * 1e3,
+                            "windows": int(stats["syev_launches"])},
             "clocks": clocks,
             "e2e": e2e,
             "cpu_baseline": cpu,
