@@ -947,22 +947,31 @@ static int tri_cluster_cl(nrg_context* ctx, const LSec* dsec, int ns, int maxn, 
     return NRG_OK;
 }
 
-// Cluster size of the one-launch tridiagonalisation: 8 blocks per sector by default; the
-// environment variable NRG_TRI_CLUSTER selects 4, 8 or 16, or 0 for the multi-kernel path.
+// Cluster size of the one-launch tridiagonalisation: 8 blocks per sector (16 for the
+// largest size class alone halves its per-block product but costs as much in the wider
+// exchanges: no net gain measured); a size that cannot be placed falls back to the next
+// smaller one.  The environment variable NRG_TRI_CLUSTER forces 4, 8 or 16, or 0 for the
+// multi-kernel path.
 static int tri_cluster(nrg_context* ctx, const LSec* dsec, int ns, int maxn, double* d_V, double* wsd,
                        int* wsi, bool* done) {
-    static const int cl = [] {
+    static const int forced = [] {
         const char* e = getenv("NRG_TRI_CLUSTER");
-        const int v = e ? atoi(e) : kTriCL;
-        return (v == 0 || v == 4 || v == 8 || v == 16) ? v : kTriCL;
+        if (!e || !*e) return -1;
+        const int v = atoi(e);
+        return (v == 0 || v == 4 || v == 8 || v == 16) ? v : -1;
     }();
     *done = false;
-    switch (cl) {
-        case 4: return tri_cluster_cl<4>(ctx, dsec, ns, maxn, d_V, wsd, wsi, done);
-        case 8: return tri_cluster_cl<8>(ctx, dsec, ns, maxn, d_V, wsd, wsi, done);
-        case 16: return tri_cluster_cl<16>(ctx, dsec, ns, maxn, d_V, wsd, wsi, done);
-        default: return NRG_OK;
+    const int cl = forced >= 0 ? forced : kTriCL;
+    if (cl == 16) {
+        NRG_TRY(tri_cluster_cl<16>(ctx, dsec, ns, maxn, d_V, wsd, wsi, done));
+        if (*done || forced == 16) return NRG_OK;
     }
+    if (cl >= 8) {
+        NRG_TRY(tri_cluster_cl<8>(ctx, dsec, ns, maxn, d_V, wsd, wsi, done));
+        if (*done || forced == 8) return NRG_OK;
+    }
+    if (cl >= 4) return tri_cluster_cl<4>(ctx, dsec, ns, maxn, d_V, wsd, wsi, done);
+    return NRG_OK;
 }
 
 int syev_large(nrg_context* ctx, const std::vector<SyevSector>& in, double* d_V, double* d_E, int slot_base) {
