@@ -116,6 +116,29 @@ int stage_in(nrg_context* ctx, const T* p, size_t n, size_t slot, const T** out)
     return NRG_OK;
 }
 
+// stage_in for an input of which the routine reads only the listed runs: pinned host
+// memory is read run by run by a kernel (only those bytes cross the host link, the
+// rest of the device copy is never read); pageable memory is copied whole
+int stage_in_segs(nrg_context* ctx, const double* p, size_t n, long long ld, const std::vector<HostSeg>& segs,
+                  size_t slot, const double** out) {
+    if (n == 0) { *out = nullptr; return NRG_OK; }
+    if (!p) { nrg_set_error_message("NULL input array"); return NRG_ERR_INVALID; }
+    cudaPointerAttributes a;
+    if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+        cudaGetLastError();
+        return stage_in(ctx, p, n, slot, out);
+    }
+    if (a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged) { *out = p; return NRG_OK; }
+    if (a.type != cudaMemoryTypeHost || !a.devicePointer) return stage_in(ctx, p, n, slot, out);
+    DevBuf& b = ctx->slot(slot);
+    NRG_TRY(b.ensure(sizeof(double) * n));
+    long long bytes = 0;
+    NRG_TRY(run_gather_segs(ctx, static_cast<const double*>(a.devicePointer), b.as<double>(), ld, segs, &bytes));
+    ctx->h2d += bytes;
+    *out = b.as<double>();
+    return NRG_OK;
+}
+
 template <class T>
 int stage_out(nrg_context* ctx, T* p, size_t n, size_t slot, T** dev) {
     if (!p) { nrg_set_error_message("NULL output array"); return NRG_ERR_INVALID; }
@@ -421,7 +444,36 @@ int nrg_diagonalization(nrg_context* ctx, int32_t iteration, const nrg_diagonali
     const double *dEo = nullptr, *dIM = nullptr;
     double *dV = nullptr, *dE = nullptr;
     if (rc == NRG_OK) rc = stage_in(ctx, io->eigenvalue_old, (size_t)nbo, kSlotIO + 0, &dEo);
-    if (rc == NRG_OK) rc = stage_in(ctx, io->invariant_matrix, (size_t)nbo * nbo * M.nCM, kSlotIO + 1, &dIM);
+    if (rc == NRG_OK) {
+        // the blocks of invariant_matrix the assembly reads (diagonalization.F90:195-237):
+        // for every ordered pair of operation groups of a sector whose coefficient scan
+        // found a term, the previous-sector rows of one group against the columns of the
+        // other (IM(jref, iref, type), swapped as the scan says)
+        std::vector<HostSeg> segs;
+        std::vector<long long> seen;
+        const int nOps = M.nOps;
+        for (int s = 0; s < S.nsub; ++s)
+            for (int a = 0; a < nOps; ++a) {
+                const int ca = S.cnt(s, a);
+                if (ca == 0) continue;
+                for (int b = 0; b < nOps; ++b) {
+                    const int cb = S.cnt(s, b);
+                    const int idx = a * nOps + b;
+                    if (cb == 0 || !M.dflag[idx]) continue;
+                    const int t = M.dtype[idx] - 1;
+                    if (t < 0 || t >= M.nCM) continue;
+                    const int ra = S.refBase[(size_t)s * nOps + a], rb = S.refBase[(size_t)s * nOps + b];
+                    const bool sw = M.dswp[idx] != 0;
+                    const int r0 = sw ? ra : rb, nr = sw ? ca : cb, c0 = sw ? rb : ra, nc = sw ? cb : ca;
+                    if (r0 < 0 || c0 < 0 || r0 + nr > nbo || c0 + nc > nbo) continue;   // the kernel flags it
+                    const long long key = ((long long)t * nbo + c0) * nbo + r0;
+                    if (std::find(seen.begin(), seen.end(), key) != seen.end()) continue;
+                    seen.push_back(key);
+                    segs.push_back({r0 + (long long)c0 * nbo + (long long)t * nbo * nbo, nr, nc});
+                }
+            }
+        rc = stage_in_segs(ctx, io->invariant_matrix, (size_t)nbo * nbo * M.nCM, nbo, segs, kSlotIO + 1, &dIM);
+    }
     if (rc == NRG_OK) rc = stage_out(ctx, io->eigenvector, (size_t)S.sizeV, kSlotIO + 2, &dV);
     if (rc == NRG_OK) rc = stage_out(ctx, io->eigenvalue, (size_t)S.nb, kSlotIO + 3, &dE);
     DiagOut out;
@@ -479,10 +531,48 @@ static int invmat_common(nrg_context* ctx, int32_t iteration, const nrg_invarian
     double* dOut = nullptr;
     const int nbk = io->numberOfBasis;
     const size_t nout = (size_t)nbk * nbk * (spec ? M.nMat : M.nCM);
-    if (rc == NRG_OK) rc = stage_in(ctx, io->eigenvector, (size_t)S.sizeV, kSlotIO + 4, &dV);
-    if (rc == NRG_OK && spec)
-        rc = stage_in(ctx, io->invariant_matrix_spectrum_old,
-                      (size_t)io->numberOfBasis_old * io->numberOfBasis_old * M.nMat, kSlotIO + 5, &dIMSo);
+    if (rc == NRG_OK) {
+        // both transforms read the kept columns of each eigenvector block only
+        // (invariantMatrixDGEMM.F90:300-317, invariantMatrixForSpectrumDGEMM.F90:296-313)
+        std::vector<HostSeg> segs;
+        for (int s = 0; s < S.nsub; ++s)
+            if (kept[s] > 0) segs.push_back({S.ce[s], S.dim[s] * kept[s], 1});
+        rc = stage_in_segs(ctx, io->eigenvector, (size_t)S.sizeV, 0, segs, kSlotIO + 4, &dV);
+    }
+    if (rc == NRG_OK && spec) {
+        // blocks of the previous d-dagger matrix the propagation reads: for each allowed
+        // (L, R, m) and local operation a, the previous sectors of (R, a) x (L, a)
+        // (invariantMatrixForSpectrumDGEMM.F90:166-256)
+        const long long nbo = io->numberOfBasis_old;
+        const int nOps = M.nOps, nVar = M.nVar;
+        std::vector<HostSeg> segs;
+        std::vector<long long> seen;
+        for (int L = 0; L < S.nsub; ++L) {
+            if (kept[L] == 0) continue;
+            for (int R = 0; R < S.nsub; ++R) {
+                if (kept[R] == 0) continue;
+                for (int m = 0; m < M.nMat; ++m) {
+                    bool ok = true;
+                    for (int v = 0; v < nVar && ok; ++v)
+                        ok = S.qn[(size_t)L * nVar + v] - S.qn[(size_t)R * nVar + v] ==
+                             M.cons_diff[(size_t)m + (size_t)v * M.nMat];
+                    if (!ok) continue;
+                    for (int a = 0; a < nOps; ++a) {
+                        const int cL = S.cnt(L, a), cR = S.cnt(R, a);
+                        if (cL == 0 || cR == 0) continue;
+                        const long long r0 = S.refBase[(size_t)R * nOps + a], c0 = S.refBase[(size_t)L * nOps + a];
+                        if (r0 < 0 || c0 < 0 || r0 + cR > nbo || c0 + cL > nbo) continue;   // rejected below
+                        const long long key = ((long long)m * nbo + c0) * nbo + r0;
+                        if (std::find(seen.begin(), seen.end(), key) != seen.end()) continue;
+                        seen.push_back(key);
+                        segs.push_back({r0 + c0 * nbo + (long long)m * nbo * nbo, cR, cL});
+                    }
+                }
+            }
+        }
+        rc = stage_in_segs(ctx, io->invariant_matrix_spectrum_old, (size_t)(nbo * nbo * M.nMat), nbo, segs,
+                           kSlotIO + 5, &dIMSo);
+    }
     if (rc == NRG_OK) rc = stage_out(ctx, io->invariant_matrix, nout, kSlotIO + 6, &dOut);
     if (rc == NRG_OK) {
         if (spec) rc = invmat_spec_device(ctx, S, kept, dV, io->numberOfBasis_old, dIMSo, dOut);
@@ -705,8 +795,12 @@ static int spike_common(nrg_context* ctx, int32_t iteration, const nrg_spike_io*
     const double *dV = nullptr, *dIMS = nullptr, *dR = nullptr;
     double *dEs = nullptr;
     if (rc == NRG_OK) rc = stage_in(ctx, io->eigenvector, (size_t)S.sizeV, kSlotIO + 9, &dV);
-    if (rc == NRG_OK) rc = stage_in(ctx, io->invariant_matrix_spectrum,
-                                    (size_t)io->numberOfBasis_old * io->numberOfBasis_old * M.nMat, kSlotIO + 10, &dIMS);
+    if (rc == NRG_OK) {
+        const int nbo = io->numberOfBasis_old;
+        const std::vector<HostSeg> segs = spike_ims_segs(M, it, cfs ? nullptr : &gs, nbo);
+        rc = stage_in_segs(ctx, io->invariant_matrix_spectrum, (size_t)nbo * nbo * M.nMat, nbo, segs,
+                           kSlotIO + 10, &dIMS);
+    }
     if (rc == NRG_OK && cfs) {
         // only the density blocks of this iteration's sectors are staged (one contiguous
         // range of the caller's array); offsets become relative to the range

@@ -144,6 +144,17 @@ struct nrg_context {
 
 namespace nrg {
 
+// a strided run of a host array: count runs of len doubles from element off, ld apart
+struct HostSeg {
+    long long off;
+    int len, count;
+};
+// copies the listed runs of src (device-accessible pinned host memory) to the same
+// positions of dst, reading them over the host link from a kernel; ld is the stride
+// between the runs of one segment
+int run_gather_segs(nrg_context* ctx, const double* src, double* dst, long long ld,
+                    const std::vector<HostSeg>& segs, long long* bytes);
+
 // raises a kernel's dynamic shared-memory limit on the current device to at least bytes
 // and never lowers it: the attribute belongs to the kernel, not to a stream, and host
 // threads running independent contexts launch the same kernels with different sizes
@@ -243,6 +254,10 @@ struct IterView {
 };
 int rdm_step_device(nrg_context* ctx, const IterView& present, const IterView& child,
                     double* d_rdm, double* d_trace_out);
+// blocks of the previous d-dagger matrix (nb_old x nb_old x nMat) the spike routines read:
+// T = 0 jobs when gs_sectors is given, CFS jobs otherwise
+std::vector<HostSeg> spike_ims_segs(const Model& M, const IterView& it, const std::vector<int>* gs_sectors,
+                                    int nb_old);
 int spike_cfs_device(nrg_context* ctx, int iteration, const IterView& it, int nb_old,
                      const double* d_IMSold, const double* d_rdm, double* d_binPos,
                      double* d_binNeg, double* d_tot);

@@ -330,6 +330,25 @@ __global__ void __launch_bounds__(256) k_broaden(const double* __restrict__ bins
     }
 }
 
+// element e of the concatenated runs: segment by binary search over the element prefix,
+// then run and offset; consecutive threads read consecutive doubles of a run
+__global__ void k_gather_segs(const double* __restrict__ src, double* __restrict__ dst, long long ld,
+                              const HostSeg* __restrict__ segs, const long long* __restrict__ prefix, int nseg,
+                              long long total) {
+    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < total;
+         e += (long long)gridDim.x * blockDim.x) {
+        int lo = 0, hi = nseg - 1;
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (prefix[mid] <= e) lo = mid; else hi = mid - 1;
+        }
+        const HostSeg g = segs[lo];
+        const long long loc = e - prefix[lo];
+        const long long p = g.off + (loc / g.len) * ld + loc % g.len;
+        dst[p] = src[p];
+    }
+}
+
 __global__ void k_fill(double* p, long long n, double v) {
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) p[i] = v;
 }
@@ -500,6 +519,33 @@ int run_broaden(nrg_context* ctx, const double* d_bins, int nbin, int nMat, doub
     k_broaden<<<(unsigned)blocks, 256, 0, ctx->stream>>>(d_bins, nbin, (long long)nbin * nMat, b, d_omega, nw, d_A);
     ctx->launches++;
     NRG_CUDA_TRY(cudaGetLastError());
+    return NRG_OK;
+}
+
+int run_gather_segs(nrg_context* ctx, const double* src, double* dst, long long ld,
+                    const std::vector<HostSeg>& segs, long long* bytes) {
+    const int ns = (int)segs.size();
+    *bytes = 0;
+    if (ns == 0) return NRG_OK;
+    std::vector<long long> prefix(ns);
+    long long total = 0;
+    for (int i = 0; i < ns; ++i) {
+        prefix[i] = total;
+        total += (long long)segs[i].len * segs[i].count;
+    }
+    if (total == 0) return NRG_OK;
+    DevBuf& bs = ctx->scratch.b[20];
+    DevBuf& bp = ctx->scratch.b[23];
+    NRG_TRY(bs.ensure(sizeof(HostSeg) * ns));
+    NRG_TRY(bp.ensure(sizeof(long long) * ns));
+    NRG_TRY(h2d_async(ctx, bs.p, segs.data(), sizeof(HostSeg) * ns));
+    NRG_TRY(h2d_async(ctx, bp.p, prefix.data(), sizeof(long long) * ns));
+    const long long grid = std::min<long long>((total + 255) / 256, 148LL * 16);
+    k_gather_segs<<<(unsigned)grid, 256, 0, ctx->stream>>>(src, dst, ld, bs.as<HostSeg>(), bp.as<long long>(), ns,
+                                                          total);
+    ctx->launches++;
+    NRG_CUDA_TRY(cudaGetLastError());
+    *bytes = total * (long long)sizeof(double);
     return NRG_OK;
 }
 

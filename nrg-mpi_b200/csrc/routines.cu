@@ -707,13 +707,12 @@ int run_spec_jobs(nrg_context* ctx, const IterView& it, std::vector<SpecJob>& jo
 
 }  // namespace
 
-int spike_cfs_device(nrg_context* ctx, int iteration, const IterView& it, int nb_old,
-                     const double* d_IMSold, const double* d_rdm, double* d_binPos,
-                     double* d_binNeg, double* d_tot) {
-    const Model& M = ctx->model;
+namespace {
+// spikeCFS jobs (calculateSpectrumDGEMM.F90:364-536): every discarded block l with the kept
+// sector k = l + positive / negative operation of matrix type m
+std::vector<SpecJob> cfs_jobs(const Model& M, const IterView& it) {
     const Sectors& S = *it.S;
     const int nVar = S.nVar;
-    (void)d_rdm;
     std::vector<SpecJob> jobs;
     std::vector<int> q(nVar);
     for (int l = 0; l < S.nsub; ++l) {
@@ -737,20 +736,19 @@ int spike_cfs_device(nrg_context* ctx, int iteration, const IterView& it, int nb
             }
         }
     }
-    return run_spec_jobs(ctx, it, jobs, nb_old, d_IMSold, M.scale(iteration), M.numberOfBin(),
-                         d_binPos, d_binNeg, d_tot);
+    return jobs;
 }
 
-int spike_t0_device(nrg_context* ctx, int iteration, const IterView& it,
-                    const std::vector<int>& gs_sectors, int nb_old, const double* d_IMSold,
-                    double* d_binPos, double* d_binNeg) {
-    const Model& M = ctx->model;
+// spikeZeroTemperature jobs (calculateSpectrumDGEMM.F90:56-211): per ground-state sector,
+// the excited sector of each matrix type and sign
+std::vector<SpecJob> t0_jobs(const Model& M, const IterView& it, const std::vector<int>& gs_sectors) {
     const Sectors& S = *it.S;
     const int nVar = S.nVar;
     const double pf = (double)gs_sectors.size();
     std::vector<SpecJob> jobs;
     std::vector<int> q(nVar);
     for (int g : gs_sectors) {
+        if (g < 0 || g >= S.nsub) continue;
         for (int part = 0; part < 2; ++part) {
             const std::vector<int>& ops = part == 0 ? M.pos_op : M.neg_op;
             for (int m = 0; m < M.nMat; ++m) {
@@ -769,6 +767,50 @@ int spike_t0_device(nrg_context* ctx, int iteration, const IterView& it,
             }
         }
     }
+    return jobs;
+}
+}  // namespace
+
+std::vector<HostSeg> spike_ims_segs(const Model& M, const IterView& it, const std::vector<int>* gs_sectors,
+                                    int nb_old) {
+    const Sectors& S = *it.S;
+    const int nOps = S.nOps;
+    const long long nbo = nb_old;
+    const std::vector<SpecJob> jobs = gs_sectors ? t0_jobs(M, it, *gs_sectors) : cfs_jobs(M, it);
+    std::vector<HostSeg> segs;
+    std::vector<long long> seen;
+    for (const auto& j : jobs)
+        for (int a = 0; a < nOps; ++a) {
+            const int ck = S.cnt(j.k, a), cl = S.cnt(j.l, a);
+            if (ck == 0 || cl == 0) continue;
+            const long long rk = S.refBase[(size_t)j.k * nOps + a], rl = S.refBase[(size_t)j.l * nOps + a];
+            if (rk < 0 || rl < 0 || rk + ck > nbo || rl + cl > nbo) continue;   // rejected by run_spec_jobs
+            // part 0 reads IMS(rows of l, columns of k, m), part 1 IMS(rows of k, columns of l, m)
+            const long long r0 = j.part == 0 ? rl : rk, c0 = j.part == 0 ? rk : rl;
+            const int nr = j.part == 0 ? cl : ck, nc = j.part == 0 ? ck : cl;
+            const long long key = ((long long)j.m * nbo + c0) * nbo + r0;
+            if (std::find(seen.begin(), seen.end(), key) != seen.end()) continue;
+            seen.push_back(key);
+            segs.push_back({r0 + c0 * nbo + (long long)j.m * nbo * nbo, nr, nc});
+        }
+    return segs;
+}
+
+int spike_cfs_device(nrg_context* ctx, int iteration, const IterView& it, int nb_old,
+                     const double* d_IMSold, const double* d_rdm, double* d_binPos,
+                     double* d_binNeg, double* d_tot) {
+    const Model& M = ctx->model;
+    (void)d_rdm;
+    std::vector<SpecJob> jobs = cfs_jobs(M, it);
+    return run_spec_jobs(ctx, it, jobs, nb_old, d_IMSold, M.scale(iteration), M.numberOfBin(),
+                         d_binPos, d_binNeg, d_tot);
+}
+
+int spike_t0_device(nrg_context* ctx, int iteration, const IterView& it,
+                    const std::vector<int>& gs_sectors, int nb_old, const double* d_IMSold,
+                    double* d_binPos, double* d_binNeg) {
+    const Model& M = ctx->model;
+    std::vector<SpecJob> jobs = t0_jobs(M, it, gs_sectors);
     DevBuf& tot = ctx->scratch.b[22];
     NRG_TRY(tot.ensure(sizeof(double) * 2 * std::max(M.nMat, 1)));
     return run_spec_jobs(ctx, it, jobs, nb_old, d_IMSold, M.scale(iteration), M.numberOfBin(),
