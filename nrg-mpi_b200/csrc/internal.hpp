@@ -81,6 +81,8 @@ struct Sectors {
     int build(int nsub, const int* si, int nb, const int* bi, int nVar, int nOps);
     int upload(nrg_context* ctx);
     int find(const int* q) const;       // findSubspace: first sector with these qn, or -1
+    std::vector<int> qnHash;            // open-addressing index of the sectors by qn (find)
+    static unsigned long long hash_qn(const int* q, int nVar);
     int cnt(int s, int a) const { return lstOff[s * nOps + a + 1] - lstOff[s * nOps + a]; }
 };
 

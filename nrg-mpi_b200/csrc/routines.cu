@@ -83,6 +83,7 @@ int Model::numberOfBin() const {
 int Sectors::build(int nsub_, const int* si, int nb_, const int* bi, int nVar_, int nOps_) {
     nsub = nsub_; nb = nb_; nVar = nVar_; nOps = nOps_;
     const int rs = nVar + 3;
+    qnHash.clear();   // rebuilt below once the table is valid
     qn.assign((size_t)nsub * nVar, 0);
     dim.assign(nsub, 0);
     start.assign(nsub, 0);
@@ -106,6 +107,23 @@ int Sectors::build(int nsub_, const int* si, int nb_, const int* bi, int nVar_, 
         acc += (long long)dim[s] * dim[s];
     }
     sizeV = acc;
+    // index by quantum numbers: the first sector of each qn (findSubspace semantics)
+    {
+        size_t cap = 16;
+        while (cap < 4 * (size_t)nsub) cap <<= 1;
+        qnHash.assign(cap, -1);
+        for (int s = 0; s < nsub; ++s) {
+            const int* q = &qn[(size_t)s * nVar];
+            for (size_t x = hash_qn(q, nVar) & (cap - 1);; x = (x + 1) & (cap - 1)) {
+                const int o = qnHash[x];
+                if (o < 0) { qnHash[x] = s; break; }
+                bool eq = true;
+                for (int v = 0; v < nVar; ++v)
+                    if (qn[(size_t)o * nVar + v] != q[v]) { eq = false; break; }
+                if (eq) break;   // an earlier sector has these qn: it stays the one found
+            }
+        }
+    }
     rowOp.resize(nb); rowRef.resize(nb); rowVar.resize(nb);
     for (int i = 0; i < nb; ++i) {
         rowRef[i] = bi[(size_t)i * rs + nVar] - 1;
@@ -222,14 +240,34 @@ int h2d_async(nrg_context* ctx, void* dst, const void* src, size_t bytes) {
     return NRG_OK;
 }
 
+unsigned long long Sectors::hash_qn(const int* q, int nVar) {
+    unsigned long long h = 1469598103934665603ULL;   // FNV-1a over the quantum numbers
+    for (int v = 0; v < nVar; ++v) {
+        h ^= (unsigned long long)(unsigned)q[v];
+        h *= 1099511628211ULL;
+    }
+    return h;
+}
+
 int Sectors::find(const int* q) const {
-    for (int s = 0; s < nsub; ++s) {
+    if (qnHash.empty()) {
+        for (int s = 0; s < nsub; ++s) {
+            bool eq = true;
+            for (int v = 0; v < nVar; ++v)
+                if (qn[(size_t)s * nVar + v] != q[v]) { eq = false; break; }
+            if (eq) return s;
+        }
+        return -1;
+    }
+    const size_t mask = qnHash.size() - 1;
+    for (size_t x = hash_qn(q, nVar) & mask;; x = (x + 1) & mask) {
+        const int s = qnHash[x];
+        if (s < 0) return -1;
         bool eq = true;
         for (int v = 0; v < nVar; ++v)
             if (qn[(size_t)s * nVar + v] != q[v]) { eq = false; break; }
         if (eq) return s;
     }
-    return -1;
 }
 
 int check_device_status(nrg_context* ctx) {
