@@ -46,7 +46,7 @@ import ctypes
 import math
 import os
 import subprocess
-from typing import Dict, List, Optional
+from typing import Dict, List, Optional, Tuple
 
 import numpy as np
 import scipy.linalg
@@ -168,6 +168,7 @@ class State:
         self.thermo: Dict[int, tuple] = {}
         self.flow: Dict[int, np.ndarray] = {}
         self.ground_state_energy: Dict[int, float] = {}
+        self.emin: Dict[int, float] = {}          # minimum before the shift (FDM energies)
         self.kept: Dict[int, int] = {}
         self.rdm_trace: Dict[int, float] = {}
         self.sum_warnings: List[tuple] = []
@@ -439,6 +440,7 @@ def diagonalization(st: State, iteration: int) -> None:
         E[s0:s0 + d] = w
         ev[c0:c0 + d * d] = V.ravel(order="F")
     st.ground_state_energy[iteration] = float(E[0])                       # :470
+    st.emin[iteration] = float(np.min(E))
     E = E - np.min(E)                                                    # :472
     E[E <= NUMERICAL_THRESHOLD] = 0.0                                     # :473-475
     st.eigenvalue = E
@@ -1072,6 +1074,178 @@ def run(directory: str, spectrum: bool = True, literal: bool = False,
         for it in range(st.startTrancation, st.nIter + 1):    # main.F90:204-224
             cfs_spectrum_calculation(st, it, literal=literal)
     return st
+
+
+# ------------------------------------------------------------------------------------
+# full-density-matrix (FDM) spectrum at temperature T.  The reference has none (its
+# spectrum is the T = 0 CFS one); restated from the published method: Weichselbaum and
+# von Delft, PRL 99, 076402 (2007), with the complete basis of Anders and Schiller, PRL
+# 95, 196801 (2005).
+# ------------------------------------------------------------------------------------
+def _shell(st: State, N: int) -> dict:
+    """Shell N from the restore store: per sector its energies by eigenvector column, the
+    kept column count (kept columns come first: a sector keeps its lowest states) and
+    the eigenvector block."""
+    nVar = st.nVar
+    R = get_restore(st, N)
+    si, bo, E = R["subspaceInfo"], R["basis_output"], R["eigenvalue"]
+    nsub = si.shape[0]
+    dims = si[:, nVar].astype(np.int64)
+    Ecol = [np.zeros(int(d)) for d in dims]
+    kept = np.zeros(nsub, dtype=np.int64)
+    last = N == st.nIter
+    for i in range(R["numberOfBasis_full"]):
+        s = _find_subspace(si, nVar, bo[i, :nVar])
+        c = int(bo[i, nVar]) - 1
+        Ecol[s][c] = E[i]
+        if i < R["numberOfBasis"] and not last:
+            kept[s] += 1
+    for s in range(nsub):
+        assert np.all(np.diff(Ecol[s]) >= -1e-12)
+    V = [R["eigenvector"][int(si[s, nVar + 1]) - 1:int(si[s, nVar + 1]) - 1 + int(dims[s]) ** 2]
+         .reshape((int(dims[s]), int(dims[s])), order="F") for s in range(nsub)]
+    return dict(R=R, si=si, dims=dims, Ecol=Ecol, kept=kept, V=V)
+
+
+def fdm_weights(st: State, T: float, shells: Dict[int, dict]) -> Tuple[Dict[int, list], float]:
+    """Boltzmann weight of every discarded state in the full density matrix,
+    P_s = d^(N_max - N) exp(-eps_s / T) / Z, with eps_s = scale(N) E_s + C_N the energy
+    on one scale for all shells (C_N = C_(N-1) + scale(N) min(H_N), the shifts the
+    iterations subtract) and d = local states per site.  Returns P[N][sector] (per
+    discarded column, kept columns 0) and ln Z."""
+    N0, Nmax = st.startTrancation, st.nIter
+    # C_N measured from C_Nmax: C_N - C_Nmax = -sum_(N' > N) scale(N') min(H_N'), small
+    # numbers, so that eps / T keeps its precision at low T
+    Cs = {Nmax: 0.0}
+    for N in range(Nmax - 1, st.first - 1, -1):
+        Cs[N] = Cs[N + 1] - st.scale(N + 1) * st.emin[N + 1]
+    logs = []
+    for N in range(N0, Nmax + 1):
+        sh = shells[N]
+        for s, Ec in enumerate(sh["Ecol"]):
+            k = int(sh["kept"][s])
+            eps = st.scale(N) * Ec[k:] + Cs[N]
+            logs.append((Nmax - N) * math.log(st.nOps) - eps / T)
+    allv = np.concatenate(logs) if logs else np.zeros(0)
+    lmax = float(np.max(allv))
+    lnZ = lmax + math.log(float(np.sum(np.exp(allv - lmax))))
+    P: Dict[int, list] = {}
+    for N in range(N0, Nmax + 1):
+        sh = shells[N]
+        P[N] = []
+        for s, Ec in enumerate(sh["Ecol"]):
+            k = int(sh["kept"][s])
+            p = np.zeros(len(Ec))
+            eps = st.scale(N) * Ec[k:] + Cs[N]
+            p[k:] = np.exp((Nmax - N) * math.log(st.nOps) - eps / T - lnZ)
+            P[N].append(p)
+    return P, lnZ
+
+
+def fdm_density(st: State, shells: Dict[int, dict], P: Dict[int, list]) -> Dict[int, list]:
+    """Kept-space reduced density matrices R_N (per kept sector, columns in eigenvector
+    order) by the backward recursion of reducedDensityMatrixDGEMM.F90:164-297, each
+    child sector carrying its kept block R_(N+1) and the weights P of its discarded
+    columns: R_S(N) = sum_op A_op blockdiag(R_child, diag(P_child)) A_op^T."""
+    nVar, nOps = st.nVar, st.nOps
+    N0, Nmax = st.startTrancation, st.nIter
+    R: Dict[int, list] = {}
+    for N in range(Nmax - 1, N0 - 1, -1):
+        sh, ch = shells[N], shells[N + 1]
+        csi, cbi = ch["si"], ch["R"]["basis_input"]
+        R[N] = []
+        for S in range(len(sh["dims"])):
+            n = int(sh["kept"][S])
+            rho = np.zeros((n, n))
+            if n == 0:
+                R[N].append(rho)
+                continue
+            qS = sh["si"][S, :nVar].astype(np.int64)
+            for op in range(nOps):
+                c = _find_subspace(csi, nVar, qS - st.operation[op, :nVar])
+                if c is None:
+                    continue
+                dc = int(ch["dims"][c])
+                b0 = int(csi[c, nVar + 2]) - 1
+                var = cbi[b0:b0 + dc, nVar + 1]
+                opr = cbi[b0:b0 + dc, nVar + 2] - 1
+                A = np.zeros((n, dc))
+                for il in range(n):
+                    hit = np.nonzero((var == il + 1) & (opr == op))[0]
+                    if len(hit):
+                        A[il, :] = ch["V"][c][int(hit[0]), :]
+                kc = int(ch["kept"][c])
+                Dm = np.diag(P[N + 1][c])
+                if kc > 0:
+                    Dm[:kc, :kc] = R[N + 1][c]
+                rho += A @ Dm @ A.T
+            R[N].append(rho)
+    return R
+
+
+def fdm_spectrum(st: State, T: float):
+    """FDM bins at temperature T (same grid and two-bin split as the CFS bins).  Per
+    shell N and matrix type m, for each sector x and y = x + positive operation of m,
+    M = <y|d^dag|x> (spectrumElementDGEMM) over all columns; the pairs not both kept
+    contribute rho_x M^2 (particle added to x) and rho_y M^2 (particle taken from y) at
+    omega = scale(N) (E_y - E_x), in the bins of the sign of omega, rho = P on discarded
+    states and the matrix R on kept ones (the kept-discarded terms with R are the CFS
+    terms).  Returns (binPos, binNeg, diagnostics)."""
+    nVar = st.nVar
+    N0, Nmax = st.startTrancation, st.nIter
+    shells = {N: _shell(st, N) for N in range(N0, Nmax + 1)}
+    P, lnZ = fdm_weights(st, T, shells)
+    Rk = fdm_density(st, shells, P)
+    # at every shell, the kept-space trace plus the weight of the states discarded up to
+    # and including it is the whole trace, 1
+    traces = {}
+    done = 0.0
+    for N in range(N0, Nmax + 1):
+        done += sum(float(np.sum(p)) for p in P[N])
+        traces[N] = done + (sum(float(np.trace(r)) for r in Rk[N]) if N < Nmax else 0.0)
+    nbin = st.numberOfBin
+    binPos = np.zeros((nbin * st.nMat, 2), order="F")
+    binNeg = np.zeros((nbin * st.nMat, 2), order="F")
+    binPos[:, 0] = st.binPos[:, 0]
+    binNeg[:, 0] = st.binNeg[:, 0]
+    for N in range(N0, Nmax + 1):
+        sh = shells[N]
+        si, R = sh["si"], sh["R"]
+        sc = st.scale(N)
+        for x in range(len(sh["dims"])):
+            qx = si[x, :nVar].astype(np.int64)
+            for m in range(st.nMat):
+                y = _find_subspace(si, nVar, qx + st.pos_op[m])
+                if y is None:
+                    continue
+                dx, dy = int(sh["dims"][x]), int(sh["dims"][y])
+                M = spectrum_element_dgemm(st, R, y, dy, 0, x, dx, 0, m)      # (dy, dx)
+                kx, ky = int(sh["kept"][x]), int(sh["kept"][y])
+                Ex, Ey = sh["Ecol"][x], sh["Ecol"][y]
+                w = (Ey[:, None] - Ex[None, :]) * sc                            # omega
+                en = np.abs(w)
+                M2 = M * M
+                notkk = np.ones((dy, dx), dtype=bool)
+                notkk[:ky, :kx] = False
+                # rho_x: P on discarded columns of x; R_x on kept columns (rows y discarded)
+                wpos = M2 * P[N][x][None, :]
+                if kx > 0:
+                    wpos[ky:, :kx] = M[ky:, :kx] * (M[ky:, :kx] @ Rk[N][x])
+                wneg = M2 * P[N][y][:, None]
+                if ky > 0:
+                    wneg[:ky, kx:] = M[:ky, kx:] * (Rk[N][y] @ M[:ky, kx:])
+                # both terms sit at omega = E_y - E_x: negative frequencies go to the
+                # negative bins (at omega = 0 the x term to the positive, the y term to
+                # the negative ones, as the T = 0 routines bin them)
+                xpos = (w >= 0.0) & notkk
+                ypos = (w > 0.0) & notkk
+                xneg = (w < 0.0) & notkk
+                yneg = (w <= 0.0) & notkk
+                bin_spikes(st, binPos, np.concatenate([en[xpos], en[ypos]]),
+                           np.concatenate([wpos[xpos], wneg[ypos]]), m)
+                bin_spikes(st, binNeg, np.concatenate([en[xneg], en[yneg]]),
+                           np.concatenate([wpos[xneg], wneg[yneg]]), m)
+    return binPos, binNeg, dict(lnZ=lnZ, traces=traces)
 
 
 def spectrum_lines(st: State):

@@ -154,3 +154,47 @@ def test_log_gaussian_broadening_keeps_the_weight():
     # A(w) peaks at E, and w A(w) (the density in ln w) at E exp(b^2/2)
     assert abs(w[np.argmax(Ap)] / 2e-4 - 1.0) < 0.01
     assert abs(w[np.argmax(Ap * w)] / (2e-4 * np.exp(0.18)) - 1.0) < 0.01
+
+
+def test_fdm_zero_temperature_limit_is_the_cfs_spectrum(truncated_run):
+    # FDM at T << the last shell's scale: only the ground states of the last iteration
+    # carry weight, and the bins are the reference-semantics CFS bins
+    st = truncated_run
+    bp, bn, diag = O.fdm_spectrum(st, 1e-3 * st.scale(st.nIter))
+    assert np.max(np.abs(bp[:, 1] - st.binPos[:, 1])) <= 1e-8
+    assert np.max(np.abs(bn[:, 1] - st.binNeg[:, 1])) <= 1e-8
+    assert max(abs(t - 1.0) for t in diag["traces"].values()) <= 1e-12
+
+
+@pytest.mark.parametrize("factor", [0.1, 1.0, 30.0])
+def test_fdm_sum_rule_and_traces_at_finite_temperature(truncated_run, factor):
+    st = truncated_run
+    bp, bn, diag = O.fdm_spectrum(st, factor * st.scale(st.nIter))
+    nbin = st.numberOfBin
+    for m in range(st.nMat):
+        tot = bp[m * nbin:(m + 1) * nbin, 1].sum() + bn[m * nbin:(m + 1) * nbin, 1].sum()
+        assert abs(tot - 1.0) <= 1e-12
+    assert max(abs(t - 1.0) for t in diag["traces"].values()) <= 1e-12
+
+
+def test_fdm_known_answer_noninteracting_at_finite_temperature(tmp_path):
+    # U = 0 without truncation: the single-particle spectral function does not depend on
+    # T, so the FDM bins at any T equal |phi_k(d)|^2 at eps_k (positive or negative)
+    inp = model.siam(U=0.0, Gamma=0.05, eps_d=0.0, Lambda=2.5, n_keep=100000, n_iterations=5)
+    d = write_case(inp, str(tmp_path))
+    st = O.run(d, spectrum=False)
+    st.startTrancation = st.nIter          # one shell: the last, every state discarded
+    n_sites = st.nIter - st.first + 1
+    eps, phi = np.linalg.eigh(_free_chain(inp, n_sites))
+    nbin = st.numberOfBin
+    exp_pos = np.zeros((nbin * st.nMat, 2), order="F")
+    exp_neg = np.zeros((nbin * st.nMat, 2), order="F")
+    w = phi[0, :] ** 2
+    for m in range(st.nMat):
+        pos = eps > 0
+        O.bin_spikes(st, exp_pos, eps[pos].copy(), w[pos].copy(), m)
+        O.bin_spikes(st, exp_neg, -np.abs(eps[~pos]).copy(), w[~pos].copy(), m)
+    for factor in (0.3, 3.0):
+        bp, bn, _ = O.fdm_spectrum(st, factor * st.scale(st.nIter))
+        assert np.max(np.abs(bp[:, 1] - exp_pos[:, 1])) < 1e-10
+        assert np.max(np.abs(bn[:, 1] - exp_neg[:, 1])) < 1e-10
