@@ -268,6 +268,15 @@ typedef struct nrg_run_input {
     int32_t host_drop_in;                 /* 1: every routine goes through the drop-in
                                              entry points with host arrays (the
                                              Fortran caller's data flow)               */
+    double temperature;                   /* 0: the reference's T = 0 CFS spectrum;
+                                             > 0 (device-resident run only): the
+                                             full-density-matrix spectrum at this
+                                             temperature (energy units of the band
+                                             half-width D), no reference counterpart:
+                                             Weichselbaum and von Delft, PRL 99,
+                                             076402 (2007); rdmTrace then holds, per
+                                             shell N, the kept-space trace plus the
+                                             weight discarded up to N (1)              */
 } nrg_run_input;
 
 typedef struct nrg_run_output {

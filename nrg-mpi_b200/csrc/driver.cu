@@ -145,6 +145,7 @@ void record_flow(nrg_run_output* out, int idx, const std::vector<double>& E, con
 
 struct IterRec {
     int nb_full = 0, nb_kept = 0;
+    double emin = 0.0;   // the minimum the shift subtracted (full-density-matrix energies)
     std::vector<int> kept;
     std::vector<double> Esec;
     std::vector<long long> rdm_off;
@@ -234,6 +235,7 @@ int run_device(nrg_context* ctx, const nrg_run_input* in, nrg_run_output* out, c
         NRG_TRY(diag_device(ctx, it, S, dEold, nb_old, dIMold, bV.as<double>(), bE.as<double>(), &dout));
         if (out && out->thermo) NRG_TRY(run_thermo(ctx, S, bE.as<double>(), dThermo + 3 * (size_t)idx));
         if (out && out->groundStateEnergy) out->groundStateEnergy[idx] = dout.groundStateEnergy;
+        R.emin = dout.emin;
         R.Esec.resize(nb);
         NRG_CUDA_TRY(cudaMemcpyAsync(R.Esec.data(), bE.p, sizeof(double) * nb, cudaMemcpyDeviceToHost, st));
         NRG_CUDA_TRY(cudaStreamSynchronize(st));
@@ -292,14 +294,74 @@ int run_device(nrg_context* ctx, const nrg_run_input* in, nrg_run_output* out, c
     double* dNeg = dPos + nw;
     NRG_TRY(run_fill(ctx, dPos, (long long)(2 * nw), 0.0));
 
+    // ---- full-density-matrix weights (temperature > 0; no reference counterpart) ----
+    // P_s = d^(N_max - N) exp(-eps_s / T) / Z for the states discarded at shell N (all
+    // states at the last shell), eps_s = scale(N) E_s + C_N with C_N - C_Nmax =
+    // -sum_(N' > N) scale(N') min(H_N'): every shell on one energy scale measured from the
+    // last shell's origin (small offsets keep eps / T precise at low T)
+    const bool fdm = spectrum && in->temperature > 0.0;
+    const int N0 = std::min(startTrancation, nIter);
+    if (fdm && N0 <= first) {
+        nrg_set_error_message("the full-density-matrix spectrum needs at least two NRG iterations");
+        return NRG_ERR_UNSUPPORTED;
+    }
+    std::vector<long long> pOff(nIt, -1);
+    std::vector<double> pShell(nIt, 0.0);
+    DevBuf& bP = ctx->slot(11);
+    if (fdm) {
+        std::vector<double> C(nIt, 0.0);
+        for (int N = nIter - 1; N >= first; --N) C[N - first] = C[N + 1 - first] - M.scale(N + 1) * recs[N + 1 - first].emin;
+        const double T = in->temperature, lnd = std::log((double)M.nOps);
+        long long tot = 0;
+        for (int N = N0; N <= nIter; ++N) { pOff[N - first] = tot; tot += recs[N - first].nb_full; }
+        std::vector<double> hP((size_t)std::max(tot, 1LL), 0.0);
+        double vmax = -INFINITY;
+        for (int pass = 0; pass < 2; ++pass) {
+            double sum = 0.0;
+            for (int N = N0; N <= nIter; ++N) {
+                const IterRec& R = recs[N - first];
+                const Sectors& S = ctx->iter_sectors[N - first];
+                const double sc = M.scale(N);
+                for (int s = 0; s < S.nsub; ++s)
+                    for (int c = (N == nIter ? 0 : R.kept[s]); c < S.dim[s]; ++c) {
+                        const double v = (nIter - N) * lnd - (sc * R.Esec[S.start[s] + c] + C[N - first]) / T;
+                        if (pass == 0) vmax = std::max(vmax, v);
+                        else hP[pOff[N - first] + S.start[s] + c] = v;
+                        if (pass == 1) sum += std::exp(v - vmax);
+                    }
+            }
+            if (pass == 1) {
+                const double lnZ = vmax + std::log(sum);
+                for (int N = N0; N <= nIter; ++N) {
+                    const IterRec& R = recs[N - first];
+                    const Sectors& S = ctx->iter_sectors[N - first];
+                    double ps = 0.0;
+                    for (int s = 0; s < S.nsub; ++s)
+                        for (int c = (N == nIter ? 0 : R.kept[s]); c < S.dim[s]; ++c) {
+                            double& p = hP[pOff[N - first] + S.start[s] + c];
+                            p = std::exp(p - lnZ);
+                            ps += p;
+                        }
+                    pShell[N - first] = ps;
+                }
+            }
+        }
+        NRG_TRY(bP.ensure(sizeof(double) * hP.size()));
+        NRG_CUDA_TRY(cudaMemcpyAsync(bP.p, hP.data(), sizeof(double) * hP.size(), cudaMemcpyHostToDevice, st));
+        NRG_CUDA_TRY(cudaStreamSynchronize(st));
+        ctx->h2d += (long long)(sizeof(double) * hP.size());
+    }
+    auto dP = [&](int idx) -> const double* { return fdm ? bP.as<double>() + pOff[idx] : nullptr; };
+
     // ---- backward reduced density matrices (initializeReducedDensity, main.F90:188-201) ----
     DevBuf& bRdm = ctx->slot(5);
     const int last = nIter - first;
-    if (spectrum && flag_truncation) {
+    if (spectrum && (flag_truncation || fdm)) {
         long long off = 0;
-        for (int N = nIter; N >= startTrancation; --N) {
+        for (int N = nIter; N >= N0; --N) {
             IterRec& R = recs[N - first];
             R.rdm_off.assign(R.kept.size(), -1);
+            if (fdm && N == nIter) continue;   // the last shell is all discarded: weights only
             for (size_t s = 0; s < R.kept.size(); ++s)
                 if (R.kept[s] > 0) { R.rdm_off[s] = off; off += (long long)R.kept[s] * R.kept[s]; }
         }
@@ -310,7 +372,7 @@ int run_device(nrg_context* ctx, const nrg_run_input* in, nrg_run_output* out, c
         int deg = 0;
         for (int i = 0; i < RL.nb_full; ++i) deg += RL.Esec[i] < 1.0e-8;
         const double inv = 1.0 / (double)deg;
-        for (int s = 0; s < SL.nsub; ++s)
+        for (int s = 0; s < SL.nsub && !fdm; ++s)
             for (int p = 0; p < RL.kept[s]; ++p)
                 if (RL.Esec[SL.start[s] + p] < 1.0e-8) {
                     NRG_TRY(h2d_async(ctx, bRdm.as<double>() + RL.rdm_off[s] + (long long)p * RL.kept[s] + p, &inv,
@@ -319,13 +381,17 @@ int run_device(nrg_context* ctx, const nrg_run_input* in, nrg_run_output* out, c
                 }
         DevBuf& bTr = ctx->slot(7);
         NRG_TRY(bTr.ensure(sizeof(double) * (size_t)(nIter + 2)));
-        for (int N = nIter - 1; N >= startTrancation; --N) {
+        for (int N = nIter - 1; N >= N0; --N) {
             IterView P, C;
             const int ip = N - first, ic = N + 1 - first;
             P.S = &ctx->iter_sectors[ip]; P.kept = recs[ip].kept; P.d_V = slotV(ip).as<double>();
             P.d_rdm = bRdm.as<double>(); P.rdm_off = recs[ip].rdm_off;
             C.S = &ctx->iter_sectors[ic]; C.kept = recs[ic].kept; C.d_V = slotV(ic).as<double>();
             C.d_rdm = bRdm.as<double>(); C.rdm_off = recs[ic].rdm_off;
+            if (fdm) {
+                C.d_P = dP(ic);
+                if (N + 1 == nIter) C.kept.assign(C.kept.size(), 0);
+            }
             NRG_TRY(rdm_step_device(ctx, P, C, bRdm.as<double>(), bTr.as<double>() + N));
         }
         if (out && out->rdmTrace) {
@@ -333,13 +399,32 @@ int run_device(nrg_context* ctx, const nrg_run_input* in, nrg_run_output* out, c
             NRG_CUDA_TRY(cudaMemcpyAsync(tr.data(), bTr.p, sizeof(double) * (nIter + 1), cudaMemcpyDeviceToHost, st));
             NRG_CUDA_TRY(cudaStreamSynchronize(st));
             ctx->d2h += (long long)sizeof(double) * (nIter + 1);
-            for (int N = 0; N <= nIter; ++N) out->rdmTrace[N] = (N >= startTrancation && N < nIter) ? tr[N] : NAN;
+            double done = 0.0;   // FDM: weight discarded up to and including shell N
+            for (int N = 0; N <= nIter; ++N) {
+                if (fdm && N >= N0) done += pShell[N - first];
+                const bool has = (N >= (fdm ? N0 : startTrancation)) && N < nIter;
+                out->rdmTrace[N] = has ? tr[N] + (fdm ? done : 0.0) : NAN;
+            }
         }
     }
     NRG_CUDA_TRY(cudaEventRecord(ev[2], st));
 
+    // ---- full-density-matrix spectrum (temperature > 0) ----
+    if (fdm) {
+        DevBuf& bTot = ctx->slot(10);
+        NRG_TRY(bTot.ensure(sizeof(double) * 4 * M.nMat));
+        for (int N = N0; N <= nIter; ++N) {
+            const int idx = N - first;
+            IterView V;
+            V.S = &ctx->iter_sectors[idx]; V.kept = recs[idx].kept; V.d_V = slotV(idx).as<double>();
+            V.d_Esec = slotE(idx).as<double>(); V.nb_kept = recs[idx].nb_kept;
+            V.d_rdm = bRdm.as<double>(); V.rdm_off = recs[idx].rdm_off; V.d_P = dP(idx);
+            NRG_TRY(spike_fdm_device(ctx, N, V, recs[idx - 1].nb_kept, slotS(idx - 1).as<double>(), N == nIter,
+                                     dPos, dNeg, bTot.as<double>()));
+        }
+    }
     // ---- CFS spectrum (main.F90:204-224) ----
-    if (spectrum) {
+    if (spectrum && !fdm) {
         DevBuf& bTmp = ctx->slot(8);
         DevBuf& bTot = ctx->slot(10);
         NRG_TRY(bTmp.ensure(sizeof(double) * 2 * nw));

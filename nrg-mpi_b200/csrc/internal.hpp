@@ -90,7 +90,7 @@ struct Sectors {
 // the context
 // ------------------------------------------------------------------------------------
 struct Scratch {
-    DevBuf b[40];
+    DevBuf b[48];
 };
 
 }  // namespace nrg
@@ -208,11 +208,22 @@ struct SpikeProb {
     long long ek_off, el_off; // offsets into the energy array (k states, l states)
     int kk, nl, m, toPos, lstride;  // lstride: 1 for consecutive l energies, 0 for a fixed one
     double sgn, cE, scale, invpf;
+    // full-density-matrix mode: spikes of the sign of this job's bins only; weights
+    // P (same offsets as the energies) on both sides; k_is_y: k holds the extra particle
+    int fdm, k_is_y;
 };
 int run_spikes(nrg_context* ctx, std::vector<SpikeProb>& probs, const double* d_work,
                const double* d_E, int nbin, int nMat, double* d_binPos, double* d_binNeg,
-               double* d_tot);
+               double* d_tot, const double* d_P = nullptr);
 int run_fill(nrg_context* ctx, double* p, long long n, double v);
+// dst[i + j n] = V[rows[i] + (c0 + j) ld] * P[j]: gathered rows of a column range scaled by
+// per-column weights, for many blocks in one launch
+struct ScaledGather {
+    long long dst, v, rows, p;
+    int n, nc, ld, c0;
+};
+int run_scaled_gather(nrg_context* ctx, const std::vector<ScaledGather>& jobs, double* dst, const double* V,
+                      const int* rows, const double* P);
 // betabar of module.F90:652, a default-real literal (single precision 0.8 widened)
 constexpr double kBetabar = (double)0.8f;
 // calcThermo (module.F90:1931-1982) of one iteration: d_out[0..2] = Cn, Sn, Xn
@@ -229,7 +240,8 @@ int run_gather_rows(nrg_context* ctx, double* dst, long long dst_ld, const doubl
 
 // ---- internal routines shared by the ABI and the driver (routines.cu) ------------------
 struct DiagOut {
-    double groundStateEnergy = 0.0;
+    double groundStateEnergy = 0.0;   // eigenvalue(1) before the shift (the reference's)
+    double emin = 0.0;                // the minimum subtracted by the shift
 };
 // diagonalization for one iteration; d_Eold/d_IMold/d_V/d_E are device pointers.
 int diag_device(nrg_context* ctx, int iteration, Sectors& S, const double* d_Eold, int nb_old,
@@ -247,6 +259,7 @@ int invmat_spec_device(nrg_context* ctx, const Sectors& S, const std::vector<int
 struct IterView {
     const Sectors* S = nullptr;
     std::vector<int> kept;            // kept per sector
+    const double* d_P = nullptr;      // full-density-matrix weights by state (sector order), or null
     const double* d_V = nullptr;      // all eigenvector blocks
     const double* d_Esec = nullptr;   // eigenvalues in sector order
     int nb_kept = 0;
@@ -266,6 +279,11 @@ int spike_cfs_device(nrg_context* ctx, int iteration, const IterView& it, int nb
 int spike_t0_device(nrg_context* ctx, int iteration, const IterView& it,
                     const std::vector<int>& gs_sectors, int nb_old, const double* d_IMSold,
                     double* d_binPos, double* d_binNeg);
+// full-density-matrix spectrum of one shell: the kept-discarded terms (the CFS products,
+// with the discarded states' weights added) and the discarded-discarded terms, each
+// spike in the bins of the sign of its frequency; last: every state is discarded
+int spike_fdm_device(nrg_context* ctx, int iteration, const IterView& it, int nb_old, const double* d_IMSold,
+                     bool last, double* d_binPos, double* d_binNeg, double* d_tot);
 
 int check_device_status(nrg_context* ctx);
 

@@ -156,7 +156,7 @@ __global__ void __launch_bounds__(256) k_spikes(const SpikeProb* __restrict__ pr
                                                 const long long* __restrict__ tilePrefix, int nprob,
                                                 const double* __restrict__ W, const double* __restrict__ E,
                                                 int nbin, double* __restrict__ binPos, double* __restrict__ binNeg,
-                                                double* __restrict__ tot) {
+                                                double* __restrict__ tot, const double* __restrict__ Pw) {
     __shared__ double hist[kSpkWin];
     __shared__ double rs[8];
     __shared__ int rmin[8], rmax[8];
@@ -188,9 +188,22 @@ __global__ void __launch_bounds__(256) k_spikes(const SpikeProb* __restrict__ pr
         if (k1 < pr.kk && l < pr.nl) {
             const long long loc = (long long)k1 + (long long)l * pr.kk;
             const double sv = W[pr.s_off + loc];
-            const double w = (pr.y_off >= 0) ? sv * W[pr.y_off + loc] : sv * sv * pr.invpf;
             const double el = E[pr.el_off + (long long)l * pr.lstride];
             const double en = pr.sgn * ((ek - pr.cE * el) * pr.scale);
+            double w;
+            if (!pr.fdm) {
+                w = (pr.y_off >= 0) ? sv * W[pr.y_off + loc] : sv * sv * pr.invpf;
+            } else {
+                // both terms of a pair sit at omega = en: the term of the state that gains
+                // the particle (x) enters the positive bins for omega >= 0, the term of the
+                // state that loses it (y) for omega > 0; the rest goes to the negative bins
+                const bool inx = pr.toPos ? (en >= 0.0) : (en < 0.0);
+                const bool iny = pr.toPos ? (en > 0.0) : (en <= 0.0);
+                const double pk = Pw[pr.ek_off + k1], pl = Pw[pr.el_off + (long long)l * pr.lstride];
+                const double px = pr.k_is_y ? pl : pk, py = pr.k_is_y ? pk : pl;
+                w = sv * sv * ((inx ? px : 0.0) + (iny ? py : 0.0));
+                if (pr.y_off >= 0 && (pr.k_is_y ? iny : inx)) w += sv * W[pr.y_off + loc];
+            }
             wsum += w;
             // binningSpike
             const double position = (log10(fabs(en)) - (-15.0)) * 1000.0 + 1.0;
@@ -349,6 +362,24 @@ __global__ void k_gather_segs(const double* __restrict__ src, double* __restrict
     }
 }
 
+__global__ void k_scaled_gather(const ScaledGather* __restrict__ jobs, const long long* __restrict__ prefix, int nj,
+                                long long total, double* __restrict__ dst, const double* __restrict__ V,
+                                const int* __restrict__ rows, const double* __restrict__ P) {
+    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < total;
+         e += (long long)gridDim.x * blockDim.x) {
+        int lo = 0, hi = nj - 1;
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (prefix[mid] <= e) lo = mid; else hi = mid - 1;
+        }
+        const ScaledGather g = jobs[lo];
+        const long long loc = e - prefix[lo];
+        const int i = (int)(loc % g.n), j = (int)(loc / g.n);
+        const int r = rows[g.rows + i];
+        dst[g.dst + loc] = V[g.v + (long long)r + (long long)(g.c0 + j) * g.ld] * P[g.p + j];
+    }
+}
+
 __global__ void k_fill(double* p, long long n, double v) {
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) p[i] = v;
 }
@@ -466,7 +497,7 @@ int run_im_gather(nrg_context* ctx, const Sectors& S, std::vector<ImGatherProb>&
 
 int run_spikes(nrg_context* ctx, std::vector<SpikeProb>& probs, const double* d_work,
                const double* d_E, int nbin, int nMat, double* d_binPos, double* d_binNeg,
-               double* d_tot) {
+               double* d_tot, const double* d_P) {
     (void)nMat;
     const int np = (int)probs.size();
     if (np == 0) return NRG_OK;
@@ -484,8 +515,13 @@ int run_spikes(nrg_context* ctx, std::vector<SpikeProb>& probs, const double* d_
     NRG_TRY(dq.ensure(sizeof(long long) * np));
     NRG_TRY(h2d_async(ctx, dp.p, probs.data(), sizeof(SpikeProb) * np));
     NRG_TRY(h2d_async(ctx, dq.p, prefix.data(), sizeof(long long) * np));
+    for (const auto& p : probs)
+        if (p.fdm && !d_P) {
+            nrg_set_error_message("full-density-matrix spikes without weights");
+            return NRG_ERR_INVALID;
+        }
     k_spikes<<<(unsigned)total, 256, 0, ctx->stream>>>(dp.as<SpikeProb>(), dq.as<long long>(), np, d_work, d_E, nbin,
-                                                     d_binPos, d_binNeg, d_tot);
+                                                     d_binPos, d_binNeg, d_tot, d_P);
     ctx->launches++;
     NRG_CUDA_TRY(cudaGetLastError());
     return NRG_OK;
@@ -546,6 +582,31 @@ int run_gather_segs(nrg_context* ctx, const double* src, double* dst, long long 
     ctx->launches++;
     NRG_CUDA_TRY(cudaGetLastError());
     *bytes = total * (long long)sizeof(double);
+    return NRG_OK;
+}
+
+int run_scaled_gather(nrg_context* ctx, const std::vector<ScaledGather>& jobs, double* dst, const double* V,
+                      const int* rows, const double* P) {
+    const int nj = (int)jobs.size();
+    if (nj == 0) return NRG_OK;
+    std::vector<long long> prefix(nj);
+    long long total = 0;
+    for (int i = 0; i < nj; ++i) {
+        prefix[i] = total;
+        total += (long long)jobs[i].n * jobs[i].nc;
+    }
+    if (total == 0) return NRG_OK;
+    DevBuf& bj = ctx->scratch.b[40];
+    DevBuf& bp = ctx->scratch.b[41];
+    NRG_TRY(bj.ensure(sizeof(ScaledGather) * nj));
+    NRG_TRY(bp.ensure(sizeof(long long) * nj));
+    NRG_TRY(h2d_async(ctx, bj.p, jobs.data(), sizeof(ScaledGather) * nj));
+    NRG_TRY(h2d_async(ctx, bp.p, prefix.data(), sizeof(long long) * nj));
+    const long long grid = std::min<long long>((total + 255) / 256, 148LL * 16);
+    k_scaled_gather<<<(unsigned)grid, 256, 0, ctx->stream>>>(bj.as<ScaledGather>(), bp.as<long long>(), nj, total, dst,
+                                                            V, rows, P);
+    ctx->launches++;
+    NRG_CUDA_TRY(cudaGetLastError());
     return NRG_OK;
 }
 

@@ -425,7 +425,10 @@ int diag_device(nrg_context* ctx, int iteration, Sectors& S, const double* d_Eol
     NRG_CUDA_TRY(cudaMemcpyAsync(mg, bmin.p, sizeof(double) * 2, cudaMemcpyDeviceToHost, ctx->stream));
     ctx->d2h += sizeof(mg);
     NRG_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
-    if (out) out->groundStateEnergy = mg[1];
+    if (out) {
+        out->groundStateEnergy = mg[1];
+        out->emin = mg[0];
+    }
     return check_device_status(ctx);
 }
 
@@ -591,14 +594,15 @@ int rdm_step_device(nrg_context* ctx, const IterView& P, const IterView& C, doub
         for (int op = 0; op < nOps; ++op) {
             for (int v = 0; v < nVar; ++v) q[v] = SP.qn[(size_t)s * nVar + v] - M.op(op, v);
             const int c = SC.find(q.data());
-            if (c < 0 || C.kept[c] == 0) continue;
+            // a child contributes its kept block and, with weights, its discarded columns
+            if (c < 0 || (C.kept[c] == 0 && (!C.d_P || SC.dim[c] == C.kept[c]))) continue;
             if (SC.cnt(c, op) != n) {
                 nrg_set_error_message("rdm: child sector rows (%d) differ from kept states (%d)",
                                       SC.cnt(c, op), n);
                 return NRG_ERR_INVALID;
             }
             links.push_back({s, c, op, colOff});
-            colOff += C.kept[c];
+            colOff += C.d_P ? SC.dim[c] : C.kept[c];
         }
         tS[s] = ttot;
         ttot += (long long)n * colOff;
@@ -606,9 +610,24 @@ int rdm_step_device(nrg_context* ctx, const IterView& P, const IterView& C, doub
     }
     NRG_TRY(T.ensure(sizeof(double) * (size_t)std::max(ttot, 1LL)));
     const int* dl = SC.d_lst.as<int>();
+    std::vector<ScaledGather> sg;
+    std::vector<GemmProblem> p3;
     for (const auto& lk : links) {
         const int n = P.kept[lk.S], c = lk.c, kc = C.kept[c], dc = SC.dim[c];
         const int* rows = dl + SC.lstOff[(size_t)c * nOps + lk.op];
+        if (C.d_P && dc > kc) {
+            // discarded columns of the child with their weights: rho_S += (A_D diag(P)) A_D^T
+            const long long toff = tS[lk.S] + (lk.colOff + kc) * n;
+            sg.push_back({toff, SC.ce[c], SC.lstOff[(size_t)c * nOps + lk.op], SC.start[c] + kc, n, dc - kc, dc, kc});
+            GemmProblem D;
+            std::memset(&D, 0, sizeof(D));
+            D.M = n; D.N = n; D.K = dc - kc; D.alpha = 1.0; D.beta = 1.0;
+            D.A = T.as<double>() + toff; D.a_si = 1; D.a_sk = n;
+            D.B = C.d_V + SC.ce[c] + (long long)kc * dc; D.b_sk = dc; D.b_ji = rows; D.b_sj = 1;
+            D.C = d_rdm + P.rdm_off[lk.S]; D.c_si = n; D.c_sj = 1;
+            p3.push_back(D);
+        }
+        if (kc == 0) continue;
         // T_op = A_op rho_c, A_op(i, k) = V_c(rows[i], k); rho_c row-major
         GemmProblem A;
         std::memset(&A, 0, sizeof(A));
@@ -629,6 +648,19 @@ int rdm_step_device(nrg_context* ctx, const IterView& P, const IterView& C, doub
     for (const auto& b : blocks) NRG_TRY(run_fill(ctx, d_rdm + b.off, (long long)b.n * b.n, 0.0));
     NRG_TRY(launch_ggemm(ctx, p1, 8));
     for (int op = 0; op < nOps; ++op) NRG_TRY(launch_ggemm(ctx, p2[op], 10));
+    if (!sg.empty()) {
+        NRG_TRY(run_scaled_gather(ctx, sg, T.as<double>(), C.d_V, dl, C.d_P));
+        // the products of one parent block are added one launch after another
+        std::vector<std::vector<GemmProblem>> byop(nOps);
+        std::vector<int> cnt(SP.nsub, 0);
+        for (const auto& D : p3) {
+            int s = 0;
+            for (const auto& b : blocks)
+                if (d_rdm + b.off == D.C) { s = b.s; break; }
+            byop[cnt[s]++].push_back(D);
+        }
+        for (int op = 0; op < nOps; ++op) NRG_TRY(launch_ggemm(ctx, byop[op], 14));
+    }
     if (d_trace_out && !blocks.empty()) {
         std::vector<long long> offs;
         std::vector<int> dims;
@@ -657,6 +689,8 @@ struct SpecJob {
     int toPos;
     long long rdm_off; // -1: T=0 weights
     long long t_off, s_off, y_off;
+    int kc0 = 0;       // first k column (discarded-discarded jobs)
+    int fdm = 0;       // full-density-matrix weights
 };
 
 int run_spec_jobs(nrg_context* ctx, const IterView& it, std::vector<SpecJob>& jobs, int nb_old,
@@ -712,7 +746,7 @@ int run_spec_jobs(nrg_context* ctx, const IterView& it, std::vector<SpecJob>& jo
         GemmProblem Q;
         std::memset(&Q, 0, sizeof(Q));
         Q.M = j.kk; Q.N = j.nl; Q.K = S.dim[k]; Q.alpha = 1.0; Q.beta = 0.0;
-        Q.A = it.d_V + S.ce[k]; Q.a_si = S.dim[k]; Q.a_sk = 1;
+        Q.A = it.d_V + S.ce[k] + (long long)j.kc0 * S.dim[k]; Q.a_si = S.dim[k]; Q.a_sk = 1;
         Q.B = T.as<double>() + j.t_off; Q.b_sk = 1; Q.b_sj = S.dim[k];
         Q.C = W.as<double>() + j.s_off; Q.c_si = 1; Q.c_sj = j.kk;
         p2.push_back(Q);
@@ -734,13 +768,14 @@ int run_spec_jobs(nrg_context* ctx, const IterView& it, std::vector<SpecJob>& jo
     for (const auto& j : jobs) {
         SpikeProb s;
         s.s_off = j.s_off; s.y_off = j.y_off;
-        s.ek_off = S.start[j.k];
+        s.ek_off = S.start[j.k] + j.kc0;
         s.el_off = S.start[j.l] + j.c0;
         s.kk = j.kk; s.nl = j.nl; s.m = j.m; s.toPos = j.toPos; s.lstride = 1;
         s.sgn = j.sgn; s.cE = j.cE; s.scale = sc; s.invpf = j.invpf;
+        s.fdm = j.fdm; s.k_is_y = j.part == 0 ? 1 : 0;
         sp.push_back(s);
     }
-    return run_spikes(ctx, sp, W.as<double>(), it.d_Esec, nbin, M.nMat, d_binPos, d_binNeg, d_tot);
+    return run_spikes(ctx, sp, W.as<double>(), it.d_Esec, nbin, M.nMat, d_binPos, d_binNeg, d_tot, it.d_P);
 }
 
 }  // namespace
@@ -840,6 +875,48 @@ int spike_cfs_device(nrg_context* ctx, int iteration, const IterView& it, int nb
     const Model& M = ctx->model;
     (void)d_rdm;
     std::vector<SpecJob> jobs = cfs_jobs(M, it);
+    return run_spec_jobs(ctx, it, jobs, nb_old, d_IMSold, M.scale(iteration), M.numberOfBin(),
+                         d_binPos, d_binNeg, d_tot);
+}
+
+int spike_fdm_device(nrg_context* ctx, int iteration, const IterView& it, int nb_old, const double* d_IMSold,
+                     bool last, double* d_binPos, double* d_binNeg, double* d_tot) {
+    const Model& M = ctx->model;
+    const Sectors& S = *it.S;
+    const int nVar = S.nVar;
+    std::vector<SpecJob> jobs;
+    // kept-discarded pairs: the CFS products, the discarded state's weight added to the
+    // kept-space density term; every job once per sign of the bins
+    if (!last)
+        for (SpecJob j : cfs_jobs(M, it))
+            for (int pos = 0; pos < 2; ++pos) {
+                j.fdm = 1;
+                j.toPos = pos;
+                jobs.push_back(j);
+            }
+    // discarded-discarded pairs: y = x + positive operation of m, <y|d^dag|x> over the
+    // discarded columns of both (every column at the last shell)
+    auto first_d = [&](int s) { return last ? 0 : it.kept[s]; };
+    std::vector<int> q(nVar);
+    for (int x = 0; x < S.nsub; ++x) {
+        const int dx = S.dim[x] - first_d(x);
+        if (dx <= 0) continue;
+        for (int m = 0; m < M.nMat; ++m) {
+            for (int v = 0; v < nVar; ++v) q[v] = S.qn[(size_t)x * nVar + v] + M.pos_op[(size_t)m + (size_t)v * M.nMat];
+            const int y = S.find(q.data());
+            if (y < 0) continue;
+            const int dy = S.dim[y] - first_d(y);
+            if (dy <= 0) continue;
+            SpecJob j;
+            j.k = y; j.kc0 = first_d(y); j.kk = dy;
+            j.l = x; j.c0 = first_d(x); j.nl = dx;
+            j.m = m; j.part = 0; j.sgn = 1.0; j.cE = 1.0; j.invpf = 0.0; j.rdm_off = -1; j.fdm = 1;
+            for (int pos = 0; pos < 2; ++pos) {
+                j.toPos = pos;
+                jobs.push_back(j);
+            }
+        }
+    }
     return run_spec_jobs(ctx, it, jobs, nb_old, d_IMSold, M.scale(iteration), M.numberOfBin(),
                          d_binPos, d_binNeg, d_tot);
 }

@@ -125,7 +125,7 @@ class RunInput(ctypes.Structure):
     _fields_ = [
         ("numberOfBasis", c_int32), ("basis_output", _pi32), ("eigenvalue", _pf64),
         ("invariant_matrix", _pf64), ("invariant_matrix_spectrum", _pf64),
-        ("spectrum", c_int32), ("host_drop_in", c_int32),
+        ("spectrum", c_int32), ("host_drop_in", c_int32), ("temperature", c_double),
     ]
 
 
@@ -456,17 +456,19 @@ class Context:
 
     # ------------------------------------------------------------------
     def run(self, spectrum: bool = True, flow_stride: int = 8, final_capacity: int = 0,
-            host_drop_in: bool = False):
+            host_drop_in: bool = False, temperature: float = 0.0):
         """main.F90:142-252; returns bins and per-iteration statistics.
 
         ``host_drop_in=True`` drives every routine through its drop-in entry point with
         host arrays (the Fortran caller's data flow) instead of keeping state on the device.
+        ``temperature > 0`` (device-resident run) gives the full-density-matrix spectrum
+        at that temperature instead of the reference's T = 0 CFS spectrum.
         """
-        args = self._run_args(spectrum, flow_stride, final_capacity, host_drop_in)
+        args = self._run_args(spectrum, flow_stride, final_capacity, host_drop_in, temperature)
         self._check(self.lib.nrg_run(self._h, ctypes.byref(args["ri"]), ctypes.byref(args["ro"])), "nrg_run")
         return self._run_result(args)
 
-    def _run_args(self, spectrum, flow_stride, final_capacity, host_drop_in):
+    def _run_args(self, spectrum, flow_stride, final_capacity, host_drop_in, temperature=0.0):
         """Input and output records of nrg_run for this context (arrays kept alive here)."""
         inp = self.inp
         nb = inp.numberOfBasis
@@ -474,7 +476,8 @@ class Context:
                  im=_f64f(inp.invariant_matrix),
                  ims=_f64f(inp.invariant_matrix_spectrum) if inp.flag_spectrum else None)
         a["ri"] = RunInput(nb, _p(a["bo"], c_int32), _p(a["E"], c_double), _p(a["im"], c_double),
-                           _p(a["ims"], c_double), int(bool(spectrum)), int(bool(host_drop_in)))
+                           _p(a["ims"], c_double), int(bool(spectrum)), int(bool(host_drop_in)),
+                           float(temperature))
         nit = inp.numberOfIteration - inp.indexOfFirstIteration + 1
         nmat = max(inp.numberOfMatrix, 1)
         nbin_cap = 20001

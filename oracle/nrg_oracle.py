@@ -833,7 +833,8 @@ def bin_spikes(st: State, container: np.ndarray, energy: np.ndarray, weight: np.
     off = m * nbin - 1
     # same-bin spikes: all weight to i1
     idx_a = np.where(one, i1, pr) + off
-    w_a = np.where(one, weight, weight * (1.0 - wb))
+    with np.errstate(invalid="ignore"):   # wb is NaN at E = 0, where the one-bin branch is taken
+        w_a = np.where(one, weight, weight * (1.0 - wb))
     np.add.at(container[:, 1], idx_a, w_a)
     two = ~one
     if np.any(two):
