@@ -21,6 +21,9 @@ the backward reduced density matrices and the T=0 CFS spectrum on the reference'
   threads) on a bounded sample of the same sweep.
 * --impl reference: the oracle port timed per NRG iteration of the same sweep (steps are
   full-size iterations), rank 0 only.
+* fdm: the same sweep with the full-density-matrix spectrum and density matrices at
+  T = 1e-6 (the workload table's temperature; no reference counterpart: the reference's
+  spectrum is the T = 0 CFS one), one warm-up and two event-timed sweeps.
 * many_instance: independent impurity models side by side (nrg_run_batch): the 27 draws
   with N_keep <= 1024 of the seeded 64-SIAM sweep (50 iterations each, T=0 CFS), run one
   at a time and then 8 in flight; wall clock around each batch with the device
@@ -66,6 +69,7 @@ def parse():
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-cpu", action="store_true")
     p.add_argument("--no-many", action="store_true")
+    p.add_argument("--no-fdm", action="store_true")
     # profiling helpers: a shorter sweep of the same model (not the headline workload)
     p.add_argument("--iterations", type=int, default=None)
     p.add_argument("--n-keep", type=int, default=None)
@@ -337,6 +341,29 @@ def main():
                "path": "drop-in entry points with host arrays (Fortran caller's data flow; module "
                        "arrays in pinned host memory, allocated in one untimed warm-up run)",
                "max_bin_diff_vs_device_resident": same}
+    fdm = None
+    if not args.no_fdm:
+        T_fdm = 1e-6
+        ctx.run(spectrum=True, temperature=T_fdm)
+        torch.cuda.synchronize(dev)
+        s2, e2 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        fph = []
+        s2.record(stream)
+        for _ in range(2):
+            rf = ctx.run(spectrum=True, temperature=T_fdm)
+            fph.append(rf["phaseSeconds"].copy())
+        e2.record(stream)
+        torch.cuda.synchronize(dev)
+        fms = s2.elapsed_time(e2) / 2
+        nbf = rf["numberOfBin"]
+        fsum = [float(rf["binPos"][m * nbf:(m + 1) * nbf, 1].sum() + rf["binNeg"][m * nbf:(m + 1) * nbf, 1].sum())
+                for m in range(inp.numberOfMatrix)]
+        fp = np.mean(np.array(fph), axis=0)
+        fdm = {"temperature": T_fdm, "ms_per_sweep": fms, "iterations_per_s": n_it * 1e3 / fms,
+               "phase_seconds": {"nrg_sweep": float(fp[0]), "rdm": float(fp[1]), "fdm_spectrum": float(fp[2])},
+               "sum_rule": fsum,
+               "shell_trace_max_dev": float(np.nanmax(np.abs(rf["rdmTrace"] - 1.0))),
+               "timing": "CUDA events on the library's stream, 2 sweeps after 1 warm-up"}
     many = None if args.no_many else many_instance(torch, dev, rank, world, dist)
     if rank == 0:
         clocks = clk.summary()
@@ -387,6 +414,7 @@ def main():
             "clocks": clocks,
             "e2e": e2e,
             "cpu_baseline": cpu,
+            "fdm": fdm,
             "many_instance": many,
         }
         print(json.dumps(line), flush=True)
