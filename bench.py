@@ -24,6 +24,9 @@ the backward reduced density matrices and the T=0 CFS spectrum on the reference'
 * fdm: the same sweep with the full-density-matrix spectrum and density matrices at
   T = 1e-6 (the workload table's temperature; no reference counterpart: the reference's
   spectrum is the T = 0 CFS one), one warm-up and two event-timed sweeps.
+* n_keep_4096: the larger SIAM workload (Lambda=2, U=0.3, Gamma=0.03, eps_d=-0.15,
+  N_keep=4096, 60 iterations, sectors of order up to ~1300), one warm-up and one
+  event-timed sweep on the same stream.
 * many_instance: independent impurity models side by side (nrg_run_batch): the 27 draws
   with N_keep <= 1024 of the seeded 64-SIAM sweep (50 iterations each, T=0 CFS), run one
   at a time and then 8 in flight; wall clock around each batch with the device
@@ -70,6 +73,7 @@ def parse():
     p.add_argument("--no-cpu", action="store_true")
     p.add_argument("--no-many", action="store_true")
     p.add_argument("--no-fdm", action="store_true")
+    p.add_argument("--no-nk4096", action="store_true")
     # profiling helpers: a shorter sweep of the same model (not the headline workload)
     p.add_argument("--iterations", type=int, default=None)
     p.add_argument("--n-keep", type=int, default=None)
@@ -193,6 +197,43 @@ def many_instance(torch, dev, rank, world, dist, concurrency=8):
             "instances": len(sample), "iterations": its, "unit": "iterations/s",
             "sequential": its / times[1], "batched": its / times[concurrency], "concurrency": concurrency,
             "ranks": world, "timing": "wall clock around each batch, device synchronised, max over ranks"}
+
+
+def larger_workload(torch, dev, local, stream):
+    """One sweep of the N_keep = 4096 SIAM workload after one warm-up sweep, CUDA events
+    on the library's stream; the context's device storage is released afterwards."""
+    from nrg_b200 import Context, model
+    inp = model.config(3)
+    n_it = inp.numberOfIteration - inp.indexOfFirstIteration + 1
+    c = Context(local)
+    try:
+        c.set_model(inp)
+        c.set_stream(stream.cuda_stream)
+        c.run(spectrum=True)
+        torch.cuda.synchronize(dev)
+        c.set_profiling(True)
+        c.reset_stats()
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s.record(stream)
+        r = c.run(spectrum=True)
+        e.record(stream)
+        torch.cuda.synchronize(dev)
+        st = c.stats()
+        c.set_profiling(False)
+        ms = s.elapsed_time(e)
+        nbin = r["numberOfBin"]
+        sums = [float(r["binPos"][m * nbin:(m + 1) * nbin, 1].sum() + r["binNeg"][m * nbin:(m + 1) * nbin, 1].sum())
+                for m in range(inp.numberOfMatrix)]
+        ph = r["phaseSeconds"]
+        return {"workload": "SIAM Lambda=2.0 U=0.3 Gamma=0.03 eps_d=-0.15 N_keep=4096, 60 iterations "
+                            "+ backward RDM + T=0 CFS spectrum",
+                "ms_per_sweep": ms, "iterations_per_s": n_it * 1e3 / ms,
+                "phase_seconds": {"nrg_sweep": float(ph[0]), "rdm": float(ph[1]), "cfs_spectrum": float(ph[2])},
+                "eigensolver_ms_per_window": st["syev_ms"] / max(st["syev_launches"], 1),
+                "sum_rule": sums,
+                "timing": "CUDA events on the library's stream, 1 sweep after 1 warm-up"}
+    finally:
+        c.close()
 
 
 def cpu_sample(n_timed=3):
@@ -364,6 +405,7 @@ def main():
                "sum_rule": fsum,
                "shell_trace_max_dev": float(np.nanmax(np.abs(rf["rdmTrace"] - 1.0))),
                "timing": "CUDA events on the library's stream, 2 sweeps after 1 warm-up"}
+    nk4096 = None if args.no_nk4096 else larger_workload(torch, dev, local, stream)
     many = None if args.no_many else many_instance(torch, dev, rank, world, dist)
     if rank == 0:
         clocks = clk.summary()
@@ -415,6 +457,7 @@ def main():
             "e2e": e2e,
             "cpu_baseline": cpu,
             "fdm": fdm,
+            "n_keep_4096": nk4096,
             "many_instance": many,
         }
         print(json.dumps(line), flush=True)

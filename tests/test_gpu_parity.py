@@ -155,14 +155,17 @@ def test_spikes_per_iteration(driven):
     assert worst <= BIN_TOL, worst
 
 
-@pytest.mark.parametrize("case", ["nkeep512", "bench_sizes"])
+@pytest.mark.parametrize("case", ["nkeep512", "bench_sizes", "nkeep4096"])
 def test_large_sector_diagonalization(ctx_factory, case):
     # N_keep = 512: sectors of order up to ~200; the benchmark workload (N_keep = 2048)
-    # reaches order ~700 by its sixth diagonalization: both take the large-sector eigensolver
+    # reaches order ~700 by its sixth diagonalization; N_keep = 4096 reaches orders 1225
+    # and 1308 (above 1024) in its sixth and seventh: all take the large-sector eigensolver
     if case == "nkeep512":
         inp = small_siam(n_keep=512, n_iterations=9)
-    else:
+    elif case == "bench_sizes":
         inp = model.config(2, n_iterations=7)
+    else:
+        inp = model.config(3, n_iterations=7)
     d = write_case(inp)
     st = O.State(d)
     ctx = ctx_factory(model.read_inputs(d))
@@ -181,7 +184,7 @@ def test_large_sector_diagonalization(ctx_factory, case):
             worst_v = max(worst_v, subspace_err(Bg, Bo, st.eigenvalue[s0:s0 + dd]))
             largest = max(largest, dd)
         O.postprocess(st, it)
-    assert largest > (600 if case == "bench_sizes" else 128)
+    assert largest > {"nkeep512": 128, "bench_sizes": 600, "nkeep4096": 1200}[case]
     assert worst_e <= EIG_TOL, worst_e
     assert worst_v <= VEC_TOL, worst_v
 
