@@ -81,11 +81,16 @@ nrg_context::~nrg_context() {
     if (ev_join2) cudaEventDestroy(ev_join2);
     if (aux2) cudaStreamDestroy(aux2);
     if (ev_join_hi) cudaEventDestroy(ev_join_hi);
+    for (cudaEvent_t e : {ev_evals_hi, ev_evals2, ev_evals_host})
+        if (e) cudaEventDestroy(e);
+    h_small.release();
+    h_evals.release();
     if (aux_hi) cudaStreamDestroy(aux_hi);
-    for (auto& t : pending_tri) {
-        cudaEventDestroy(t.a);
-        cudaEventDestroy(t.b);
-    }
+    for (auto* pl : {&pending_tri, &pending_syev})
+        for (auto& t : *pl) {
+            cudaEventDestroy(t.a);
+            cudaEventDestroy(t.b);
+        }
     if (stage_host) cudaFreeHost(stage_host);
 }
 
@@ -269,6 +274,7 @@ int nrg_context_get_stats(const nrg_context* ctx, nrg_stats* out) {
 
 int nrg_context_reset_stats(nrg_context* ctx) {
     if (!ctx) return NRG_ERR_INVALID;
+    NRG_TRY(flush_profile_timers(ctx));   // timers of an unfinished run are dropped below
     ctx->syev_launches = 0;
     ctx->syev_ms = 0.0;
     ctx->syev_flops = 0.0;

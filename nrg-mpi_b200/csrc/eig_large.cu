@@ -795,10 +795,10 @@ __global__ void __launch_bounds__(256) k_bt_prep(const LSec* __restrict__ secs, 
 }
 
 // Z(:, c0 .. c0+CBK-1) <- H_0 ... H_{n-2} Z(:, ...) panel by panel (last panel first), the
-// column block resident in shared memory; the result and the eigenvalues go to the output
+// column block resident in shared memory; the result goes to the output
 template <int CBK>
 __global__ void __launch_bounds__(256, 1) k_bt_apply(const LSec* __restrict__ secs, int nsec, double* eigbuf,
-                                                     double* evals, double* wsd, int* wsi) {
+                                                     double* wsd, int* wsi) {
     constexpr int JPT = CBK / 4;       // columns per thread
     extern __shared__ double asm_[];
     int bid = blockIdx.x, s = 0;
@@ -886,17 +886,22 @@ __global__ void __launch_bounds__(256, 1) k_bt_apply(const LSec* __restrict__ se
     for (int j = 0; j < nc; ++j)
         for (int row = tid; row < n; row += 256)
             L.A[(size_t)row + (size_t)(c0 + j) * n] = Zs[(size_t)j * n + row];
-    for (int j = tid; j < nc; j += 256) evals[sec.e_off + c0 + j] = L.D[c0 + j];
 }
 
-__global__ void k_large_out(const LSec* __restrict__ secs, double* eigbuf, double* evals, double* wsd, int* wsi) {
+__global__ void k_large_out(const LSec* __restrict__ secs, double* eigbuf, double* wsd, int* wsi) {
     const LSec sec = secs[blockIdx.y];
     LView L = lview(sec, eigbuf, wsd, wsi);
     const long long n = sec.n, sq = n * n;
     for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < sq; e += (long long)gridDim.x * blockDim.x)
         L.A[e] = L.Z[e];
-    if (blockIdx.x == 0)
-        for (int i = threadIdx.x; i < sec.n; i += blockDim.x) evals[sec.e_off + i] = L.D[i];
+}
+
+// the eigenvalues (ascending, the divide and conquer's order) to the output, one block
+// per sector, as soon as the divide and conquer has finished
+__global__ void k_large_evals(const LSec* __restrict__ secs, double* eigbuf, double* evals, double* wsd, int* wsi) {
+    const LSec sec = secs[blockIdx.x];
+    LView L = lview(sec, eigbuf, wsd, wsi);
+    for (int i = threadIdx.x; i < sec.n; i += blockDim.x) evals[sec.e_off + i] = L.D[i];
 }
 
 }  // namespace
@@ -974,7 +979,8 @@ static int tri_cluster(nrg_context* ctx, const LSec* dsec, int ns, int maxn, dou
     return NRG_OK;
 }
 
-int syev_large(nrg_context* ctx, const std::vector<SyevSector>& in, double* d_V, double* d_E, int slot_base) {
+int syev_large(nrg_context* ctx, const std::vector<SyevSector>& in, double* d_V, double* d_E, int slot_base,
+               cudaEvent_t evals_ready) {
     const int ns = (int)in.size();
     if (ns == 0) return NRG_OK;
     cudaStream_t st = ctx->stream;
@@ -1148,6 +1154,11 @@ int syev_large(nrg_context* ctx, const std::vector<SyevSector>& in, double* d_V,
         NRG_CUDA_TRY(cudaGetLastError());
     }
 
+    k_large_evals<<<ns, TPB, 0, st>>>(dsec, d_V, d_E, wsd, wsi);
+    ctx->launches++;
+    NRG_CUDA_TRY(cudaGetLastError());
+    if (evals_ready) NRG_CUDA_TRY(cudaEventRecord(evals_ready, st));
+
     // ---- 3. back-transformation ----
     // one pass per column block with the block resident in shared memory, when it fits
     {
@@ -1168,10 +1179,10 @@ int syev_large(nrg_context* ctx, const std::vector<SyevSector>& in, double* d_V,
             const size_t sm = apply_smem(cbk);
             if (cbk == 16) {
                 NRG_TRY(raise_smem_limit((const void*)k_bt_apply<16>, sm));
-                k_bt_apply<16><<<nblk, 256, sm, st>>>(dsec, ns, d_V, d_E, wsd, wsi);
+                k_bt_apply<16><<<nblk, 256, sm, st>>>(dsec, ns, d_V, wsd, wsi);
             } else {
                 NRG_TRY(raise_smem_limit((const void*)k_bt_apply<8>, sm));
-                k_bt_apply<8><<<nblk, 256, sm, st>>>(dsec, ns, d_V, d_E, wsd, wsi);
+                k_bt_apply<8><<<nblk, 256, sm, st>>>(dsec, ns, d_V, wsd, wsi);
             }
             ctx->launches += 2;
             NRG_CUDA_TRY(cudaGetLastError());
@@ -1243,7 +1254,7 @@ int syev_large(nrg_context* ctx, const std::vector<SyevSector>& in, double* d_V,
         NRG_TRY(launch_ggemm(ctx, g2, gslot));
         NRG_TRY(launch_ggemm(ctx, g3, gslot));
     }
-    k_large_out<<<dim3(32, ns), TPB, 0, st>>>(dsec, d_V, d_E, wsd, wsi);
+    k_large_out<<<dim3(32, ns), TPB, 0, st>>>(dsec, d_V, wsd, wsi);
     ctx->launches++;
     NRG_CUDA_TRY(cudaGetLastError());
     return NRG_OK;

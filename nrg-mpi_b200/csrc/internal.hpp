@@ -131,6 +131,15 @@ struct nrg_context {
     // that timing does not stall the launch queue
     struct PendingTimer { cudaEvent_t a, b; double flops, bytes; };
     std::vector<PendingTimer> pending_tri;
+    std::vector<PendingTimer> pending_syev;   // eigensolver windows (flops only)
+    // early eigenvalues (device-resident sweep): each large-sector group records its
+    // event once the divide and conquer has written the eigenvalues; the caller's stream
+    // shifts them and copies them to pinned host memory (ev_evals_host) before it waits
+    // for the back-transformations, so the host bookkeeping of the next iteration runs
+    // while they finish
+    cudaEvent_t ev_evals_hi = nullptr, ev_evals2 = nullptr, ev_evals_host = nullptr;
+    nrg::HostBuf h_small;   // pinned: the shift's minimum and E(1), the status word
+    nrg::HostBuf h_evals;   // pinned: the shifted eigenvalues of the current iteration
     nrg::DevBuf& slot(size_t i) {
         if (store.size() <= i) store.resize(i + 1);
         return store[i];
@@ -185,15 +194,20 @@ int launch_ggemm(nrg_context* ctx, std::vector<GemmProblem>& probs, int scratch_
 // eigensolver for sectors of order > 128 across the whole GPU (eig_large.cu); the
 // descriptors use a_off / e_off / n only
 // (scratch slots slot_base .. slot_base + 6; on ctx->stream)
-int syev_large(nrg_context* ctx, const std::vector<SyevSector>& secs, double* d_V, double* d_E, int slot_base);
+// evals_ready (optional) is recorded on ctx->stream once the eigenvalues are in d_E,
+// before the back-transformation
+int syev_large(nrg_context* ctx, const std::vector<SyevSector>& secs, double* d_V, double* d_E, int slot_base,
+               cudaEvent_t evals_ready = nullptr);
 constexpr int kLargeSector = 128;
 
 // ---- kernels (kernels.cu) ------------------------------------------------------------
 int run_assemble(nrg_context* ctx, int iteration, const Sectors& S, const SyevSector* d_secs,
                  const long long* d_colPrefix, const int* d_secStart, int nsec, long long ncols,
                  const double* d_Eold, int nb_old, const double* d_IMold, double* d_V);
-int run_eig_finalize(nrg_context* ctx, double* d_E, int nb, long long sizeV, double* d_V,
-                     double* d_min_and_gs);
+// the shift of the eigenvalues (E -= min E, E <= 1e-12 -> 0; min and E(1) to
+// d_min_and_gs) and the chop of the eigenvectors (|V| < 1e-14 -> 0), on ctx->stream
+int run_eig_shift(nrg_context* ctx, double* d_E, int nb, double* d_min_and_gs);
+int run_eig_chop(nrg_context* ctx, long long sizeV, double* d_V);
 
 struct ImGatherProb {
     long long t_off;    // T (dL x kR) col-major
@@ -244,8 +258,43 @@ struct DiagOut {
     double emin = 0.0;                // the minimum subtracted by the shift
 };
 // diagonalization for one iteration; d_Eold/d_IMold/d_V/d_E are device pointers.
+// With h_E (pinned host, nb doubles) the call returns as soon as the shifted eigenvalues
+// are in h_E: the eigenvectors are still being formed on the device, ordered before
+// any later work on ctx->stream.
 int diag_device(nrg_context* ctx, int iteration, Sectors& S, const double* d_Eold, int nb_old,
-                const double* d_IMold, double* d_V, double* d_E, DiagOut* out);
+                const double* d_IMold, double* d_V, double* d_E, DiagOut* out, double* h_E = nullptr);
+// reads the profiling timers of completed eigensolver windows into the counters
+int flush_profile_timers(nrg_context* ctx);
+
+// ---- restart.dat of the CFS phase (restart.cu; module.F90:1710-1890) -------------------
+// one iteration of the restore stock as getRestore hands it to the spike routines
+struct RestoreView {
+    const int* si = nullptr;     // subspaceInfo [nsub*(nVar+3)]
+    const int* bi = nullptr;     // basis_input [nb_full*(nVar+3)]
+    const int* bo = nullptr;     // basis_output after the truncation reorder
+    const double* E = nullptr;   // eigenvalue [nb_full], same order as bo
+    const double* V = nullptr;   // eigenvector blocks [nV]
+    const double* ims = nullptr; // d† matrices of the kept states (nb, nb, nMat); none at the last iteration
+    long long nV = 0;
+    int nb = 0, nb_full = 0, nsub = 0;
+};
+// words of HamiltonianInfo_type (module.F90:722-760) read back by the drop-in replay
+constexpr int kHamiStartTrancation = 17, kHamiFlagTruncation = 18;
+struct RestartData {
+    int32_t iteration = 0;
+    int32_t hami[20];
+    int nb0 = 0;
+    std::vector<int32_t> restoreInfo, si, bi, bo, fsi, map;
+    std::vector<double> ims, ims0, E, V, rdm, binPos, binNeg;
+    std::vector<RestoreView> its;   // first .. nIter, pointing into the arrays above
+};
+void restart_hami(const Model& M, int numberOfBasis, int startTrancation, bool flag_truncation, int32_t hami[20]);
+// its: iterations first .. nIter; map: mapFullSubspaceInfo(-1:nIter); bins (nbin*nMat, 2)
+int restart_save(const char* path, const Model& M, int iteration, const int32_t hami[20],
+                 const std::vector<RestoreView>& its, int nb0, const double* ims0, const double* rdm, long long nrdm,
+                 const int* fsi, long long nfsi, const int* map, const double* binPos, const double* binNeg,
+                 int nbin);
+int restart_load(const char* path, const Model& M, int nbin, RestartData* D);
 
 // kept counts per sector from the kept prefix of basis_output (invariantMatrixDGEMM.F90:84-100)
 std::vector<int> kept_per_sector(const Sectors& S, int nb_kept, const int* basis_output_kept);

@@ -461,12 +461,17 @@ int run_assemble(nrg_context* ctx, int iteration, const Sectors& S, const SyevSe
     return NRG_OK;
 }
 
-int run_eig_finalize(nrg_context* ctx, double* d_E, int nb, long long sizeV, double* d_V,
-                     double* d_min_and_gs) {
+int run_eig_shift(nrg_context* ctx, double* d_E, int nb, double* d_min_and_gs) {
     k_min<<<1, 1024, 0, ctx->stream>>>(d_E, nb, d_min_and_gs);
     k_shift<<<grid_for(nb, 256), 256, 0, ctx->stream>>>(d_E, nb, d_min_and_gs);
+    ctx->launches += 2;
+    NRG_CUDA_TRY(cudaGetLastError());
+    return NRG_OK;
+}
+
+int run_eig_chop(nrg_context* ctx, long long sizeV, double* d_V) {
     k_chop<<<grid_for(sizeV, 256), 256, 0, ctx->stream>>>(d_V, sizeV);
-    ctx->launches += 3;
+    ctx->launches++;
     NRG_CUDA_TRY(cudaGetLastError());
     return NRG_OK;
 }

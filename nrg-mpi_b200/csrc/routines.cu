@@ -286,7 +286,8 @@ int check_device_status(nrg_context* ctx) {
 // diagonalization (diagonalization.F90:185-528)
 // ------------------------------------------------------------------------------------
 int diag_device(nrg_context* ctx, int iteration, Sectors& S, const double* d_Eold, int nb_old,
-                const double* d_IMold, double* d_V, double* d_E, DiagOut* out) {
+                const double* d_IMold, double* d_V, double* d_E, DiagOut* out, double* h_E) {
+    const bool early = h_E != nullptr;
     const int nsec = S.nsub;
     std::vector<int> order(nsec);
     std::iota(order.begin(), order.end(), 0);
@@ -348,32 +349,36 @@ int diag_device(nrg_context* ctx, int iteration, Sectors& S, const double* d_Eol
     // stream, and the sectors of order <= 128 (one block each) on the second stream.  The
     // largest sectors' pipeline sets the critical path; the blocks of the other groups
     // fill the SMs it leaves idle.
+    // With early eigenvalues the largest sectors always take their own stream, so that
+    // the caller's stream can pick up the eigenvalues before the back-transformations
+    // end; without a second large group that stream has the normal priority (the
+    // priority only orders the two large groups of one instance, and independent
+    // instances side by side should not all claim the greatest one).
     std::vector<SyevSector> g1, g2;
     for (const auto& q : large) (5 * q.n >= 4 * large[0].n ? g1 : g2).push_back(q);
     const bool fork_small = nsec > nlarge && nlarge > 0;
-    const bool fork_large = !g2.empty();
-    if (fork_small || fork_large) {
-        if (!ctx->aux) {
-            int lo = 0, hi = 0;
-            NRG_CUDA_TRY(cudaDeviceGetStreamPriorityRange(&lo, &hi));
-            NRG_CUDA_TRY(cudaStreamCreateWithFlags(&ctx->aux, cudaStreamNonBlocking));
-            NRG_CUDA_TRY(cudaStreamCreateWithFlags(&ctx->aux2, cudaStreamNonBlocking));
-            NRG_CUDA_TRY(cudaStreamCreateWithPriority(&ctx->aux_hi, cudaStreamNonBlocking, hi));
-            NRG_CUDA_TRY(cudaEventCreateWithFlags(&ctx->ev_fork, cudaEventDisableTiming));
-            NRG_CUDA_TRY(cudaEventCreateWithFlags(&ctx->ev_join, cudaEventDisableTiming));
-            NRG_CUDA_TRY(cudaEventCreateWithFlags(&ctx->ev_join2, cudaEventDisableTiming));
-            NRG_CUDA_TRY(cudaEventCreateWithFlags(&ctx->ev_join_hi, cudaEventDisableTiming));
-        }
-        NRG_CUDA_TRY(cudaEventRecord(ctx->ev_fork, ctx->stream));
+    const bool fork_large = !g2.empty() || (early && !g1.empty());
+    cudaStream_t s1 = nullptr;
+    if (!ctx->aux) {
+        int lo = 0, hi = 0;
+        NRG_CUDA_TRY(cudaDeviceGetStreamPriorityRange(&lo, &hi));
+        NRG_CUDA_TRY(cudaStreamCreateWithFlags(&ctx->aux, cudaStreamNonBlocking));
+        NRG_CUDA_TRY(cudaStreamCreateWithFlags(&ctx->aux2, cudaStreamNonBlocking));
+        NRG_CUDA_TRY(cudaStreamCreateWithPriority(&ctx->aux_hi, cudaStreamNonBlocking, hi));
+        for (cudaEvent_t* e : {&ctx->ev_fork, &ctx->ev_join, &ctx->ev_join2, &ctx->ev_join_hi, &ctx->ev_evals_hi,
+                               &ctx->ev_evals2, &ctx->ev_evals_host})
+            NRG_CUDA_TRY(cudaEventCreateWithFlags(e, cudaEventDisableTiming));
     }
+    if (fork_small || fork_large) NRG_CUDA_TRY(cudaEventRecord(ctx->ev_fork, ctx->stream));
     int rl = NRG_OK;
     if (fork_large) {
-        NRG_CUDA_TRY(cudaStreamWaitEvent(ctx->aux_hi, ctx->ev_fork, 0));
+        s1 = g2.empty() ? ctx->aux2 : ctx->aux_hi;
+        NRG_CUDA_TRY(cudaStreamWaitEvent(s1, ctx->ev_fork, 0));
         cudaStream_t caller = ctx->stream;
-        ctx->stream = ctx->aux_hi;
-        rl = syev_large(ctx, g1, d_V, d_E, 24);
+        ctx->stream = s1;
+        rl = syev_large(ctx, g1, d_V, d_E, 24, early && !g1.empty() ? ctx->ev_evals_hi : nullptr);
         ctx->stream = caller;
-        NRG_CUDA_TRY(cudaEventRecord(ctx->ev_join_hi, ctx->aux_hi));
+        NRG_CUDA_TRY(cudaEventRecord(ctx->ev_join_hi, s1));
     } else {
         rl = syev_large(ctx, g1, d_V, d_E, 24);
     }
@@ -384,43 +389,55 @@ int diag_device(nrg_context* ctx, int iteration, Sectors& S, const double* d_Eol
         ctx->launches++;
     }
     if (fork_small) NRG_CUDA_TRY(cudaEventRecord(ctx->ev_join, ctx->aux));
-    if (fork_large) {
+    const bool has_g2 = fork_large && !g2.empty();
+    if (has_g2) {
         NRG_CUDA_TRY(cudaStreamWaitEvent(ctx->aux2, ctx->ev_fork, 0));
         cudaStream_t caller = ctx->stream;
         ctx->stream = ctx->aux2;
-        if (rl == NRG_OK) rl = syev_large(ctx, g2, d_V, d_E, 31);
+        if (rl == NRG_OK) rl = syev_large(ctx, g2, d_V, d_E, 31, early ? ctx->ev_evals2 : nullptr);
         ctx->stream = caller;
         NRG_CUDA_TRY(cudaEventRecord(ctx->ev_join2, ctx->aux2));
-        NRG_CUDA_TRY(cudaStreamWaitEvent(ctx->stream, ctx->ev_join2, 0));
-        NRG_CUDA_TRY(cudaStreamWaitEvent(ctx->stream, ctx->ev_join_hi, 0));
     }
-    if (fork_small) NRG_CUDA_TRY(cudaStreamWaitEvent(ctx->stream, ctx->ev_join, 0));
     NRG_TRY(rl);
+    double* hs = nullptr;
+    if (early) {
+        // eigenvalues of every group -> shift -> host, then the eigenvectors' join
+        NRG_TRY(ctx->h_small.ensure(64));
+        hs = ctx->h_small.as<double>();
+        if (fork_large && !g1.empty()) NRG_CUDA_TRY(cudaStreamWaitEvent(ctx->stream, ctx->ev_evals_hi, 0));
+        if (has_g2) NRG_CUDA_TRY(cudaStreamWaitEvent(ctx->stream, ctx->ev_evals2, 0));
+        if (fork_small) NRG_CUDA_TRY(cudaStreamWaitEvent(ctx->stream, ctx->ev_join, 0));
+        NRG_TRY(run_eig_shift(ctx, d_E, S.nb, bmin.as<double>()));
+        NRG_CUDA_TRY(cudaMemcpyAsync(h_E, d_E, sizeof(double) * S.nb, cudaMemcpyDeviceToHost, ctx->stream));
+        NRG_CUDA_TRY(cudaMemcpyAsync(hs, bmin.p, sizeof(double) * 2, cudaMemcpyDeviceToHost, ctx->stream));
+        NRG_CUDA_TRY(cudaMemcpyAsync(hs + 2, ctx->d_status.p, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+        ctx->d2h += (long long)sizeof(double) * (S.nb + 2) + (long long)sizeof(int);
+        NRG_CUDA_TRY(cudaEventRecord(ctx->ev_evals_host, ctx->stream));
+    }
+    if (fork_large) NRG_CUDA_TRY(cudaStreamWaitEvent(ctx->stream, ctx->ev_join_hi, 0));
+    if (has_g2) NRG_CUDA_TRY(cudaStreamWaitEvent(ctx->stream, ctx->ev_join2, 0));
+    if (fork_small && !early) NRG_CUDA_TRY(cudaStreamWaitEvent(ctx->stream, ctx->ev_join, 0));
     if (ctx->profiling) {
         NRG_CUDA_TRY(cudaEventRecord(e1, ctx->stream));
-        NRG_CUDA_TRY(cudaEventSynchronize(e1));
-        float ms = 0.f;
-        NRG_CUDA_TRY(cudaEventElapsedTime(&ms, e0, e1));
-        cudaEventDestroy(e0);
-        cudaEventDestroy(e1);
-        ctx->syev_ms += ms;
-        ctx->syev_launches++;
-        for (auto& t : ctx->pending_tri) {
-            float tm = 0.f;
-            NRG_CUDA_TRY(cudaEventElapsedTime(&tm, t.a, t.b));
-            cudaEventDestroy(t.a);
-            cudaEventDestroy(t.b);
-            ctx->tri_launches++;
-            ctx->tri_ms += tm;
-            ctx->tri_flops += t.flops;
-            ctx->tri_bytes += t.bytes;
-        }
-        ctx->pending_tri.clear();
         double f = 0.0;
         for (int s = 0; s < nsec; ++s) f += (4.0 / 3.0 + 2.0) * double(S.dim[s]) * S.dim[s] * S.dim[s];
-        ctx->syev_flops += f;
+        ctx->pending_syev.push_back({e0, e1, f, 0.0});
+        if (!early) NRG_TRY(flush_profile_timers(ctx));
     }
-    NRG_TRY(run_eig_finalize(ctx, d_E, S.nb, S.sizeV, d_V, bmin.as<double>()));
+    if (early) {
+        NRG_TRY(run_eig_chop(ctx, S.sizeV, d_V));
+        NRG_CUDA_TRY(cudaEventSynchronize(ctx->ev_evals_host));
+        if (out) {
+            out->groundStateEnergy = hs[1];
+            out->emin = hs[0];
+        }
+        int st = 0;
+        std::memcpy(&st, hs + 2, sizeof(int));
+        if (st != 0) return check_device_status(ctx);   // reports and clears the flags
+        return NRG_OK;
+    }
+    NRG_TRY(run_eig_shift(ctx, d_E, S.nb, bmin.as<double>()));
+    NRG_TRY(run_eig_chop(ctx, S.sizeV, d_V));
     double mg[2];
     NRG_CUDA_TRY(cudaMemcpyAsync(mg, bmin.p, sizeof(double) * 2, cudaMemcpyDeviceToHost, ctx->stream));
     ctx->d2h += sizeof(mg);
@@ -430,6 +447,33 @@ int diag_device(nrg_context* ctx, int iteration, Sectors& S, const double* d_Eol
         out->emin = mg[0];
     }
     return check_device_status(ctx);
+}
+
+int flush_profile_timers(nrg_context* ctx) {
+    for (auto& t : ctx->pending_syev) {
+        float ms = 0.f;
+        NRG_CUDA_TRY(cudaEventSynchronize(t.b));
+        NRG_CUDA_TRY(cudaEventElapsedTime(&ms, t.a, t.b));
+        cudaEventDestroy(t.a);
+        cudaEventDestroy(t.b);
+        ctx->syev_ms += ms;
+        ctx->syev_launches++;
+        ctx->syev_flops += t.flops;
+    }
+    ctx->pending_syev.clear();
+    for (auto& t : ctx->pending_tri) {
+        float tm = 0.f;
+        NRG_CUDA_TRY(cudaEventSynchronize(t.b));
+        NRG_CUDA_TRY(cudaEventElapsedTime(&tm, t.a, t.b));
+        cudaEventDestroy(t.a);
+        cudaEventDestroy(t.b);
+        ctx->tri_launches++;
+        ctx->tri_ms += tm;
+        ctx->tri_flops += t.flops;
+        ctx->tri_bytes += t.bytes;
+    }
+    ctx->pending_tri.clear();
+    return NRG_OK;
 }
 
 std::vector<int> kept_per_sector(const Sectors& S, int nb_kept, const int* bo) {
