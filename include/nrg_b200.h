@@ -277,6 +277,20 @@ typedef struct nrg_run_input {
                                              076402 (2007); rdmTrace then holds, per
                                              shell N, the kept-space trace plus the
                                              weight discarded up to N (1)              */
+    /* restart.dat of the CFS phase (saveRestart / loadRestart, module.F90:1710-1890;
+     * main.F90:165-224), in the reference's byte layout: Fortran stream output of the
+     * restore stock, the full stock, the density matrices and the bins.  Drop-in replay
+     * only (host_drop_in = 1) and with the spectrum on; NRG_ERR_INVALID otherwise, and
+     * for a missing, broken or foreign file. */
+    const char* restart_file;             /* path; NULL or "": "restart.dat"            */
+    int32_t save_restart;                 /* param%saveRestart: rewrite the file before
+                                             every CFS step (after the file's step when
+                                             resuming)                                  */
+    int32_t load_restart;                 /* param%loadRestart: skip the NRG sweep and the
+                                             density matrices and resume the CFS loop at
+                                             the file's iteration; kept and
+                                             numberOfBasisFull come from the file, the
+                                             sweep's other outputs are NaN             */
 } nrg_run_input;
 
 typedef struct nrg_run_output {

@@ -174,6 +174,10 @@ void write_bins(const Model& M, nrg_run_output* out, int nbin, const double* pos
 // ------------------------------------------------------------------------------------
 int run_device(nrg_context* ctx, const nrg_run_input* in, nrg_run_output* out, cudaEvent_t* ev) {
     const Model& M = ctx->model;
+    if (in->save_restart || in->load_restart) {
+        nrg_set_error_message("restart.dat is written and read by the drop-in replay (host_drop_in = 1)");
+        return NRG_ERR_INVALID;
+    }
     const int nVar = M.nVar, rs = nVar + 3, first = M.first, nIter = M.nIter;
     const int nIt = nIter - first + 1;
     const bool spectrum = in->spectrum && M.nMat > 0;
@@ -231,15 +235,25 @@ int run_device(nrg_context* ctx, const nrg_run_input* in, nrg_run_output* out, c
         DevBuf& bE = slotE(idx);
         NRG_TRY(bV.ensure(sizeof(double) * (size_t)S.sizeV));
         NRG_TRY(bE.ensure(sizeof(double) * (size_t)nb));
+        // the call returns with the shifted eigenvalues on the host while the eigenvectors
+        // are still being formed: the truncation and the next iteration's tables are built
+        // meanwhile, and every later launch on the stream is ordered after them
         DiagOut dout;
-        NRG_TRY(diag_device(ctx, it, S, dEold, nb_old, dIMold, bV.as<double>(), bE.as<double>(), &dout));
+        if (ctx->early_evals) {
+            NRG_TRY(ctx->h_evals.ensure(sizeof(double) * (size_t)nb));
+            NRG_TRY(diag_device(ctx, it, S, dEold, nb_old, dIMold, bV.as<double>(), bE.as<double>(), &dout,
+                                ctx->h_evals.as<double>()));
+            R.Esec.assign(ctx->h_evals.as<double>(), ctx->h_evals.as<double>() + nb);
+        } else {
+            NRG_TRY(diag_device(ctx, it, S, dEold, nb_old, dIMold, bV.as<double>(), bE.as<double>(), &dout));
+            R.Esec.resize(nb);
+            NRG_CUDA_TRY(cudaMemcpyAsync(R.Esec.data(), bE.p, sizeof(double) * nb, cudaMemcpyDeviceToHost, st));
+            NRG_CUDA_TRY(cudaStreamSynchronize(st));
+            ctx->d2h += (long long)sizeof(double) * nb;
+        }
         if (out && out->thermo) NRG_TRY(run_thermo(ctx, S, bE.as<double>(), dThermo + 3 * (size_t)idx));
         if (out && out->groundStateEnergy) out->groundStateEnergy[idx] = dout.groundStateEnergy;
         R.emin = dout.emin;
-        R.Esec.resize(nb);
-        NRG_CUDA_TRY(cudaMemcpyAsync(R.Esec.data(), bE.p, sizeof(double) * nb, cudaMemcpyDeviceToHost, st));
-        NRG_CUDA_TRY(cudaStreamSynchronize(st));
-        ctx->d2h += (long long)sizeof(double) * nb;
         std::vector<int> order;
         const int nbk = truncate_host(M, it, R.Esec, &order, &startTrancation, &flag_truncation);
         record_flow(out, idx, R.Esec, order, nbk);
@@ -455,6 +469,7 @@ int run_device(nrg_context* ctx, const nrg_run_input* in, nrg_run_output* out, c
     }
     NRG_CUDA_TRY(cudaEventRecord(ev[3], st));
     NRG_CUDA_TRY(cudaStreamSynchronize(st));
+    NRG_TRY(flush_profile_timers(ctx));
     NRG_TRY(check_device_status(ctx));
     if (dThermo) {
         NRG_CUDA_TRY(cudaMemcpy(out->thermo, dThermo, sizeof(double) * 3 * (size_t)nIt, cudaMemcpyDeviceToHost));
@@ -492,14 +507,110 @@ struct HostRestore {
 // per iteration for the restore stock, the full stock of eigenvectors)
 constexpr size_t kHostIM = 0, kHostFV = 2, kHostV = 16, kHostIMS = 16 + 4096;
 
+// one step of the CFS loop (cfsSpectrumCalculation, module.F90:1683-1706) through the
+// drop-in spike entry points, from the restore stock of iteration N and N-1
+int cfs_step_drop_in(nrg_context* ctx, int N, const std::vector<RestoreView>& its, int nb0, const double* ims0,
+                     const std::vector<int>& fsi, const std::vector<int>& map, const std::vector<double>& rdm,
+                     double* binPos, double* binNeg, double* tot) {
+    const Model& M = ctx->model;
+    const RestoreView& R = its[N - M.first];
+    const bool has_prev = N > M.first;
+    nrg_spike_io sio;
+    std::memset(&sio, 0, sizeof(sio));
+    sio.numberOfSubspace = R.nsub; sio.subspaceInfo = R.si; sio.numberOfBasis = R.nb;
+    sio.numberOfBasisFull = R.nb_full; sio.basis_input = R.bi; sio.basis_output = R.bo;
+    sio.eigenvalue = R.E; sio.eigenvector = R.V; sio.sizeOfEigenvector = (int64_t)R.nV;
+    sio.numberOfBasis_old = has_prev ? its[N - 1 - M.first].nb : nb0;
+    sio.invariant_matrix_spectrum = has_prev ? its[N - 1 - M.first].ims : ims0;
+    sio.fullSubspaceInfo = fsi.data(); sio.mapFullSubspaceInfo = map.data();
+    sio.elementNumFullSubspace = (int32_t)(fsi.size() / (M.nVar + 6)); sio.reducedDensityMatrix = rdm.data();
+    sio.sizeOfReducedDensity = (int64_t)rdm.size(); sio.numberOfBin = M.numberOfBin();
+    sio.binnedSpikePositive = binPos; sio.binnedSpikeNegative = binNeg;
+    sio.total_sum = tot;
+    if (N == M.nIter) return nrg_spike_zero_temperature(ctx, N, &sio);
+    return nrg_spike_cfs(ctx, N, &sio);
+}
+
+// the energy column of the bins (main.F90:142-157); the weights start at zero
+void bin_energies(const Model& M, int nbin, std::vector<double>& pos, std::vector<double>& neg) {
+    const size_t nw = (size_t)nbin * M.nMat;
+    pos.assign(2 * nw, 0.0);
+    neg.assign(2 * nw, 0.0);
+    for (int m = 0; m < M.nMat; ++m)
+        for (int i = 0; i < nbin; ++i) {
+            const double e = std::pow(10.0, -15.0 + double(i) / 1000.0);
+            pos[(size_t)m * nbin + i] = e;
+            neg[(size_t)m * nbin + i] = -e;
+        }
+}
+
+// loadRestart (module.F90:1787-1890) and the CFS loop of main.F90:204-224 from the
+// file's iteration on: the NRG sweep and the density matrices are skipped, the file is
+// rewritten before every later step when save is set
+int resume_drop_in(nrg_context* ctx, nrg_run_output* out, cudaEvent_t* ev, const char* path, bool save) {
+    const Model& M = ctx->model;
+    const int nbin = M.numberOfBin(), first = M.first, nIter = M.nIter, nIt = nIter - first + 1;
+    const size_t nw = (size_t)nbin * M.nMat;
+    RestartData D;
+    NRG_TRY(restart_load(path, M, nbin, &D));
+    NRG_CUDA_TRY(cudaEventRecord(ev[1], ctx->stream));
+    NRG_CUDA_TRY(cudaEventRecord(ev[2], ctx->stream));
+    std::vector<double> tot(4 * M.nMat);
+    const long long nfsi = (long long)(D.fsi.size() / (M.nVar + 6));
+    for (int N = D.iteration; N <= nIter; ++N) {
+        if (save && N > D.iteration) {
+            int32_t hami[20];
+            std::memcpy(hami, D.hami, sizeof(hami));
+            hami[9] = D.its[N - 1 - first].nb;   // hami%numberOfBasis after getRestore(N-1)
+            NRG_TRY(restart_save(path, M, N, hami, D.its, D.nb0, D.ims0.data(), D.rdm.data(), (long long)D.rdm.size(),
+                                 D.fsi.data(), nfsi, D.map.data(), D.binPos.data(), D.binNeg.data(), nbin));
+        }
+        NRG_TRY(cfs_step_drop_in(ctx, N, D.its, D.nb0, D.ims0.data(), D.fsi, D.map, D.rdm, D.binPos.data(),
+                                 D.binNeg.data(), tot.data()));
+    }
+    NRG_CUDA_TRY(cudaEventRecord(ev[3], ctx->stream));
+    NRG_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+    if (out) {
+        out->numberOfBin = nbin;
+        out->startTrancation = D.hami[kHamiStartTrancation];
+        if (out->binnedSpikePositive && out->binnedSpikeNegative && out->binCapacity >= (int64_t)(2 * nw))
+            write_bins(M, out, nbin, D.binPos.data() + nw, D.binNeg.data() + nw, false);
+        for (int x = 0; x < nIt; ++x) {   // what the file keeps of the sweep
+            if (out->kept) out->kept[x] = D.its[x].nb;
+            if (out->numberOfBasisFull) out->numberOfBasisFull[x] = D.its[x].nb_full;
+            if (out->groundStateEnergy) out->groundStateEnergy[x] = std::nan("");
+            if (out->thermo)
+                for (int k = 0; k < 3; ++k) out->thermo[3 * x + k] = std::nan("");
+            if (out->flow && out->flowStride > 0)
+                for (int q = 0; q < out->flowStride; ++q) out->flow[(size_t)x * out->flowStride + q] = std::nan("");
+        }
+        if (out->rdmTrace)
+            for (int N = 0; N <= nIter; ++N) out->rdmTrace[N] = std::nan("");
+        if (out->finalEigenvalue) {
+            const RestoreView& RL = D.its[nIt - 1];
+            for (int i = 0; i < out->finalCapacity && i < RL.nb_full; ++i) out->finalEigenvalue[i] = RL.E[i];
+        }
+    }
+    return NRG_OK;
+}
+
 int run_drop_in(nrg_context* ctx, const nrg_run_input* in, nrg_run_output* out, cudaEvent_t* ev) {
     const Model& M = ctx->model;
+    const bool save = in->save_restart != 0, load = in->load_restart != 0;
+    const char* rpath = (in->restart_file && in->restart_file[0]) ? in->restart_file : "restart.dat";
+    if ((save || load) && !(in->spectrum && M.nMat > 0)) {
+        nrg_set_error_message("restart.dat belongs to the CFS spectrum phase: the run has no spectrum");
+        return NRG_ERR_INVALID;
+    }
+    if (load) return resume_drop_in(ctx, out, ev, rpath, save);
     if (out && out->thermo)   // thermodynamics are the caller's part of postprocess here
         for (int k = 0; k < 3 * (M.nIter - M.first + 1); ++k) out->thermo[k] = std::nan("");
     const int nVar = M.nVar, rs = nVar + 3, rsf = nVar + 6, first = M.first, nIter = M.nIter;
     const int nIt = nIter - first + 1;
     const bool spectrum = in->spectrum && M.nMat > 0;
     int nb_old = in->numberOfBasis;
+    const int nb0 = in->numberOfBasis;
+    const double* ims0 = in->invariant_matrix_spectrum;   // invariant_matrix_spectrum_initial
     if (nIt > (int)(kHostIMS - kHostV)) return NRG_ERR_TOO_LARGE;
     std::vector<int> bo(in->basis_output, in->basis_output + (size_t)nb_old * rs);
     std::vector<double> E(in->eigenvalue, in->eigenvalue + nb_old);
@@ -629,7 +740,8 @@ int run_drop_in(nrg_context* ctx, const nrg_run_input* in, nrg_run_output* out, 
     NRG_CUDA_TRY(cudaEventRecord(ev[1], ctx->stream));
     const int nbin = M.numberOfBin();
     const size_t nw = (size_t)nbin * std::max(M.nMat, 1);
-    std::vector<double> binPos(2 * nw, 0.0), binNeg(2 * nw, 0.0);
+    std::vector<double> binPos, binNeg;
+    bin_energies(M, nbin, binPos, binNeg);
     std::vector<double> rdm;
     const int elementNum = (int)(pointFS - 1);
     if (spectrum && flag_truncation) {
@@ -665,23 +777,25 @@ int run_drop_in(nrg_context* ctx, const nrg_run_input* in, nrg_run_output* out, 
     }
     NRG_CUDA_TRY(cudaEventRecord(ev[2], ctx->stream));
     if (spectrum) {
+        std::vector<RestoreView> views(nIt);
+        for (int x = 0; x < nIt; ++x) {
+            const HostRestore& R = rest[x];
+            RestoreView& v = views[x];
+            v.si = R.si.data(); v.bi = R.bi.data(); v.bo = R.bo.data(); v.E = R.E.data(); v.V = R.V;
+            v.ims = R.ims; v.nV = R.nV; v.nb = R.nb; v.nb_full = R.nb_full; v.nsub = R.nsub;
+        }
         std::vector<double> tot(4 * M.nMat);
         for (int N = startTrancation; N <= nIter; ++N) {
-            const HostRestore& R = rest[N - first];
-            const HostRestore& P = rest[N - 1 - first];
-            nrg_spike_io sio;
-            std::memset(&sio, 0, sizeof(sio));
-            sio.numberOfSubspace = R.nsub; sio.subspaceInfo = R.si.data(); sio.numberOfBasis = R.nb;
-            sio.numberOfBasisFull = R.nb_full; sio.basis_input = R.bi.data(); sio.basis_output = R.bo.data();
-            sio.eigenvalue = R.E.data(); sio.eigenvector = R.V; sio.sizeOfEigenvector = (int64_t)R.nV;
-            sio.numberOfBasis_old = P.nb; sio.invariant_matrix_spectrum = P.ims;
-            sio.fullSubspaceInfo = fsi.data(); sio.mapFullSubspaceInfo = map.data();
-            sio.elementNumFullSubspace = elementNum; sio.reducedDensityMatrix = rdm.data();
-            sio.sizeOfReducedDensity = (int64_t)rdm.size(); sio.numberOfBin = nbin;
-            sio.binnedSpikePositive = binPos.data(); sio.binnedSpikeNegative = binNeg.data();
-            sio.total_sum = tot.data();
-            if (N == nIter) NRG_TRY(nrg_spike_zero_temperature(ctx, N, &sio));
-            else NRG_TRY(nrg_spike_cfs(ctx, N, &sio));
+            if (save) {   // main.F90:216-220: before every step, overwriting the file
+                int32_t hami[20];
+                const int nbh = N == startTrancation ? rest[nIt - 1].nb : rest[N - 1 - first].nb;
+                restart_hami(M, nbh, startTrancation, flag_truncation, hami);
+                NRG_TRY(restart_save(rpath, M, N, hami, views, nb0, ims0, rdm.data(), (long long)rdm.size(),
+                                     fsi.data(), (long long)elementNum, map.data(), binPos.data(), binNeg.data(),
+                                     nbin));
+            }
+            NRG_TRY(cfs_step_drop_in(ctx, N, views, nb0, ims0, fsi, map, rdm, binPos.data(), binNeg.data(),
+                                     tot.data()));
         }
     }
     NRG_CUDA_TRY(cudaEventRecord(ev[3], ctx->stream));
@@ -749,7 +863,12 @@ extern "C" int nrg_run_batch(nrg_context* const* ctxs, const nrg_run_input* in, 
                     c->stream = own;
                 }
             }
-            if (rc == NRG_OK) rc = run_one(c, in + i, out + i);
+            if (rc == NRG_OK) {
+                const bool early = c->early_evals;
+                c->early_evals = early && nthr == 1;
+                rc = run_one(c, in + i, out + i);
+                c->early_evals = early;
+            }
             if (c && (flags & NRG_BATCH_RELEASE)) {
                 const int rr = nrg_context_release_storage(c);
                 if (rc == NRG_OK) rc = rr;

@@ -138,6 +138,10 @@ struct nrg_context {
     // for the back-transformations, so the host bookkeeping of the next iteration runs
     // while they finish
     cudaEvent_t ev_evals_hi = nullptr, ev_evals2 = nullptr, ev_evals_host = nullptr;
+    // measured policy: the early path gains ~6 % for an instance that has the device to
+    // itself and loses ~10 % with eight instances in flight (their work already fills
+    // the host gap), so nrg_run_batch turns it off when it runs instances side by side
+    bool early_evals = true;
     nrg::HostBuf h_small;   // pinned: the shift's minimum and E(1), the status word
     nrg::HostBuf h_evals;   // pinned: the shifted eigenvalues of the current iteration
     nrg::DevBuf& slot(size_t i) {

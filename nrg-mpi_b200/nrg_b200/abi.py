@@ -126,6 +126,7 @@ class RunInput(ctypes.Structure):
         ("numberOfBasis", c_int32), ("basis_output", _pi32), ("eigenvalue", _pf64),
         ("invariant_matrix", _pf64), ("invariant_matrix_spectrum", _pf64),
         ("spectrum", c_int32), ("host_drop_in", c_int32), ("temperature", c_double),
+        ("restart_file", ctypes.c_char_p), ("save_restart", c_int32), ("load_restart", c_int32),
     ]
 
 
@@ -456,28 +457,36 @@ class Context:
 
     # ------------------------------------------------------------------
     def run(self, spectrum: bool = True, flow_stride: int = 8, final_capacity: int = 0,
-            host_drop_in: bool = False, temperature: float = 0.0):
+            host_drop_in: bool = False, temperature: float = 0.0, restart_file: Optional[str] = None,
+            save_restart: bool = False, load_restart: bool = False):
         """main.F90:142-252; returns bins and per-iteration statistics.
 
         ``host_drop_in=True`` drives every routine through its drop-in entry point with
         host arrays (the Fortran caller's data flow) instead of keeping state on the device.
         ``temperature > 0`` (device-resident run) gives the full-density-matrix spectrum
         at that temperature instead of the reference's T = 0 CFS spectrum.
+        ``save_restart`` / ``load_restart`` (drop-in replay with the spectrum on) are the
+        reference's param%saveRestart / param%loadRestart: the file (``restart_file``,
+        default "restart.dat") is rewritten before every CFS step, or the run resumes the
+        CFS loop from it (module.F90:1710-1890, main.F90:165-224).
         """
-        args = self._run_args(spectrum, flow_stride, final_capacity, host_drop_in, temperature)
+        args = self._run_args(spectrum, flow_stride, final_capacity, host_drop_in, temperature,
+                              restart_file, save_restart, load_restart)
         self._check(self.lib.nrg_run(self._h, ctypes.byref(args["ri"]), ctypes.byref(args["ro"])), "nrg_run")
         return self._run_result(args)
 
-    def _run_args(self, spectrum, flow_stride, final_capacity, host_drop_in, temperature=0.0):
+    def _run_args(self, spectrum, flow_stride, final_capacity, host_drop_in, temperature=0.0,
+                  restart_file=None, save_restart=False, load_restart=False):
         """Input and output records of nrg_run for this context (arrays kept alive here)."""
         inp = self.inp
         nb = inp.numberOfBasis
         a = dict(bo=_i32(inp.basis_output), E=np.ascontiguousarray(inp.eigenvalue, dtype=np.float64),
                  im=_f64f(inp.invariant_matrix),
-                 ims=_f64f(inp.invariant_matrix_spectrum) if inp.flag_spectrum else None)
+                 ims=_f64f(inp.invariant_matrix_spectrum) if inp.flag_spectrum else None,
+                 path=os.fsencode(restart_file) if restart_file else None)
         a["ri"] = RunInput(nb, _p(a["bo"], c_int32), _p(a["E"], c_double), _p(a["im"], c_double),
                            _p(a["ims"], c_double), int(bool(spectrum)), int(bool(host_drop_in)),
-                           float(temperature))
+                           float(temperature), a["path"], int(bool(save_restart)), int(bool(load_restart)))
         nit = inp.numberOfIteration - inp.indexOfFirstIteration + 1
         nmat = max(inp.numberOfMatrix, 1)
         nbin_cap = 20001

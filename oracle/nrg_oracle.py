@@ -1078,6 +1078,162 @@ def run(directory: str, spectrum: bool = True, literal: bool = False,
 
 
 # ------------------------------------------------------------------------------------
+# restart.dat of the CFS phase (module.F90:1710-1890; main.F90:165-224)
+# ------------------------------------------------------------------------------------
+MODE_RESTART_NON = 1000            # module.F90:1718
+MODE_RESTART_CFS = 1002            # module.F90:1720
+_RESTORE_FIELDS = 10               # type restore, module.F90:983-994
+
+
+def _hami_words(st: State, numberOfBasis: int) -> np.ndarray:
+    """HamiltonianInfo_type (module.F90:722-760) as written by ``write(fd) hami``: its
+    components in order, 4-byte integers and logicals (.true. = 1)."""
+    cb = st.cb.ravel(order="F")
+    return np.array([st.nIter, st.nChain, st.nVar, cb[0], cb[1], cb[2], cb[3], st.nMat, st.nCM,
+                     numberOfBasis, st.nCoef, 0, st.nOps, st.nBCS, st.first, int(st.flag_spectrum), 0,
+                     st.startTrancation, int(st.flag_truncation), int(st.flag_BCS)], dtype="<i4")
+
+
+def save_restart(st: State, iteration: int, path: str, numberOfBasis: int) -> None:
+    """saveRestart (module.F90:1723-1785): Fortran stream output (no record markers).
+    ``numberOfBasis`` is hami%numberOfBasis at the call (the kept count of the last
+    iteration before the first CFS step, that of iteration-1 after getRestore)."""
+    its = range(st.first, st.nIter + 1)
+    ri = np.zeros((st.nIter + 2 - st.first, _RESTORE_FIELDS), dtype=np.int64)
+    e0 = v0 = s0 = m0 = 1
+    for x, it in enumerate(its):                      # initRestore/appendRestore :1388-1567
+        r = st.restore[it]
+        nf, nv, ns, nb = r["numberOfBasis_full"], r["eigenvector"].size, len(r["subspaceInfo"]), r["numberOfBasis"]
+        nm = nb * nb * st.nMat if it < st.nIter else 0
+        ri[x] = [e0, nf, v0, nv, s0, ns, e0, m0 if nm else 0, nm, nb]
+        e0, v0, s0, m0 = e0 + nf, v0 + nv, s0 + ns, m0 + nm
+
+    def i4(a):
+        return np.ascontiguousarray(a, dtype="<i4").tobytes()
+
+    def f8(a):
+        return np.ascontiguousarray(a, dtype="<f8").tobytes()
+
+    R = [st.restore[it] for it in its]
+    with open(path, "wb") as f:
+        f.write(i4([MODE_RESTART_CFS, iteration]))
+        f.write(_hami_words(st, numberOfBasis).tobytes())
+        f.write(i4([st.first, st.nIter + 1]) + i4(ri.ravel()))
+        for key in ("subspaceInfo", "basis_input", "basis_output"):
+            recs = [r[key][:r["numberOfBasis_full"]] if key != "subspaceInfo" else r[key] for r in R]
+            f.write(i4([sum(len(a) for a in recs)]))
+            for a in recs:
+                f.write(i4(a))
+        ims = [r["ims"].ravel(order="F") for it, r in zip(its, R) if it < st.nIter]
+        f.write(i4([sum(a.size for a in ims)]))
+        for a in ims:
+            f.write(f8(a))
+        f.write(i4(list(st.ims_initial.shape)) + f8(st.ims_initial.ravel(order="F")))
+        f.write(i4([sum(r["numberOfBasis_full"] for r in R)]))
+        for r in R:
+            f.write(f8(r["eigenvalue"][:r["numberOfBasis_full"]]))
+        f.write(i4([sum(r["eigenvector"].size for r in R)]))
+        for r in R:
+            f.write(f8(r["eigenvector"]))
+        f.write(i4([st.rdm.size]) + f8(st.rdm))
+        f.write(i4([len(st.FSI)]) + i4(st.FSI))
+        mp = np.zeros(st.nIter + 2, dtype=np.int64)
+        for it, v in st.mapFull.items():
+            mp[it + 1] = v
+        f.write(i4([-1, st.nIter]) + i4(mp))
+        for b in (st.binPos, st.binNeg):
+            f.write(i4([b.size]) + f8(b.ravel(order="F")))
+
+
+def load_restart(st: State, path: str) -> int:
+    """loadRestart (module.F90:1787-1890): the restore and full stocks, the density
+    matrices and the bins; returns iteration_restart."""
+    buf = open(path, "rb").read()
+    pos = 0
+
+    def take(n, dt):
+        nonlocal pos
+        a = np.frombuffer(buf, dtype=dt, count=n, offset=pos)
+        pos += a.nbytes
+        return a
+
+    def i4(n=1):
+        return take(n, "<i4").astype(np.int64)
+
+    mode, iteration = (int(x) for x in i4(2))
+    if mode != MODE_RESTART_CFS:
+        raise ValueError("broken restart file")
+    h = i4(20)
+    st.startTrancation, st.flag_truncation = int(h[17]), bool(h[18])
+    lo, hi = (int(x) for x in i4(2))
+    ri = i4((hi - lo + 1) * _RESTORE_FIELDS).reshape(-1, _RESTORE_FIELDS)
+    rs, rsf = st.nVar + 3, st.nVar + 6
+    arrays = {}
+    for key in ("subspaceInfo", "basis_input", "basis_output"):
+        n = int(i4()[0])
+        arrays[key] = i4(n * rs).reshape(n, rs)
+    ims = take(int(i4()[0]), "<f8")
+    d = [int(x) for x in i4(3)]
+    st.ims_initial = take(d[0] * d[1] * d[2], "<f8").reshape(d, order="F").copy()
+    E = take(int(i4()[0]), "<f8")
+    V = take(int(i4()[0]), "<f8")
+    st.rdm = take(int(i4()[0]), "<f8").copy()
+    n = int(i4()[0])
+    st.FSI = i4(n * rsf).reshape(n, rsf)
+    st.elementNumFullSubspace = n
+    lo, hi = (int(x) for x in i4(2))
+    mp = i4(hi - lo + 1)
+    st.mapFull = {it: int(mp[it - lo]) for it in range(lo, hi + 1) if mp[it - lo] != 0}
+    for name in ("binPos", "binNeg"):
+        n = int(i4()[0])
+        setattr(st, name, take(n, "<f8").reshape((n // 2, 2), order="F").copy())
+    assert pos == len(buf), "trailing bytes in the restart file"
+    st.restore = {}
+    for x, it in enumerate(range(st.first, st.nIter + 1)):     # getRestore :1596-1660
+        e, nf, v, nv, s, ns, b, m, nm, nb = (int(q) for q in ri[x])
+        st.restore[it] = dict(
+            eigenvalue=E[e - 1:e - 1 + nf].copy(), eigenvector=V[v - 1:v - 1 + nv].copy(),
+            basis_output=arrays["basis_output"][b - 1:b - 1 + nf].copy(),
+            basis_input=arrays["basis_input"][b - 1:b - 1 + nf].copy(),
+            subspaceInfo=arrays["subspaceInfo"][s - 1:s - 1 + ns].copy(), numberOfBasis=nb,
+            numberOfBasis_full=nf,
+            ims=(ims[m - 1:m - 1 + nm].reshape((nb, nb, st.nMat), order="F").copy() if nm else None))
+    return iteration
+
+
+def run_with_restart(directory: str, save_path: Optional[str] = None, load_path: Optional[str] = None,
+                     stop_before: Optional[int] = None) -> State:
+    """main.F90:160-224 with param%saveRestart (``save_path``) and param%loadRestart
+    (``load_path``).  ``stop_before`` ends the run right after the file was written for
+    that CFS step, as an interrupted job would leave it."""
+    st = State(directory)
+    mode = MODE_RESTART_NON
+    it_r = None
+    if load_path:
+        it_r = load_restart(st, load_path)
+        mode = MODE_RESTART_CFS
+    if mode != MODE_RESTART_CFS:
+        for it in range(st.first, st.nIter + 1):
+            nrg_iteration(st, it)
+        if st.flag_truncation:
+            initialize_reduced_density(st)
+            reduced_density_matrix_calculation(st)
+    first_step = True
+    for it in range(st.startTrancation, st.nIter + 1):
+        if mode == MODE_RESTART_CFS and it < it_r:
+            continue
+        if save_path and (mode != MODE_RESTART_CFS or it > it_r):
+            nb = st.restore[st.nIter]["numberOfBasis"] if (first_step and mode != MODE_RESTART_CFS) \
+                else st.restore[it - 1]["numberOfBasis"]
+            save_restart(st, it, save_path, nb)
+        first_step = False
+        if stop_before is not None and it == stop_before:
+            return st
+        cfs_spectrum_calculation(st, it)
+    return st
+
+
+# ------------------------------------------------------------------------------------
 # full-density-matrix (FDM) spectrum at temperature T.  The reference has none (its
 # spectrum is the T = 0 CFS one); restated from the published method: Weichselbaum and
 # von Delft, PRL 99, 076402 (2007), with the complete basis of Anders and Schiller, PRL
