@@ -219,6 +219,14 @@ int run_device(nrg_context* ctx, const nrg_run_input* in, nrg_run_output* out, c
         dThermo = bT.as<double>();
     }
 
+    // the pinned eigenvalue buffer of the early path, sized once for the run: no iteration
+    // keeps more than max(nOps * nb0, 1.2 N_keep) states (postprocess.F90:79-126), so no
+    // iteration has more than nOps times that
+    if (ctx->early_evals) {
+        const long long keep = std::max<long long>((long long)M.nOps * in->numberOfBasis,
+                                                   (long long)(M.truncation * 1.2) + 1);
+        NRG_TRY(ctx->h_evals.ensure(sizeof(double) * (size_t)(keep * M.nOps)));
+    }
     // ---- forward sweep ----
     for (int it = first; it <= nIter; ++it) {
         const int idx = it - first;
