@@ -127,6 +127,22 @@ NRG_API const char* nrg_last_error(void);
 NRG_API const char* nrg_status_string(int status);
 NRG_API int nrg_version(void);
 
+/* ---- prepareBasis(iteration)  (prepareBasis.F90:1-119) --------------------------------
+ * The product basis of the kept states of the last iteration with the states the new
+ * site adds: basis(i*nOps + j) = (basis_output(i)%basis - operation(j, 1:nVar), reference
+ * i, variation of i, operation j) (:42-57), sorted by sortBasisArray (module.F90:531-602:
+ * by quantum numbers, then reference, with that exchange sort's order among equal keys),
+ * then the sector table subspaceInfo = (basis, dimension, count_eigenvector, start_input)
+ * (:63-114).  Integer bookkeeping on the host, as in the reference; it needs no context
+ * and no device (the device-resident sweep calls the same code).  operation is the
+ * Fortran (nOps, nVar+nChain) table; basis_input receives nb_old*nOps records;
+ * numberOfSubspace receives the sector count, also when subspaceCapacity is too small
+ * (NRG_ERR_INVALID). */
+NRG_API int nrg_prepare_basis(int32_t numberOfVariation, int32_t numberOfOperation, int32_t numberOfChain,
+                              const int32_t* operation, int32_t numberOfBasis_old, const int32_t* basis_output,
+                              int32_t* basis_input, int32_t* subspaceInfo, int32_t subspaceCapacity,
+                              int32_t* numberOfSubspace);
+
 /* ---- diagonalization(iteration, ismysubspace)  (diagonalization.F90:1-529) ----------
  * Replaces the routine called from nrgIteration.F90:23.  Per symmetry sector: assemble
  * the block Hamiltonian (diagonalization.F90:272-381), diagonalise it (dsyev 'V','U',

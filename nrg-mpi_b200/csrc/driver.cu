@@ -825,6 +825,39 @@ int run_one(nrg_context* ctx, const nrg_run_input* in, nrg_run_output* out);
 
 }  // namespace
 
+extern "C" int nrg_prepare_basis(int32_t numberOfVariation, int32_t numberOfOperation, int32_t numberOfChain,
+                                 const int32_t* operation, int32_t numberOfBasis_old, const int32_t* basis_output,
+                                 int32_t* basis_input, int32_t* subspaceInfo, int32_t subspaceCapacity,
+                                 int32_t* numberOfSubspace) {
+    const int nVar = numberOfVariation, nOps = numberOfOperation, rs = nVar + 3;
+    if (nVar < 1 || nOps < 1 || numberOfChain < 0 || numberOfBasis_old < 0 || subspaceCapacity < 0 || !operation ||
+        !numberOfSubspace || (numberOfBasis_old > 0 && (!basis_output || !basis_input || !subspaceInfo))) {
+        nrg_set_error_message("nrg_prepare_basis: inconsistent sizes or NULL arrays");
+        return NRG_ERR_INVALID;
+    }
+    if ((long long)numberOfBasis_old * nOps > 0x7fffffffLL) {
+        nrg_set_error_message("nrg_prepare_basis: %d x %d states exceed the 32-bit basis index", numberOfBasis_old,
+                              nOps);
+        return NRG_ERR_TOO_LARGE;
+    }
+    Model M;
+    M.nVar = nVar;
+    M.nOps = nOps;
+    M.nChain = numberOfChain;
+    M.operation.assign(operation, operation + (size_t)nOps * (nVar + numberOfChain));
+    std::vector<int> bo(basis_output, basis_output + (size_t)numberOfBasis_old * rs), rec, si;
+    prepare_basis_host(M, bo, numberOfBasis_old, &rec, &si);
+    const int nsub = (int)(si.size() / rs);
+    *numberOfSubspace = nsub;
+    if (nsub > subspaceCapacity) {
+        nrg_set_error_message("nrg_prepare_basis: %d sectors, subspaceInfo holds %d", nsub, subspaceCapacity);
+        return NRG_ERR_INVALID;
+    }
+    std::memcpy(basis_input, rec.data(), sizeof(int) * rec.size());
+    std::memcpy(subspaceInfo, si.data(), sizeof(int) * si.size());
+    return NRG_OK;
+}
+
 extern "C" int nrg_run(nrg_context* ctx, const nrg_run_input* in, nrg_run_output* out) {
     return run_one(ctx, in, out);
 }

@@ -45,7 +45,7 @@ EXPORTS = [
     "nrg_spike_zero_temperature", "nrg_spike_cfs", "nrg_run", "nrg_context_get_stats",
     "nrg_context_reset_stats", "nrg_context_set_profiling", "nrg_block_eigh_noalloc",
     "nrg_host_alloc", "nrg_host_free", "nrg_run_batch", "nrg_context_release_storage",
-    "nrg_broaden_log_gaussian",
+    "nrg_broaden_log_gaussian", "nrg_prepare_basis",
 ]
 
 
@@ -179,6 +179,8 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
     lib.nrg_context_release_storage.argtypes = [c_void_p]
     lib.nrg_broaden_log_gaussian.argtypes = [c_void_p, POINTER(c_double), c_int32, c_int32, c_double,
                                              POINTER(c_double), c_int32, POINTER(c_double)]
+    lib.nrg_prepare_basis.argtypes = [c_int32, c_int32, c_int32, POINTER(c_int32), c_int32, POINTER(c_int32),
+                                      POINTER(c_int32), POINTER(c_int32), c_int32, POINTER(c_int32)]
     lib.nrg_context_get_stats.argtypes = [c_void_p, POINTER(Stats)]
     lib.nrg_context_reset_stats.argtypes = [c_void_p]
     lib.nrg_context_set_profiling.argtypes = [c_void_p, ctypes.c_int]
@@ -201,6 +203,29 @@ def _f64f(a) -> np.ndarray:
 
 def _p(a, t):
     return None if a is None else a.ctypes.data_as(POINTER(t))
+
+
+def prepare_basis(operation, nVar: int, basis_output):
+    """nrg_prepare_basis (prepareBasis.F90:1-119): the product basis of the kept records
+    ``basis_output`` (nb_old, nVar+3) with the new site's ``operation`` table (nOps,
+    nVar+nChain); returns (basis_input (nb_old*nOps, nVar+3), subspaceInfo (nsub, nVar+3)),
+    1-based values as in the reference.  Host integer work: no context, no device."""
+    lib = load_library()
+    op = np.asarray(operation, dtype=np.int32)
+    nOps, ncol = op.shape
+    rs = nVar + 3
+    bo = np.ascontiguousarray(np.asarray(basis_output, dtype=np.int32).reshape(-1, rs))
+    nb = bo.shape[0] * nOps
+    bi = np.zeros((nb, rs), dtype=np.int32)
+    cap = max(nb, 1)
+    si = np.zeros((cap, rs), dtype=np.int32)
+    opf = _i32f(op)
+    nsub = c_int32(0)
+    rc = lib.nrg_prepare_basis(nVar, nOps, ncol - nVar, _p(opf, c_int32), bo.shape[0], _p(bo, c_int32),
+                               _p(bi, c_int32), _p(si, c_int32), cap, ctypes.byref(nsub))
+    if rc != 0:
+        raise NrgError(rc, "nrg_prepare_basis", lib.nrg_last_error().decode(errors="replace"))
+    return bi, si[:nsub.value].copy()
 
 
 class Context:
