@@ -27,8 +27,8 @@ using namespace nrg;
 namespace {
 
 // sortBasisArray (module.F90:531-602): exchange sort of whole records.  When no two
-// records share (basis, reference) any correct sort gives its result; ties are resolved
-// by replaying the exchange sequence.
+// records share (basis, reference) any correct sort gives its result; otherwise the
+// order among equal keys is the exchange sequence's, which is replayed.
 void sort_basis(std::vector<int>& rec, int n, int nVar) {
     const int rs = nVar + 3;
     auto greater = [&](const int* a, const int* b) {
@@ -55,17 +55,49 @@ void sort_basis(std::vector<int>& rec, int n, int nVar) {
         rec.swap(out);
         return;
     }
-    std::vector<int> tmp(rs);
-    for (int i = 0; i < n; ++i)
-        for (int j = i + 1; j < n; ++j) {
-            int* a = &rec[(size_t)i * rs];
-            int* b = &rec[(size_t)j * rs];
-            if (greater(a, b)) {
-                std::memcpy(tmp.data(), a, sizeof(int) * rs);
-                std::memcpy(a, b, sizeof(int) * rs);
-                std::memcpy(b, tmp.data(), sizeof(int) * rs);
+    // The exchange sequence on integer ranks of the keys (equal keys, equal ranks) with
+    // the records' ids carried along.  Pass i carries the smallest key seen so far and
+    // swaps it with every strictly smaller key after it; it ends once the carried key is
+    // the i-th smallest of all (known from the stable sort above), since no key after it
+    // can then be smaller: the same swaps as the full scan, without the tail.
+    std::vector<int> rk(n), id(n), target(n);
+    for (int k = 0, r = -1; k < n; ++k) {
+        if (k == 0 || greater(&rec[(size_t)idx[k] * rs], &rec[(size_t)idx[k - 1] * rs])) ++r;
+        rk[idx[k]] = r;
+        target[k] = r;
+    }
+    std::iota(id.begin(), id.end(), 0);
+    int* R = rk.data();
+    int* I = id.data();
+    for (int i = 0; i < n; ++i) {
+        int c = R[i], ci = I[i];
+        const int t = target[i];
+        int j = i + 1;
+        while (c > t && j < n) {
+            // skip keys not smaller than the carried one, eight at a time
+            while (j + 8 <= n) {
+                int m = 0;
+                for (int u = 0; u < 8; ++u) m |= R[j + u] < c;
+                if (m) break;
+                j += 8;
+            }
+            for (const int end = std::min(n, j + 8); c > t && j < end; ++j) {
+                const int x = R[j];
+                if (x < c) {
+                    R[j] = c;
+                    c = x;
+                    const int xi = I[j];
+                    I[j] = ci;
+                    ci = xi;
+                }
             }
         }
+        R[i] = c;
+        I[i] = ci;
+    }
+    std::vector<int> out((size_t)n * rs);
+    for (int i = 0; i < n; ++i) std::memcpy(&out[(size_t)i * rs], &rec[(size_t)I[i] * rs], sizeof(int) * rs);
+    rec.swap(out);
 }
 
 // prepareBasis (prepareBasis.F90:31-114): product basis, sort, sector table
