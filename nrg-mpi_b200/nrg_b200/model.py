@@ -34,7 +34,7 @@ from __future__ import annotations
 import dataclasses
 import math
 import os
-from typing import Dict, List, Optional
+from typing import Callable, Dict, List, Optional, Tuple
 
 import numpy as np
 
@@ -226,14 +226,16 @@ def _local_site_tables(n_chain: int):
 # --------------------------------------------------------------------------------------
 def _build(imp_modes: int, h_imp: np.ndarray, n_chain: int, Lambda: float, D: float,
            hyb: List[float], n_iter: int, n_keep: int, description: str,
-           with_spectrum: bool = True, a_lambda: bool = True) -> NrgInput:
+           with_spectrum: bool = True, a_lambda: bool = True,
+           chain: Optional[Tuple[np.ndarray, np.ndarray]] = None) -> NrgInput:
     """Assemble an :class:`NrgInput` for an impurity with ``imp_modes`` fermion modes.
 
     ``h_imp`` is the impurity Hamiltonian in the Fock basis of ``imp_modes`` modes (bit
     masks, dense).  Impurity mode ``2c+s`` hybridises with Wilson chain ``c`` spin ``s``
     with strength ``hyb[c]`` (already the physical V).  The impurity block is
     diagonalised per (Q, 2Sz) sector; its eigenstates become the initial
-    ``basis_output``.
+    ``basis_output``.  ``chain = (eps, t)`` (physical units, at least numberOfIteration+2
+    on-site energies and hoppings) replaces the flat band's Wilson chain in every chain.
     """
     scalingType, z = 1, 1.0
     first = -1
@@ -319,10 +321,14 @@ def _build(imp_modes: int, h_imp: np.ndarray, n_chain: int, Lambda: float, D: fl
 
     # ---- Wilson chain (physical units, as in initial.dat; rescaled by the reader)
     n_pts = n_iter + 2
-    t_n = wilson_flat_band_hoppings(Lambda, D, n_pts)
+    t_n = wilson_flat_band_hoppings(Lambda, D, n_pts) if chain is None else np.asarray(chain[1][:n_pts])
+    e_n = np.zeros(n_pts) if chain is None else np.asarray(chain[0][:n_pts])
+    if len(t_n) != n_pts or len(e_n) != n_pts:
+        raise ValueError(f"the chain needs {n_pts} on-site energies and hoppings")
     chain_diag = np.zeros((n_pts, n_chain))
     chain_nond = np.zeros((n_pts - first, n_chain))
     for c in range(n_chain):
+        chain_diag[:, c] = e_n           # site n's energy, added at iteration n-1
         chain_nond[1:, c] = t_n          # indices 0..n_iter+1
         chain_nond[0, c] = hyb[c] / scale(first)   # index -1: used as written
 
@@ -375,6 +381,28 @@ def siam(U: float, Gamma: float, eps_d: Optional[float] = None, Lambda: float = 
             f"iterations={n_iterations}")
     return _build(2, h, 1, Lambda, D, [V], n_iterations - 2, n_keep, desc,
                   a_lambda=a_lambda)
+
+
+def siam_bath(U: float, eps_d: float, hybridization: Callable[[float], float], Lambda: float = 2.0,
+              n_keep: int = 512, n_iterations: int = 40, D: float = 1.0, scheme: str = "campo",
+              name: str = "") -> NrgInput:
+    """Single-impurity Anderson model with an arbitrary bath: ``hybridization(eps)`` is
+    Gamma(eps) = pi sum_k |V_k|^2 delta(eps - eps_k) on [-D, D] (energies in the units of
+    D).  The Wilson chain (on-site energies and hoppings) comes from its logarithmic
+    discretisation with the ``scheme``'s representative energies ("campo": Campo and
+    Oliveira, no A_Lambda correction; "wilson": interval means, as for siam() without
+    a_lambda), z = 1; see nrg_b200.chain."""
+    from . import chain as _chain
+    n_pts = n_iterations                      # numberOfIteration + 2 chain sites used
+    V, e, t = _chain.log_discretized_chain(hybridization, D, Lambda, n_pts + 1, 1.0, scheme)
+    h = np.zeros((4, 4))
+    for st in range(4):
+        n_up, n_dn = st & 1, (st >> 1) & 1
+        h[st, st] = eps_d * (n_up + n_dn) + U * n_up * n_dn
+    desc = (f"SIAM bath {name or 'custom'} ({scheme}) U={U} eps_d={eps_d} Lambda={Lambda} "
+            f"N_keep={n_keep} iterations={n_iterations}")
+    return _build(2, h, 1, Lambda, D, [V], n_iterations - 2, n_keep, desc, a_lambda=False,
+                  chain=(e, t))
 
 
 def two_orbital_hund(U: float = 0.2, J: float = 0.02, Gamma: float = 0.015,
