@@ -26,6 +26,62 @@ using namespace nrg;
 
 namespace {
 
+// The stable order of the records by (quantum numbers, reference) without comparisons:
+// records come in generation order (old state i, operation j), so within one set of
+// quantum numbers the references never decrease, and a stable counting sort over the
+// distinct quantum numbers (a few hundred) gives the stable sort's order.  Returns false
+// (the caller sorts by comparison) when the references do decrease somewhere.
+bool bucket_order(const std::vector<int>& rec, int n, int nVar, std::vector<int>* idx) {
+    const int rs = nVar + 3;
+    std::vector<int> bucket(n);
+    std::vector<int> keys;            // distinct quantum numbers, nVar per bucket
+    std::vector<int> last_ref;        // reference of the bucket's last record
+    std::vector<int> table(64, -1);   // open addressing: bucket per hash slot
+    size_t mask = table.size() - 1;
+    auto slot_of = [&](const int* q) {
+        size_t h = 1469598103934665603ULL;
+        for (int v = 0; v < nVar; ++v) h = (h ^ (size_t)(uint32_t)q[v]) * 1099511628211ULL;
+        return h;
+    };
+    for (int r = 0; r < n; ++r) {
+        const int* q = &rec[(size_t)r * rs];
+        if (2 * keys.size() / nVar >= table.size() / 2) {   // grow and rehash
+            table.assign(table.size() * 4, -1);
+            mask = table.size() - 1;
+            for (int b = 0; b < (int)(keys.size() / nVar); ++b)
+                for (size_t x = slot_of(&keys[(size_t)b * nVar]) & mask;; x = (x + 1) & mask)
+                    if (table[x] < 0) { table[x] = b; break; }
+        }
+        int b = -1;
+        for (size_t x = slot_of(q) & mask;; x = (x + 1) & mask) {
+            if (table[x] < 0) {
+                b = (int)(keys.size() / nVar);
+                table[x] = b;
+                keys.insert(keys.end(), q, q + nVar);
+                last_ref.push_back(q[nVar]);
+                break;
+            }
+            if (std::equal(q, q + nVar, &keys[(size_t)table[x] * nVar])) { b = table[x]; break; }
+        }
+        if (q[nVar] < last_ref[b]) return false;
+        last_ref[b] = q[nVar];
+        bucket[r] = b;
+    }
+    const int nb = (int)(keys.size() / nVar);
+    std::vector<int> order(nb);
+    std::iota(order.begin(), order.end(), 0);
+    std::sort(order.begin(), order.end(), [&](int a, int b) {
+        return std::lexicographical_compare(&keys[(size_t)a * nVar], &keys[(size_t)a * nVar] + nVar,
+                                            &keys[(size_t)b * nVar], &keys[(size_t)b * nVar] + nVar);
+    });
+    std::vector<int> start(nb + 1, 0), rank(nb);
+    for (int k = 0; k < nb; ++k) rank[order[k]] = k;
+    for (int r = 0; r < n; ++r) start[rank[bucket[r]] + 1]++;
+    for (int k = 0; k < nb; ++k) start[k + 1] += start[k];
+    for (int r = 0; r < n; ++r) (*idx)[start[rank[bucket[r]]]++] = r;
+    return true;
+}
+
 // sortBasisArray (module.F90:531-602): exchange sort of whole records.  When no two
 // records share (basis, reference) any correct sort gives its result; otherwise the
 // order among equal keys is the exchange sequence's, which is replayed.
@@ -39,10 +95,12 @@ void sort_basis(std::vector<int>& rec, int n, int nVar) {
         return a[nVar] > b[nVar];
     };
     std::vector<int> idx(n);
-    std::iota(idx.begin(), idx.end(), 0);
-    std::stable_sort(idx.begin(), idx.end(), [&](int x, int y) {
-        return greater(&rec[(size_t)y * rs], &rec[(size_t)x * rs]);
-    });
+    if (!bucket_order(rec, n, nVar, &idx)) {
+        std::iota(idx.begin(), idx.end(), 0);
+        std::stable_sort(idx.begin(), idx.end(), [&](int x, int y) {
+            return greater(&rec[(size_t)y * rs], &rec[(size_t)x * rs]);
+        });
+    }
     bool ties = false;
     for (int i = 1; i < n && !ties; ++i) {
         const int* a = &rec[(size_t)idx[i - 1] * rs];
