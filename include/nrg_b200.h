@@ -143,6 +143,20 @@ NRG_API int nrg_prepare_basis(int32_t numberOfVariation, int32_t numberOfOperati
                               int32_t* basis_input, int32_t* subspaceInfo, int32_t subspaceCapacity,
                               int32_t* numberOfSubspace);
 
+/* ---- truncation and reorder of postprocess(iteration)  (postprocess.F90:69-168) --------
+ * eigenvalue (sector order, as diagonalization leaves it) is sorted stably
+ * (sortWithIndex, :75); unless iteration is the first or the last or nb <= truncation,
+ * the kept count is N_keep extended over energies within 1e-6 of E(N_keep) and then cut
+ * back by 0.001 steps until it is at most 1.2 N_keep (:79-126); the kept states are put
+ * back in index order (sortByIndex, :140) and followed by the discarded ones in energy
+ * order, and eigenvalue and basis_output (may be NULL) are permuted in place (:143-160).
+ * startTrancation and flag_truncation are hami's fields, updated at the first truncated
+ * iteration (:83-86).  Host work: no context, no device. */
+NRG_API int nrg_truncate(int32_t iteration, int32_t indexOfFirstIteration, int32_t numberOfIteration,
+                         int32_t truncation, int32_t numberOfVariation, int32_t numberOfBasis, double* eigenvalue,
+                         int32_t* basis_output, int32_t* numberOfBasis_kept, int32_t* startTrancation,
+                         int32_t* flag_truncation);
+
 /* ---- diagonalization(iteration, ismysubspace)  (diagonalization.F90:1-529) ----------
  * Replaces the routine called from nrgIteration.F90:23.  Per symmetry sector: assemble
  * the block Hamiltonian (diagonalization.F90:272-381), diagonalise it (dsyev 'V','U',

@@ -948,6 +948,38 @@ extern "C" int nrg_prepare_basis(int32_t numberOfVariation, int32_t numberOfOper
     return NRG_OK;
 }
 
+extern "C" int nrg_truncate(int32_t iteration, int32_t indexOfFirstIteration, int32_t numberOfIteration,
+                            int32_t truncation, int32_t numberOfVariation, int32_t numberOfBasis, double* eigenvalue,
+                            int32_t* basis_output, int32_t* numberOfBasis_kept, int32_t* startTrancation,
+                            int32_t* flag_truncation) {
+    if (numberOfBasis < 0 || truncation < 1 || numberOfVariation < 1 || !numberOfBasis_kept || !startTrancation ||
+        !flag_truncation || (numberOfBasis > 0 && !eigenvalue)) {
+        nrg_set_error_message("nrg_truncate: inconsistent sizes or NULL arrays");
+        return NRG_ERR_INVALID;
+    }
+    Model M;
+    M.first = indexOfFirstIteration;
+    M.nIter = numberOfIteration;
+    M.truncation = truncation;
+    M.nVar = numberOfVariation;
+    const int nb = numberOfBasis, rs = numberOfVariation + 3;
+    std::vector<double> E(eigenvalue, eigenvalue + nb);
+    std::vector<int> order;
+    int st = *startTrancation;
+    bool fl = *flag_truncation != 0;
+    const int nbk = truncate_host(M, iteration, E, &order, &st, &fl);
+    for (int q = 0; q < nb; ++q) eigenvalue[q] = E[order[q]];
+    if (basis_output) {
+        std::vector<int> bo(basis_output, basis_output + (size_t)nb * rs);
+        for (int q = 0; q < nb; ++q)
+            std::memcpy(basis_output + (size_t)q * rs, &bo[(size_t)order[q] * rs], sizeof(int) * rs);
+    }
+    *numberOfBasis_kept = nbk;
+    *startTrancation = st;
+    *flag_truncation = fl ? 1 : 0;
+    return NRG_OK;
+}
+
 extern "C" int nrg_run(nrg_context* ctx, const nrg_run_input* in, nrg_run_output* out) {
     return run_one(ctx, in, out);
 }

@@ -45,7 +45,7 @@ EXPORTS = [
     "nrg_spike_zero_temperature", "nrg_spike_cfs", "nrg_run", "nrg_context_get_stats",
     "nrg_context_reset_stats", "nrg_context_set_profiling", "nrg_block_eigh_noalloc",
     "nrg_host_alloc", "nrg_host_free", "nrg_run_batch", "nrg_context_release_storage",
-    "nrg_broaden_log_gaussian", "nrg_prepare_basis",
+    "nrg_broaden_log_gaussian", "nrg_prepare_basis", "nrg_truncate",
 ]
 
 
@@ -181,6 +181,8 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
                                              POINTER(c_double), c_int32, POINTER(c_double)]
     lib.nrg_prepare_basis.argtypes = [c_int32, c_int32, c_int32, POINTER(c_int32), c_int32, POINTER(c_int32),
                                       POINTER(c_int32), POINTER(c_int32), c_int32, POINTER(c_int32)]
+    lib.nrg_truncate.argtypes = [c_int32, c_int32, c_int32, c_int32, c_int32, c_int32, POINTER(c_double),
+                                 POINTER(c_int32), POINTER(c_int32), POINTER(c_int32), POINTER(c_int32)]
     lib.nrg_context_get_stats.argtypes = [c_void_p, POINTER(Stats)]
     lib.nrg_context_reset_stats.argtypes = [c_void_p]
     lib.nrg_context_set_profiling.argtypes = [c_void_p, ctypes.c_int]
@@ -226,6 +228,22 @@ def prepare_basis(operation, nVar: int, basis_output):
     if rc != 0:
         raise NrgError(rc, "nrg_prepare_basis", lib.nrg_last_error().decode(errors="replace"))
     return bi, si[:nsub.value].copy()
+
+
+def truncate(iteration: int, first: int, nIter: int, n_keep: int, nVar: int, eigenvalue, basis_output,
+             startTrancation: int, flag_truncation: bool):
+    """nrg_truncate (postprocess.F90:69-168): returns (eigenvalue, basis_output) reordered
+    (kept states in index order, then the discarded ones in energy order), the kept count
+    and the updated (startTrancation, flag_truncation).  Host work: no context, no device."""
+    lib = load_library()
+    E = np.array(eigenvalue, dtype=np.float64, copy=True)
+    bo = np.ascontiguousarray(np.array(basis_output, dtype=np.int32, copy=True).reshape(len(E), nVar + 3))
+    kept, s_t, f_t = c_int32(0), c_int32(int(startTrancation)), c_int32(int(bool(flag_truncation)))
+    rc = lib.nrg_truncate(iteration, first, nIter, n_keep, nVar, len(E), _p(E, c_double), _p(bo, c_int32),
+                          ctypes.byref(kept), ctypes.byref(s_t), ctypes.byref(f_t))
+    if rc != 0:
+        raise NrgError(rc, "nrg_truncate", lib.nrg_last_error().decode(errors="replace"))
+    return E, bo, kept.value, s_t.value, bool(f_t.value)
 
 
 class Context:
