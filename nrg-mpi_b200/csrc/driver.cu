@@ -195,12 +195,44 @@ void prepare_basis_host(const Model& M, const std::vector<int>& bo, int nb_old, 
 
 // sortWithIndex + truncation + sortByIndex (postprocess.F90:71-140).  E is indexed by
 // row (sector order); returns the kept count and the new order of the rows.
+// Stable ascending order of E (std::stable_sort's order under <) by an LSD radix sort on
+// the IEEE bit patterns: negative values have every bit flipped, the others the sign bit
+// set, so unsigned order is numerical order; -0.0 counts as +0.0 (they compare equal).
+// Digits that all keys share are skipped.
+void stable_energy_order(const std::vector<double>& E, std::vector<int>* order) {
+    const int n = (int)E.size();
+    std::vector<uint64_t> key(n);
+    for (int i = 0; i < n; ++i) {
+        const double x = E[i] == 0.0 ? 0.0 : E[i];
+        uint64_t b;
+        std::memcpy(&b, &x, sizeof(b));
+        key[i] = (b >> 63) ? ~b : (b | (1ULL << 63));
+    }
+    std::vector<uint32_t> hist(8 * 256, 0);
+    for (int i = 0; i < n; ++i)
+        for (int d = 0; d < 8; ++d) hist[d * 256 + ((key[i] >> (8 * d)) & 255)]++;
+    std::vector<int> a(n), b(n);
+    std::iota(a.begin(), a.end(), 0);
+    for (int d = 0; d < 8; ++d) {
+        uint32_t* h = &hist[d * 256];
+        if (h[(key[a[0]] >> (8 * d)) & 255] == (uint32_t)n) continue;   // one bucket: order kept
+        uint32_t sum = 0;
+        for (int k = 0; k < 256; ++k) {
+            const uint32_t c = h[k];
+            h[k] = sum;
+            sum += c;
+        }
+        for (int i = 0; i < n; ++i) b[h[(key[a[i]] >> (8 * d)) & 255]++] = a[i];
+        a.swap(b);
+    }
+    order->swap(a);
+}
+
 int truncate_host(const Model& M, int it, const std::vector<double>& E, std::vector<int>* order,
                   int* startTrancation, bool* flag_truncation) {
     const int nb = (int)E.size();
-    order->resize(nb);
-    std::iota(order->begin(), order->end(), 0);
-    std::stable_sort(order->begin(), order->end(), [&](int a, int b) { return E[a] < E[b]; });
+    if (nb > 0) stable_energy_order(E, order);
+    else order->clear();
     int nbk = nb;
     if (it != M.first && it != M.nIter && nb > M.truncation) {
         if (*startTrancation > it) { *startTrancation = it; *flag_truncation = true; }
@@ -220,7 +252,11 @@ int truncate_host(const Model& M, int it, const std::vector<double>& E, std::vec
         }
         nbk = cutoff;
     }
-    std::sort(order->begin(), order->begin() + nbk);
+    // sortByIndex on the kept prefix (:140): the kept rows in increasing order
+    std::vector<char> kept(nb, 0);
+    for (int q = 0; q < nbk; ++q) kept[(*order)[q]] = 1;
+    for (int r = 0, q = 0; r < nb; ++r)
+        if (kept[r]) (*order)[q++] = r;
     return nbk;
 }
 
@@ -228,7 +264,8 @@ void record_flow(nrg_run_output* out, int idx, const std::vector<double>& E, con
     if (!out || !out->flow || out->flowStride <= 0) return;
     std::vector<double> e(nbk);
     for (int q = 0; q < nbk; ++q) e[q] = E[order[q]];
-    std::sort(e.begin(), e.end());
+    const int m = std::min(out->flowStride, nbk);
+    std::partial_sort(e.begin(), e.begin() + m, e.end());
     for (int q = 0; q < out->flowStride; ++q)
         out->flow[(size_t)idx * out->flowStride + q] = q < nbk ? e[q] : NAN;
 }
