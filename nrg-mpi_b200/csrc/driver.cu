@@ -348,11 +348,12 @@ int run_device(nrg_context* ctx, const nrg_run_input* in, nrg_run_output* out, c
 
     // the pinned eigenvalue buffer of the early path, sized once for the run: no iteration
     // keeps more than max(nOps * nb0, 1.2 N_keep) states (postprocess.F90:79-126), so no
-    // iteration has more than nOps times that
+    // iteration has more than nOps times that (capped at 4M values, 32 MB: a run that
+    // effectively never truncates grows the buffer as it goes instead)
     if (ctx->early_evals) {
         const long long keep = std::max<long long>((long long)M.nOps * in->numberOfBasis,
                                                    (long long)(M.truncation * 1.2) + 1);
-        NRG_TRY(ctx->h_evals.ensure(sizeof(double) * (size_t)(keep * M.nOps)));
+        NRG_TRY(ctx->h_evals.ensure(sizeof(double) * (size_t)std::min(keep * M.nOps, 1LL << 22)));
     }
     // ---- forward sweep ----
     for (int it = first; it <= nIter; ++it) {
