@@ -8,6 +8,7 @@ import numpy as np
 import pytest
 
 from oracle import nrg_oracle as O
+from nrg_b200 import model
 
 from helpers import small_siam, write_case
 
@@ -16,6 +17,23 @@ from helpers import small_siam, write_case
 def case(tmp_path_factory):
     d = write_case(small_siam(n_keep=48, n_iterations=14), str(tmp_path_factory.mktemp("restart")))
     return d, O.run(d)
+
+
+@pytest.fixture(scope="module")
+def two_orbital(tmp_path_factory):
+    d = write_case(model.two_orbital_hund(n_keep=96, n_iterations=6), str(tmp_path_factory.mktemp("restart2")))
+    return d, O.run(d)
+
+
+def test_two_orbital_resume_gives_the_full_spectrum(two_orbital, tmp_path):
+    # four matrix types, tied basis records, truncation from the second iteration on
+    d, full = two_orbital
+    assert full.nMat == 4 and full.startTrancation < full.nIter
+    for k in range(full.startTrancation, full.nIter + 1):
+        path = str(tmp_path / f"restart_{k}.dat")
+        O.run_with_restart(d, save_path=path, stop_before=k)
+        st = O.run_with_restart(d, load_path=path)
+        assert np.array_equal(st.binPos, full.binPos) and np.array_equal(st.binNeg, full.binNeg)
 
 
 def test_resume_from_an_interrupted_cfs_loop_gives_the_full_spectrum(case, tmp_path):
