@@ -82,6 +82,86 @@ bool bucket_order(const std::vector<int>& rec, int n, int nVar, std::vector<int>
     return true;
 }
 
+// One pass i of the exchange sequence on ranks R (ids I carried along): the carried key
+// is swapped with every strictly smaller key after position i, until it is the pass's
+// target (the i-th smallest key), after which no key can be smaller.  ready(e) returns
+// once the positions below e hold the previous pass's result; publish(j) announces that
+// this pass is done with the positions below j.
+template <class Ready, class Publish>
+void exchange_pass(int* R, int* I, int n, int i, int t, Ready&& ready, Publish&& publish) {
+    ready(i + 1);
+    int c = R[i], ci = I[i];
+    int j = i + 1;
+    while (c > t && j < n) {
+        ready(std::min(n, j + 256));
+        const int stop = std::min(n, j + 256);
+        while (c > t && j < stop) {
+            // skip keys not smaller than the carried one, eight at a time
+            while (j + 8 <= stop) {
+                int m = 0;
+                for (int u = 0; u < 8; ++u) m |= R[j + u] < c;
+                if (m) break;
+                j += 8;
+            }
+            for (const int end = std::min(stop, j + 8); c > t && j < end; ++j) {
+                const int x = R[j];
+                if (x < c) {
+                    R[j] = c;
+                    c = x;
+                    const int xi = I[j];
+                    I[j] = ci;
+                    ci = xi;
+                }
+            }
+        }
+        publish(j);
+    }
+    R[i] = c;
+    I[i] = ci;
+}
+
+// All passes of the exchange sequence.  Large inputs run consecutive passes on several
+// host threads in a wavefront: pass i+1 reads a position only after pass i has moved past
+// it (an acquire/release progress word per thread, tagged with the pass number), so every
+// swap is the one the serial sequence makes, in the same order per position.
+void exchange_replay(int* R, int* I, const int* target, int n) {
+    const unsigned hw = std::thread::hardware_concurrency();
+    const int T = (int)std::min<unsigned>(8, hw ? hw : 1);
+    if (n < 16384 || T < 2) {
+        for (int i = 0; i < n; ++i)
+            exchange_pass(R, I, n, i, target[i], [](int) {}, [](int) {});
+        return;
+    }
+    // progress word of the pass a thread runs: (pass + 1) << 32 | first position not done
+    std::vector<std::atomic<uint64_t>> prog(T);
+    for (auto& p : prog) p.store(0, std::memory_order_relaxed);
+    auto worker = [&](int k) {
+        for (int i = k; i < n; i += T) {
+            std::atomic<uint64_t>& mine = prog[k];
+            std::atomic<uint64_t>& prev = prog[(k + T - 1) % T];
+            int known = i == 0 ? n : 0;      // positions the previous pass is done with
+            auto ready = [&](int e) {
+                for (int spins = 0; known < e; ++spins) {
+                    const uint64_t v = prev.load(std::memory_order_acquire);
+                    const long long pass = (long long)(v >> 32) - 1;
+                    known = pass > i - 1 ? n : (pass == i - 1 ? (int)(uint32_t)v : 0);
+                    if (known < e && spins > 64) std::this_thread::yield();
+                }
+            };
+            auto publish = [&](int j) {
+                mine.store(((uint64_t)(i + 1) << 32) | (uint32_t)j, std::memory_order_release);
+            };
+            publish(i + 1);
+            exchange_pass(R, I, n, i, target[i], ready, publish);
+            publish(n);
+        }
+    };
+    std::vector<std::thread> pool;
+    for (int k = 1; k < T; ++k) pool.emplace_back(worker, k);
+    worker(0);
+    for (auto& th : pool) th.join();
+}
+
 // sortBasisArray (module.F90:531-602): exchange sort of whole records.  When no two
 // records share (basis, reference) any correct sort gives its result; otherwise the
 // order among equal keys is the exchange sequence's, which is replayed.
@@ -125,34 +205,8 @@ void sort_basis(std::vector<int>& rec, int n, int nVar) {
         target[k] = r;
     }
     std::iota(id.begin(), id.end(), 0);
-    int* R = rk.data();
-    int* I = id.data();
-    for (int i = 0; i < n; ++i) {
-        int c = R[i], ci = I[i];
-        const int t = target[i];
-        int j = i + 1;
-        while (c > t && j < n) {
-            // skip keys not smaller than the carried one, eight at a time
-            while (j + 8 <= n) {
-                int m = 0;
-                for (int u = 0; u < 8; ++u) m |= R[j + u] < c;
-                if (m) break;
-                j += 8;
-            }
-            for (const int end = std::min(n, j + 8); c > t && j < end; ++j) {
-                const int x = R[j];
-                if (x < c) {
-                    R[j] = c;
-                    c = x;
-                    const int xi = I[j];
-                    I[j] = ci;
-                    ci = xi;
-                }
-            }
-        }
-        R[i] = c;
-        I[i] = ci;
-    }
+    exchange_replay(rk.data(), id.data(), target.data(), n);
+    const int* I = id.data();
     std::vector<int> out((size_t)n * rs);
     for (int i = 0; i < n; ++i) std::memcpy(&out[(size_t)i * rs], &rec[(size_t)I[i] * rs], sizeof(int) * rs);
     rec.swap(out);
