@@ -10,6 +10,7 @@
 #include <execinfo.h>
 #include <signal.h>
 #include <unistd.h>
+#include <unordered_set>
 #include <vector>
 
 namespace {
@@ -456,7 +457,7 @@ int nrg_diagonalization(nrg_context* ctx, int32_t iteration, const nrg_diagonali
         // found a term, the previous-sector rows of one group against the columns of the
         // other (IM(jref, iref, type), swapped as the scan says)
         std::vector<HostSeg> segs;
-        std::vector<long long> seen;
+        std::unordered_set<long long> seen;   // segments already listed
         const int nOps = M.nOps;
         for (int s = 0; s < S.nsub; ++s)
             for (int a = 0; a < nOps; ++a) {
@@ -473,8 +474,7 @@ int nrg_diagonalization(nrg_context* ctx, int32_t iteration, const nrg_diagonali
                     const int r0 = sw ? ra : rb, nr = sw ? ca : cb, c0 = sw ? rb : ra, nc = sw ? cb : ca;
                     if (r0 < 0 || c0 < 0 || r0 + nr > nbo || c0 + nc > nbo) continue;   // the kernel flags it
                     const long long key = ((long long)t * nbo + c0) * nbo + r0;
-                    if (std::find(seen.begin(), seen.end(), key) != seen.end()) continue;
-                    seen.push_back(key);
+                    if (!seen.insert(key).second) continue;
                     segs.push_back({r0 + (long long)c0 * nbo + (long long)t * nbo * nbo, nr, nc});
                 }
             }
@@ -552,7 +552,7 @@ static int invmat_common(nrg_context* ctx, int32_t iteration, const nrg_invarian
         const long long nbo = io->numberOfBasis_old;
         const int nOps = M.nOps, nVar = M.nVar;
         std::vector<HostSeg> segs;
-        std::vector<long long> seen;
+        std::unordered_set<long long> seen;   // segments already listed
         for (int L = 0; L < S.nsub; ++L) {
             if (kept[L] == 0) continue;
             for (int R = 0; R < S.nsub; ++R) {
@@ -569,8 +569,7 @@ static int invmat_common(nrg_context* ctx, int32_t iteration, const nrg_invarian
                         const long long r0 = S.refBase[(size_t)R * nOps + a], c0 = S.refBase[(size_t)L * nOps + a];
                         if (r0 < 0 || c0 < 0 || r0 + cR > nbo || c0 + cL > nbo) continue;   // rejected below
                         const long long key = ((long long)m * nbo + c0) * nbo + r0;
-                        if (std::find(seen.begin(), seen.end(), key) != seen.end()) continue;
-                        seen.push_back(key);
+                        if (!seen.insert(key).second) continue;
                         segs.push_back({r0 + c0 * nbo + (long long)m * nbo * nbo, cR, cL});
                     }
                 }

@@ -9,6 +9,7 @@
 #include <cmath>
 #include <cstring>
 #include <numeric>
+#include <unordered_set>
 
 namespace nrg {
 
@@ -895,7 +896,7 @@ std::vector<HostSeg> spike_ims_segs(const Model& M, const IterView& it, const st
     const long long nbo = nb_old;
     const std::vector<SpecJob> jobs = gs_sectors ? t0_jobs(M, it, *gs_sectors) : cfs_jobs(M, it);
     std::vector<HostSeg> segs;
-    std::vector<long long> seen;
+    std::unordered_set<long long> seen;   // segments already listed
     for (const auto& j : jobs)
         for (int a = 0; a < nOps; ++a) {
             const int ck = S.cnt(j.k, a), cl = S.cnt(j.l, a);
@@ -906,8 +907,7 @@ std::vector<HostSeg> spike_ims_segs(const Model& M, const IterView& it, const st
             const long long r0 = j.part == 0 ? rl : rk, c0 = j.part == 0 ? rk : rl;
             const int nr = j.part == 0 ? cl : ck, nc = j.part == 0 ? ck : cl;
             const long long key = ((long long)j.m * nbo + c0) * nbo + r0;
-            if (std::find(seen.begin(), seen.end(), key) != seen.end()) continue;
-            seen.push_back(key);
+            if (!seen.insert(key).second) continue;
             segs.push_back({r0 + c0 * nbo + (long long)j.m * nbo * nbo, nr, nc});
         }
     return segs;
