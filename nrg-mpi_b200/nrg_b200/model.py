@@ -1,6 +1,6 @@
 """Input side of the NRG hot path: model generators and the reference's input files.
 
-The reference reads three files (SURVEY layout, reference files cited inline):
+The reference reads three files (reference files cited inline):
 
 * ``parameter.txt``      namelist ``&nrg``             (module.F90:656-688)
 * ``hamiltonianInfo.dat`` namelist ``&hamiltonianInfo`` (module.F90:846-862)

@@ -1,8 +1,8 @@
 """CPU oracle for the NRG hot path of eminamitani/nrg-mpi.
 
 TEST INFRASTRUCTURE.  Only ``tests/``, ``__graft_entry__.smoke()`` and the CPU-baseline
-leg of ``bench.py`` may import this module, and only as the checker or as the timed CPU
-baseline: the product never routes work through it.
+leg of ``bench.py`` may import this module, and only as the reference that results are
+compared with or as the timed CPU baseline: the product never routes work through it.
 
 What it is: a restatement, in numpy/scipy plus a small C helper, of the reference's
 per-iteration NRG algorithm and of the CFS spectrum that follows it, with the reference's
