@@ -20,6 +20,7 @@
 #include <numeric>
 #include <string>
 #include <thread>
+#include <unordered_map>
 #include <vector>
 
 using namespace nrg;
@@ -322,6 +323,57 @@ void record_flow(nrg_run_output* out, int idx, const std::vector<double>& E, con
     std::partial_sort(e.begin(), e.begin() + m, e.end());
     for (int q = 0; q < out->flowStride; ++q)
         out->flow[(size_t)idx * out->flowStride + q] = q < nbk ? e[q] : NAN;
+}
+
+// For each sector s of the table si (nsub records of nVar+3 ints): how many of the first
+// nbk records of bo carry its quantum numbers, and the index of the first of them (-1
+// when none), as the scan of postprocess.F90:303-321 finds them; one pass over the
+// records with exact 64-bit keys (up to four 16-bit quantum numbers), the scan itself
+// otherwise (or when two sectors share their numbers).
+void kept_in_sectors(const std::vector<int>& si, int nsub, const std::vector<int>& bo, int nbk, int nVar,
+                     std::vector<int>* count, std::vector<int>* first) {
+    const int rs = nVar + 3;
+    count->assign(nsub, 0);
+    first->assign(nsub, -1);
+    auto key = [&](const int* q, uint64_t* k) {
+        uint64_t x = 0;
+        for (int v = 0; v < nVar; ++v) {
+            if (q[v] < -32768 || q[v] > 32767) return false;
+            x = (x << 16) | (uint16_t)(int16_t)q[v];
+        }
+        *k = x;
+        return true;
+    };
+    bool packed = nVar <= 4;
+    std::unordered_map<uint64_t, int> sector;
+    if (packed) {
+        sector.reserve(2 * (size_t)nsub);
+        for (int s = 0; s < nsub && packed; ++s) {
+            uint64_t k = 0;
+            packed = key(&si[(size_t)s * rs], &k) && sector.emplace(k, s).second;
+        }
+    }
+    for (int j = 0; packed && j < nbk; ++j) {
+        uint64_t k = 0;
+        if (!key(&bo[(size_t)j * rs], &k)) { packed = false; break; }
+        const auto it = sector.find(k);
+        if (it == sector.end()) continue;
+        if ((*first)[it->second] < 0) (*first)[it->second] = j;
+        (*count)[it->second]++;
+    }
+    if (packed) return;
+    count->assign(nsub, 0);
+    first->assign(nsub, -1);
+    for (int s = 0; s < nsub; ++s)
+        for (int j = 0; j < nbk; ++j) {
+            bool eq = true;
+            for (int v = 0; v < nVar; ++v)
+                if (si[(size_t)s * rs + v] != bo[(size_t)j * rs + v]) { eq = false; break; }
+            if (eq) {
+                if ((*first)[s] < 0) (*first)[s] = j;
+                (*count)[s]++;
+            }
+        }
 }
 
 struct IterRec {
@@ -892,14 +944,10 @@ int run_drop_in(nrg_context* ctx, const nrg_run_input* in, nrg_run_output* out, 
                 fbo.insert(fbo.end(), bo_re.begin(), bo_re.begin() + (size_t)nbk * rs);
                 fE.insert(fE.end(), E_re.begin(), E_re.begin() + nbk);
                 fbi.insert(fbi.end(), bi.begin(), bi.end());
+                std::vector<int> kcount, kfirst;
+                kept_in_sectors(si, nsub, bo_re, nbk, nVar, &kcount, &kfirst);
                 for (int s = 0; s < nsub; ++s) {
-                    int k = 0, first_out = -1;
-                    for (int j = 0; j < nbk; ++j) {
-                        bool eq = true;
-                        for (int v = 0; v < nVar; ++v)
-                            if (si[(size_t)s * rs + v] != bo_re[(size_t)j * rs + v]) { eq = false; break; }
-                        if (eq) { if (first_out < 0) first_out = j; ++k; }
-                    }
+                    const int k = kcount[s], first_out = kfirst[s];
                     if (k == 0) continue;
                     const int d = si[(size_t)s * rs + nVar];
                     for (int v = 0; v < nVar; ++v) fsi.push_back(si[(size_t)s * rs + v]);
