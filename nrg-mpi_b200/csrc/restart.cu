@@ -72,8 +72,22 @@ int get_count(FILE* f, int32_t* v) {
     }
     return NRG_OK;
 }
+// n elements read into v; a count read from the file is checked against the bytes the
+// file still holds before anything is allocated, so a damaged count is reported as a
+// broken file rather than failing an allocation
 template <class T>
 int get_vec(FILE* f, std::vector<T>& v, size_t n) {
+    const long long here = ftello(f);
+    long long end = -1;
+    if (here >= 0 && fseeko(f, 0, SEEK_END) == 0) end = ftello(f);
+    if (end < here || fseeko(f, here, SEEK_SET) != 0) {
+        nrg_set_error_message("broken restart file: cannot seek");
+        return NRG_ERR_INVALID;
+    }
+    if (n > (size_t)(end - here) / sizeof(T)) {
+        nrg_set_error_message("broken restart file: truncated");
+        return NRG_ERR_INVALID;
+    }
     v.resize(n);
     return get(f, v.data(), sizeof(T) * n);
 }
@@ -226,7 +240,7 @@ int restart_load(const char* path, const Model& M, int nbin, RestartData* D) {
     NRG_TRY(get_count(f, &d1));
     NRG_TRY(get_count(f, &d2));
     NRG_TRY(get_count(f, &d3));
-    if (d1 != d2 || d3 != M.nMat) {
+    if (d1 != d2 || d3 != M.nMat || d1 > (1 << 20)) {
         nrg_set_error_message("broken restart file: initial spectrum matrices (%d, %d, %d)", d1, d2, d3);
         return NRG_ERR_INVALID;
     }
