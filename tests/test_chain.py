@@ -5,7 +5,8 @@ Campo-Oliveira flat-band chain, which is Wilson's divided by A_Lambda (same weig
 energies scaled by 1/A_Lambda); zero on-site energies for a particle-hole symmetric
 bath; the chain of a whole star reproduces the star's levels and weights; and through
 the oracle, the NRG spectrum of a non-interacting impurity on a particle-hole asymmetric
-bath equals the free-fermion spectrum of the same chain."""
+bath equals the free-fermion spectrum of the same chain, and its T = 0 spectral weights
+the single-particle weights |phi_k(d)|^2 at eps_k."""
 import itertools
 import math
 
@@ -86,3 +87,17 @@ def test_noninteracting_impurity_on_an_asymmetric_bath(tmp_path):
     e_nrg = np.sort(st.eigenvalue)
     assert e_nrg.size == e_mb.size
     assert np.max(np.abs(e_nrg - e_mb)) < 1e-10 * max(1.0, e_mb[-1])
+    # T = 0 spectral weights: |phi_k(d)|^2 at eps_k, positive or negative (one spin)
+    O.spike_zero_temperature(st, last)
+    eps, phi = np.linalg.eigh(h)
+    nbin = st.numberOfBin
+    exp_pos = np.zeros((nbin * st.nMat, 2), order="F")
+    exp_neg = np.zeros((nbin * st.nMat, 2), order="F")
+    w = phi[0, :] ** 2
+    for m in range(st.nMat):
+        pos = eps > 0
+        O.bin_spikes(st, exp_pos, eps[pos].copy(), w[pos].copy(), m)
+        O.bin_spikes(st, exp_neg, -np.abs(eps[~pos]).copy(), w[~pos].copy(), m)
+    assert np.max(np.abs(st.binPos[:, 1] - exp_pos[:, 1])) < 1e-10
+    assert np.max(np.abs(st.binNeg[:, 1] - exp_neg[:, 1])) < 1e-10
+    assert abs(w[eps > 0].sum() - w[eps < 0].sum()) > 1e-3          # the asymmetry shows
