@@ -6,8 +6,8 @@
  * below replaces one of those routines; its arguments are exactly the module arrays the
  * routine reads and writes (raw pointers, sizes, 1-based integer values inside the
  * packed records, Fortran column-major real arrays), so a Fortran caller binds them with
- * ISO_C_BINDING (see INTEGRATION.md for the interface block and the wrapper subroutines
- * that keep the reference's names).
+ * ISO_C_BINDING: a bind(C) interface block for the entries and records below, and
+ * wrapper subroutines with the reference's names that pass the module arrays.
  *
  * Pointers may be host or device memory (CUDA unified addressing tells them apart).
  * Host arrays are copied to the device inside the call and results copied back before
@@ -21,7 +21,9 @@
  *
  * Every call returns an NRG_* status; nrg_last_error() describes the last failure.
  * There is no CPU fallback: without a usable CUDA device every compute call fails with
- * NRG_ERR_DEVICE.
+ * NRG_ERR_DEVICE.  The two host bookkeeping entries (nrg_prepare_basis, nrg_truncate)
+ * are integer and sorting work that the reference also does on the host; they need no
+ * device.
  */
 #ifndef NRG_B200_H
 #define NRG_B200_H
