@@ -1,32 +1,38 @@
 """Benchmark of the NRG hot path on B200.
 
-One step = one full run of the reference's driver (main.F90) on the plain-FP64 SIAM
-workload: Lambda=2, U=0.2, Gamma=0.02, eps_d=-0.1, N_keep=2048, 60 NRG iterations, then
-the backward reduced density matrices and the T=0 CFS spectrum on the reference's
-1000-bins-per-decade grid.  Metric: NRG iterations per second (60 per step), whole job.
+One step = one full run of the reference's driver (main.F90) on the SIAM workload with
+N_keep = 4096: Lambda=2, U=0.3, Gamma=0.03, eps_d=-0.15, 60 NRG iterations (sectors of
+order up to ~1300), then the backward reduced density matrices and the T=0 CFS spectrum
+on the reference's 1000-bins-per-decade grid, all in FP64.  Metric: NRG iterations per
+second (60 per step), whole job.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
 
 * value: device-resident run (nrg_run), inputs resident, timed with CUDA events on the
   stream the library launches on, barrier + synchronize on both sides, max over ranks.
+* forward_only: the same sweep without the density matrices and the spectrum (the scope
+  of the reference arm's steps).
 * e2e: the same metric through the drop-in entry points with host arrays (every routine
-  copies its module arrays host->device and back, as a Fortran caller would).
-* roofline: k_tri_cluster, the Householder tridiagonalisation of the sectors of order
-  > 128 (the largest share of device time): algorithmic flops sum_s 4/3 d_s^3 per launch
-  over its event-timed launch duration, against a cuBLAS DGEMM peak measured here (the
-  FP64 ceiling; tcgen05 has no FP64 kind); traffic = DRAM bytes per launch from the ncu
-  capture summarised in profiles/.  "eigensolver" gives the same for the whole
-  eigensolver of an iteration (sum_s (4/3+2) d_s^3 over the event-timed window).
+  copies its module arrays host->device and back, as a Fortran caller would), with the
+  caller's arrays page-locked; e2e.pageable: the same with pageable arrays (a Fortran
+  allocatable), which the routines copy whole.
+* roofline: the kernel with the largest share of device time, k_tri_cluster (Householder
+  tridiagonalisation of the sectors of order > 128): algorithmic flops sum_s 4/3 d_s^3
+  per launch over its event-timed launch duration, against a cuBLAS DGEMM peak measured
+  here (the FP64 ceiling; tcgen05 has no FP64 kind); traffic = DRAM bytes per launch of an
+  ncu capture of this workload, read from profiles/roofline_traffic.json (null without
+  it).  "eigensolver" gives the same for the whole eigensolver of an iteration
+  (sum_s (4/3+2) d_s^3 over the event-timed window).
 * cpu_baseline: the oracle (numpy/scipy port of the reference path, OpenBLAS on all host
-  threads) on a bounded sample of the same sweep.
-* --impl reference: the oracle port timed per NRG iteration of the same sweep (steps are
-  full-size iterations), rank 0 only.
-* fdm: the same sweep with the full-density-matrix spectrum and density matrices at
+  threads) on full-size forward iterations of the same sweep (a bounded sample).
+* --impl reference: the oracle port timed per full-size forward NRG iteration of the same
+  sweep (prepareBasis, dsyev per sector, truncation, both invariant-matrix routines),
+  rank 0 only: the reference cannot be built here (Fortran, MPI, MKL).
+* n_keep_2048: the N_keep = 2048 SIAM workload (Lambda=2, U=0.2, Gamma=0.02,
+  eps_d=-0.1, 60 iterations), one warm-up and two event-timed sweeps.
+* fdm: that workload with the full-density-matrix spectrum and density matrices at
   T = 1e-6 (the workload table's temperature; no reference counterpart: the reference's
   spectrum is the T = 0 CFS one), one warm-up and two event-timed sweeps.
-* n_keep_4096: the larger SIAM workload (Lambda=2, U=0.3, Gamma=0.03, eps_d=-0.15,
-  N_keep=4096, 60 iterations, sectors of order up to ~1300), one warm-up and one
-  event-timed sweep on the same stream.
 * many_instance: independent impurity models side by side (nrg_run_batch): the 27 draws
   with N_keep <= 1024 of the seeded 64-SIAM sweep (50 iterations each, T=0 CFS), run one
   at a time and then 8 in flight; wall clock around each batch with the device
@@ -52,15 +58,13 @@ for _p in (ROOT, os.path.join(ROOT, "nrg-mpi_b200")):
 
 import numpy as np  # noqa: E402
 
-WORKLOAD = dict(U=0.2, Gamma=0.02, eps_d=-0.1, Lambda=2.0, n_keep=2048, n_iterations=60)
-WORKLOAD_NAME = ("SIAM flat band Lambda=2.0 U=0.2 Gamma=0.02 eps_d=-0.1 N_keep=2048, "
+WORKLOAD = dict(U=0.3, Gamma=0.03, eps_d=-0.15, Lambda=2.0, n_keep=4096, n_iterations=60)
+WORKLOAD_NAME = ("SIAM flat band Lambda=2.0 U=0.3 Gamma=0.03 eps_d=-0.15 N_keep=4096, "
                  "60 NRG iterations + backward RDM + T=0 CFS spectrum (1000 bins/decade)")
+SECOND = dict(U=0.2, Gamma=0.02, eps_d=-0.1, Lambda=2.0, n_keep=2048, n_iterations=60)
 METRIC = "NRG iterations/s (full sweep + RDM + CFS spectrum, FP64, eig err <= 1e-12)"
-# DRAM bytes (read + write) per k_tri_cluster launch of this workload, from the ncu
-# capture in profiles/k_tri_cluster_siam_nkeep2048.md (average over the two launches of
-# one iteration)
-TRI_TRAFFIC_BYTES = 12.03e6
-TRI_TRAFFIC_SOURCE = "profiles/k_tri_cluster_siam_nkeep2048.md"
+# DRAM bytes per launch of the roofline kernel, from an ncu capture of this workload
+TRAFFIC_FILE = os.path.join(ROOT, "profiles", "roofline_traffic.json")
 
 
 def parse():
@@ -73,7 +77,9 @@ def parse():
     p.add_argument("--no-cpu", action="store_true")
     p.add_argument("--no-many", action="store_true")
     p.add_argument("--no-fdm", action="store_true")
-    p.add_argument("--no-nk4096", action="store_true")
+    p.add_argument("--no-nk2048", action="store_true")
+    p.add_argument("--no-pageable", action="store_true")
+    p.add_argument("--e2e-steps", type=int, default=3)
     # profiling helpers: a shorter sweep of the same model (not the headline workload)
     p.add_argument("--iterations", type=int, default=None)
     p.add_argument("--n-keep", type=int, default=None)
@@ -199,45 +205,49 @@ def many_instance(torch, dev, rank, world, dist, concurrency=8):
             "ranks": world, "timing": "wall clock around each batch, device synchronised, max over ranks"}
 
 
-def larger_workload(torch, dev, local, stream):
-    """One sweep of the N_keep = 4096 SIAM workload after one warm-up sweep, CUDA events
-    on the library's stream; the context's device storage is released afterwards."""
+def second_workload(torch, dev, local, stream, fdm_temperature=None):
+    """The N_keep = 2048 workload: one warm-up and two sweeps, CUDA events on the library's
+    stream (T = 0 CFS spectrum, or with fdm_temperature the FDM spectrum at that T); the
+    context's storage is released afterwards."""
     from nrg_b200 import Context, model
-    inp = model.config(3)
+    inp = model.siam(**SECOND)
     n_it = inp.numberOfIteration - inp.indexOfFirstIteration + 1
+    T = fdm_temperature or 0.0
     c = Context(local)
     try:
         c.set_model(inp)
         c.set_stream(stream.cuda_stream)
-        c.run(spectrum=True)
+        c.run(spectrum=True, temperature=T)
         torch.cuda.synchronize(dev)
-        c.set_profiling(True)
-        c.reset_stats()
         s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        ph = []
         s.record(stream)
-        r = c.run(spectrum=True)
+        for _ in range(2):
+            r = c.run(spectrum=True, temperature=T)
+            ph.append(r["phaseSeconds"].copy())
         e.record(stream)
         torch.cuda.synchronize(dev)
-        st = c.stats()
-        c.set_profiling(False)
-        ms = s.elapsed_time(e)
+        ms = s.elapsed_time(e) / 2
         nbin = r["numberOfBin"]
         sums = [float(r["binPos"][m * nbin:(m + 1) * nbin, 1].sum() + r["binNeg"][m * nbin:(m + 1) * nbin, 1].sum())
                 for m in range(inp.numberOfMatrix)]
-        ph = r["phaseSeconds"]
-        return {"workload": "SIAM Lambda=2.0 U=0.3 Gamma=0.03 eps_d=-0.15 N_keep=4096, 60 iterations "
-                            "+ backward RDM + T=0 CFS spectrum",
-                "ms_per_sweep": ms, "iterations_per_s": n_it * 1e3 / ms,
-                "phase_seconds": {"nrg_sweep": float(ph[0]), "rdm": float(ph[1]), "cfs_spectrum": float(ph[2])},
-                "eigensolver_ms_per_window": st["syev_ms"] / max(st["syev_launches"], 1),
-                "sum_rule": sums,
-                "timing": "CUDA events on the library's stream, 1 sweep after 1 warm-up"}
+        p = np.mean(np.array(ph), axis=0)
+        out = {"workload": "SIAM Lambda=2.0 U=0.2 Gamma=0.02 eps_d=-0.1 N_keep=2048, 60 iterations + backward "
+                           + ("RDM + T=0 CFS spectrum" if not T else f"density matrices + FDM spectrum at T={T}"),
+               "ms_per_sweep": ms, "iterations_per_s": n_it * 1e3 / ms,
+               "phase_seconds": {"nrg_sweep": float(p[0]), "rdm": float(p[1]), "spectrum": float(p[2])},
+               "sum_rule": sums,
+               "timing": "CUDA events on the library's stream, 2 sweeps after 1 warm-up"}
+        if T:
+            out["temperature"] = T
+            out["shell_trace_max_dev"] = float(np.nanmax(np.abs(r["rdmTrace"] - 1.0)))
+        return out
     finally:
         c.close()
 
 
-def cpu_sample(n_timed=3):
-    """Oracle port on full-size iterations of the same sweep (forward path only)."""
+def cpu_sample(n_timed=2):
+    """Oracle port on full-size forward iterations of the same sweep."""
     from nrg_b200 import model
     from oracle import nrg_oracle as O
     inp = model.siam(**WORKLOAD)
@@ -253,7 +263,17 @@ def cpu_sample(n_timed=3):
         O.nrg_iteration(st, it)
         it += 1
     dt = time.perf_counter() - t0
-    return n_timed / dt, dt, it - n_timed, it - 1
+    return n_timed / dt, dt, it - n_timed, it - 1, int(st.numberOfBasis_full)
+
+
+def roofline_traffic():
+    """DRAM bytes per launch of the roofline kernel on this workload (ncu), if captured."""
+    try:
+        with open(TRAFFIC_FILE) as f:
+            t = json.load(f)
+        return float(t["bytes_per_launch"]), os.path.relpath(TRAFFIC_FILE, ROOT)
+    except (OSError, ValueError, KeyError):
+        return None, None
 
 
 def reference_arm(args):
@@ -290,8 +310,11 @@ def reference_arm(args):
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": dt / args.steps * 1e3, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": WORKLOAD_NAME, "n_keep": 2048, "iterations": 60,
-                   "parallelism": "replicas", "step": "one full-size NRG iteration (nb ~ 8200)"},
+        "config": {"workload": WORKLOAD_NAME, "n_keep": WORKLOAD["n_keep"], "iterations": 60,
+                   "parallelism": "replicas",
+                   "step": f"one full-size forward NRG iteration (nb ~ {int(st.numberOfBasis_full)})",
+                   "scope": "forward iterations only (prepareBasis, dsyev per sector, truncation, both "
+                            "invariant-matrix routines): compare with the b200 arm's forward_only"},
         "cpu_baseline": {"value": v, "unit": "iterations/s", "cores": cores, "kind": "port",
                          "sample": f"forward NRG iterations {it - args.steps}..{it - 1} of the sweep "
                                    "(prepareBasis, dsyev per sector, truncation, invariant matrices)"},
@@ -355,57 +378,55 @@ def main():
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         t_max = float(t.item())
     value = n_it * args.steps * world / t_max
-    # end to end through the drop-in entry points with host arrays
-    e2e = None
-    if not args.no_e2e:
-        # one untimed run pins the host module arrays (first-use allocation), then K timed
-        r2 = ctx.run(spectrum=True, host_drop_in=True)
+    # the forward sweep alone (the reference arm's scope), one event-timed sweep
+    sf, ef = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    sf.record(stream)
+    ctx.run(spectrum=False)
+    ef.record(stream)
+    torch.cuda.synchronize(dev)
+    forward_only = {"value": n_it * 1e3 / sf.elapsed_time(ef), "unit": "iterations/s",
+                    "timing": "one sweep without density matrices and spectrum, CUDA events"}
+
+    def drop_in(pageable, steps):
+        # one untimed run allocates the emulated caller's module arrays, then K timed runs
+        r = ctx.run(spectrum=True, host_drop_in=True, host_pageable=pageable)
         torch.cuda.synchronize(dev)
         ctx.reset_stats()
         if dist is not None:
             dist.barrier()
         t0 = time.perf_counter()
-        for _ in range(args.steps):
-            r2 = ctx.run(spectrum=True, host_drop_in=True)
+        for _ in range(steps):
+            r = ctx.run(spectrum=True, host_drop_in=True, host_pageable=pageable)
         torch.cuda.synchronize(dev)
-        dt = (time.perf_counter() - t0) / args.steps
+        dt = (time.perf_counter() - t0) / steps
         st2 = ctx.stats()
         if dist is not None:
             t = torch.tensor([dt], device=dev, dtype=torch.float64)
             dist.all_reduce(t, op=dist.ReduceOp.MAX)
             dt = float(t.item())
-        same = float(max(np.max(np.abs(r2["binPos"][:, 1] - res["binPos"][:, 1])),
-                         np.max(np.abs(r2["binNeg"][:, 1] - res["binNeg"][:, 1]))))
-        e2e = {"value": n_it * world / dt, "unit": "iterations/s",
-               "h2d_bytes_per_step": int(st2["h2d_bytes"]) // args.steps,
-               "d2h_bytes_per_step": int(st2["d2h_bytes"]) // args.steps,
-               "path": "drop-in entry points with host arrays (Fortran caller's data flow; module "
-                       "arrays in pinned host memory, allocated in one untimed warm-up run)",
-               "max_bin_diff_vs_device_resident": same}
-    fdm = None
-    if not args.no_fdm:
-        T_fdm = 1e-6
-        ctx.run(spectrum=True, temperature=T_fdm)
-        torch.cuda.synchronize(dev)
-        s2, e2 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        fph = []
-        s2.record(stream)
-        for _ in range(2):
-            rf = ctx.run(spectrum=True, temperature=T_fdm)
-            fph.append(rf["phaseSeconds"].copy())
-        e2.record(stream)
-        torch.cuda.synchronize(dev)
-        fms = s2.elapsed_time(e2) / 2
-        nbf = rf["numberOfBin"]
-        fsum = [float(rf["binPos"][m * nbf:(m + 1) * nbf, 1].sum() + rf["binNeg"][m * nbf:(m + 1) * nbf, 1].sum())
-                for m in range(inp.numberOfMatrix)]
-        fp = np.mean(np.array(fph), axis=0)
-        fdm = {"temperature": T_fdm, "ms_per_sweep": fms, "iterations_per_s": n_it * 1e3 / fms,
-               "phase_seconds": {"nrg_sweep": float(fp[0]), "rdm": float(fp[1]), "fdm_spectrum": float(fp[2])},
-               "sum_rule": fsum,
-               "shell_trace_max_dev": float(np.nanmax(np.abs(rf["rdmTrace"] - 1.0))),
-               "timing": "CUDA events on the library's stream, 2 sweeps after 1 warm-up"}
-    nk4096 = None if args.no_nk4096 else larger_workload(torch, dev, local, stream)
+        same = float(max(np.max(np.abs(r["binPos"][:, 1] - res["binPos"][:, 1])),
+                         np.max(np.abs(r["binNeg"][:, 1] - res["binNeg"][:, 1]))))
+        return {"value": n_it * world / dt, "unit": "iterations/s",
+                "h2d_bytes_per_step": int(st2["h2d_bytes"]) // steps,
+                "d2h_bytes_per_step": int(st2["d2h_bytes"]) // steps, "steps": steps,
+                "max_bin_diff_vs_device_resident": same}
+
+    # end to end through the drop-in entry points with host arrays
+    e2e = None
+    if not args.no_e2e:
+        k = max(1, min(args.steps, args.e2e_steps))
+        e2e = drop_in(False, k)
+        e2e["path"] = ("drop-in entry points with host arrays (the Fortran caller's data flow), module "
+                       "arrays in page-locked host memory allocated in one untimed run; host<->device "
+                       "copies inside the timed region")
+        e2e["timing"] = "wall clock around the runs, device synchronised, max over ranks"
+        if not args.no_pageable:
+            pg = drop_in(True, 1)
+            pg["path"] = "the same with the module arrays in pageable memory (a Fortran allocatable)"
+            e2e["pageable"] = pg
+    ctx.release_storage()   # the headline's device storage; the model stays set
+    nk2048 = None if args.no_nk2048 else second_workload(torch, dev, local, stream)
+    fdm = None if args.no_fdm else second_workload(torch, dev, local, stream, fdm_temperature=1e-6)
     many = None if args.no_many else many_instance(torch, dev, rank, world, dist)
     if rank == 0:
         clocks = clk.summary()
@@ -419,26 +440,30 @@ def main():
         tri_avg_s = stats["tri_ms"] * 1e-3 / max(stats["tri_launches"], 1)
         tri_flops = stats["tri_flops"] / max(stats["tri_launches"], 1)
         tri_ach = tri_flops / tri_avg_s / 1e12 if tri_avg_s > 0 else None
+        traffic, traffic_src = roofline_traffic()
         cpu = None
         if not args.no_cpu:
-            v, dt, i0, i1 = cpu_sample()
+            v, dt, i0, i1, nbf = cpu_sample()
             cpu = {"value": v, "unit": "iterations/s", "cores": os.cpu_count(), "kind": "port",
-                   "sample": f"forward NRG iterations {i0}..{i1} of the same sweep (nb ~ 8200 each), "
-                             f"{dt:.1f} s, numpy/scipy-OpenBLAS oracle; forward path only"}
+                   "sample": f"forward NRG iterations {i0}..{i1} of the same sweep (nb ~ {nbf} each), "
+                             f"{dt:.1f} s, numpy/scipy-OpenBLAS oracle; forward path only (compare with "
+                             "forward_only)"}
         line = {
             "metric": METRIC, "value": value, "unit": "iterations/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": t_max / args.steps * 1e3,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic (generated Wilson chain and impurity tables)",
-            "config": {"workload": WORKLOAD_NAME, "n_keep": 2048, "iterations": n_it,
+            "config": {"workload": WORKLOAD_NAME, "n_keep": WORKLOAD["n_keep"], "iterations": n_it,
                        "parallelism": f"replicas x{world}",
-                       "l2": "working set > L2: each step writes ~1 GB of eigenvector blocks"},
+                       "l2": "working set > L2: each step writes ~20 GB of eigenvector blocks and "
+                             "spectral matrices"},
             "phase_seconds": {"nrg_sweep": float(ph[0]), "rdm": float(ph[1]), "cfs_spectrum": float(ph[2])},
             "spectrum_seconds": float(ph[2]),
+            "forward_only": forward_only,
             "sum_rule": sums,
             "gpu_launches": int(launches),
             "roofline": {"kernel": "k_tri_cluster (FP64 Householder tridiagonalisation of the sectors of "
-                                   "order > 128, one 8-block cluster per sector)",
+                                   "order > 128, one thread-block cluster per sector)",
                          "bound": "tensor", "pipe": "fp64",
                          "achieved": tri_ach, "peak": peak, "unit": "TFLOP/s",
                          "frac": (tri_ach / peak) if (tri_ach and peak) else None,
@@ -446,7 +471,7 @@ def main():
                                         "FP64 figure)",
                          "flops_per_launch": tri_flops, "avg_launch_ms": tri_avg_s * 1e3,
                          "launches": int(stats["tri_launches"]),
-                         "traffic": TRI_TRAFFIC_BYTES, "traffic_source": TRI_TRAFFIC_SOURCE},
+                         "traffic": traffic, "traffic_source": traffic_src},
             "eigensolver": {"what": "all sectors of one iteration: tridiagonalisation, divide and conquer, "
                                     "back-transformation (three streams)",
                             "achieved": achieved, "unit": "TFLOP/s", "peak": peak,
@@ -456,8 +481,8 @@ def main():
             "clocks": clocks,
             "e2e": e2e,
             "cpu_baseline": cpu,
+            "n_keep_2048": nk2048,
             "fdm": fdm,
-            "n_keep_4096": nk4096,
             "many_instance": many,
         }
         print(json.dumps(line), flush=True)

@@ -159,11 +159,11 @@ NRG_API int nrg_truncate(int32_t iteration, int32_t indexOfFirstIteration, int32
                          int32_t* basis_output, int32_t* numberOfBasis_kept, int32_t* startTrancation,
                          int32_t* flag_truncation);
 
-/* ---- diagonalization(iteration, ismysubspace)  (diagonalization.F90:1-529) ----------
+/* ---- diagonalization(iteration, ismysubspace)  (diagonalization.F90:1-410) ----------
  * Replaces the routine called from nrgIteration.F90:23.  Per symmetry sector: assemble
- * the block Hamiltonian (diagonalization.F90:272-381), diagonalise it (dsyev 'V','U',
- * :386), chop |V| < 1e-14 (:392-399); then shift the eigenvalues by their minimum and
- * zero those <= 1e-12 (:469-475) and rebuild basis_output (:513-526).  ismysubspace of
+ * the block Hamiltonian (diagonalization.F90:162-262), diagonalise it (dsyev 'V','U',
+ * :267), chop |V| < 1e-14 (:273-280); then shift the eigenvalues by their minimum and
+ * zero those <= 1e-12 (:353-356) and rebuild basis_output (:394-407).  ismysubspace of
  * the reference is not needed: one device owns all sectors. */
 typedef struct nrg_diagonalization_io {
     int32_t numberOfSubspace;          /* in                                             */
@@ -177,7 +177,7 @@ typedef struct nrg_diagonalization_io {
     double* eigenvector;               /* out [sizeOfEigenvector] column-major blocks    */
     int64_t sizeOfEigenvector;         /* in  capacity = sum over sectors of dimension^2 */
     int32_t* basis_output;             /* out [nb*(nVar+3)]                              */
-    double* groundStateEnergy;         /* out eigenvalue(1) before the shift (:470)      */
+    double* groundStateEnergy;         /* out eigenvalue(1) before the shift (:351)      */
 } nrg_diagonalization_io;
 NRG_API int nrg_diagonalization(nrg_context* ctx, int32_t iteration, const nrg_diagonalization_io* io);
 
@@ -267,12 +267,19 @@ NRG_API int nrg_spike_cfs(nrg_context* ctx, int32_t iteration, const nrg_spike_i
  * column order.  H, eigenvalues and eigenvectors are caller-owned device arrays (H may
  * equal eigenvectors).  No context is needed: the call runs on the current device and on
  * `stream` (NULL = default stream), and returns after the stream has drained.
- * Its workspace is a static device array of about 417 KB, present on every device that
- * loads the library until the process exits.  The first call on a device looks up that
- * array's address (cudaGetSymbolAddress), so make the first call before any stream
- * capture.  Every call shares the one array: calls that overlap on the GPU (concurrent
- * streams, threads) race and must be serialised by the caller.  Orders above the maximum
- * return NRG_ERR_TOO_LARGE. */
+ * Its workspace is a static device array of about 417 KB, created on a device when the
+ * library's device code is loaded there (with lazy module loading, the CUDA default, at
+ * the first call on that device: a warm-up call during the caller's set-up keeps that
+ * load out of later work) and held until the process exits.  The first call on a device
+ * looks up that array's address (cudaGetSymbolAddress) and keeps it for the device's
+ * CUDA context; after a device reset the next call looks it up again.  So make the first
+ * call before any stream capture.  Each call copies a small descriptor to the device,
+ * reads a status word back and returns after `stream` has drained.  Every call shares the
+ * one array, which keeps the previous call's contents (the call clears its status word
+ * itself): calls that overlap on the GPU (concurrent streams, threads) race and must be
+ * serialised by the caller.  H, eigenvalues and eigenvectors must be memory of the current
+ * device or managed memory (NRG_ERR_INVALID otherwise).  A block holding NaN or Inf
+ * returns NRG_ERR_NUMERIC.  Orders above the maximum return NRG_ERR_TOO_LARGE. */
 #define NRG_NOALLOC_MAX_ORDER 128
 NRG_API int nrg_block_eigh_noalloc(const double* H, int32_t n, double* eigenvalues,
                                    double* eigenvectors, void* stream);
@@ -323,6 +330,11 @@ typedef struct nrg_run_input {
                                              the file's iteration; kept and
                                              numberOfBasisFull come from the file, the
                                              sweep's other outputs are NaN             */
+    int32_t host_arrays_pageable;         /* drop-in replay: 1 keeps the emulated caller's
+                                             large module arrays (eigenvector, invariant
+                                             matrices, the full stock) in pageable memory,
+                                             as a Fortran allocatable is; 0 in page-locked
+                                             memory                                      */
 } nrg_run_input;
 
 typedef struct nrg_run_output {

@@ -8,6 +8,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <execinfo.h>
+#include <initializer_list>
 #include <signal.h>
 #include <unistd.h>
 #include <unordered_set>
@@ -107,6 +108,28 @@ bool is_device_ptr(const void* p) {
         return false;
     }
     return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
+}
+
+// Every entry point checks its arrays first: device memory must belong to the context's
+// device (the library sets up no peer access, so a kernel reading another GPU's memory
+// would fault); host memory of any kind and managed memory are accepted.
+int reject_foreign(const nrg_context* ctx, const char* who, std::initializer_list<const void*> ptrs) {
+    int k = 0;
+    for (const void* p : ptrs) {
+        ++k;
+        if (!p) continue;
+        cudaPointerAttributes a;
+        if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+            cudaGetLastError();
+            continue;
+        }
+        if (a.type == cudaMemoryTypeDevice && a.device != ctx->device) {
+            nrg_set_error_message("%s: array %d is memory of device %d, the context runs on device %d", who, k,
+                                  a.device, ctx->device);
+            return NRG_ERR_INVALID;
+        }
+    }
+    return NRG_OK;
 }
 
 template <class T>
@@ -428,6 +451,9 @@ int nrg_diagonalization(nrg_context* ctx, int32_t iteration, const nrg_diagonali
     NRG_TRY(need_model(ctx));
     if (!io) return NRG_ERR_INVALID;
     NRG_CUDA_TRY(cudaSetDevice(ctx->device));
+    NRG_TRY(reject_foreign(ctx, "nrg_diagonalization",
+                           {io->subspaceInfo, io->basis_input, io->eigenvalue_old, io->invariant_matrix, io->eigenvalue,
+                            io->eigenvector, io->basis_output, io->groundStateEnergy}));
     const Model& M = ctx->model;
     if (iteration < M.first || iteration > M.nIter) {
         nrg_set_error_message("iteration %d outside [%d, %d]", iteration, M.first, M.nIter);
@@ -509,6 +535,9 @@ static int invmat_common(nrg_context* ctx, int32_t iteration, const nrg_invarian
     NRG_TRY(need_model(ctx));
     if (!io) return NRG_ERR_INVALID;
     NRG_CUDA_TRY(cudaSetDevice(ctx->device));
+    NRG_TRY(reject_foreign(ctx, spec ? "nrg_invariant_matrix_for_spectrum_dgemm" : "nrg_invariant_matrix_dgemm",
+                           {io->subspaceInfo, io->basis_input, io->basis_output, io->eigenvector,
+                            io->invariant_matrix_spectrum_old, io->invariant_matrix}));
     const Model& M = ctx->model;
     (void)iteration;
     if (spec && M.nMat == 0) { nrg_set_error_message("model has no spectrum tables"); return NRG_ERR_STATE; }
@@ -674,6 +703,9 @@ int nrg_reduced_density_matrix(nrg_context* ctx, const nrg_reduced_density_io* i
     NRG_TRY(need_model(ctx));
     if (!io) return NRG_ERR_INVALID;
     NRG_CUDA_TRY(cudaSetDevice(ctx->device));
+    NRG_TRY(reject_foreign(ctx, "nrg_reduced_density_matrix",
+                           {io->mapFullSubspaceInfo, io->fullSubspaceInfo, io->fullBasisInput, io->fullBasisOutput,
+                            io->fullEigenvector, io->reducedDensityMatrix, io->pointReducedDensity, io->trace}));
     const Model& M = ctx->model;
     const int nVar = M.nVar, rsf = nVar + 6, rs = nVar + 3;
     const int nIter = io->numberOfIteration, start = io->startTrancation;
@@ -745,6 +777,11 @@ static int spike_common(nrg_context* ctx, int32_t iteration, const nrg_spike_io*
     NRG_TRY(need_model(ctx));
     if (!io) return NRG_ERR_INVALID;
     NRG_CUDA_TRY(cudaSetDevice(ctx->device));
+    NRG_TRY(reject_foreign(ctx, cfs ? "nrg_spike_cfs" : "nrg_spike_zero_temperature",
+                           {io->subspaceInfo, io->basis_input, io->basis_output, io->eigenvalue, io->eigenvector,
+                            io->invariant_matrix_spectrum, io->fullSubspaceInfo, io->mapFullSubspaceInfo,
+                            io->reducedDensityMatrix, io->binnedSpikePositive, io->binnedSpikeNegative,
+                            io->total_sum}));
     const Model& M = ctx->model;
     if (M.nMat == 0) { nrg_set_error_message("model has no spectrum tables"); return NRG_ERR_STATE; }
     const int nVar = M.nVar, rs = nVar + 3, rsf = nVar + 6;
@@ -903,6 +940,7 @@ int nrg_broaden_log_gaussian(nrg_context* ctx, const double* bins, int32_t numbe
     }
     if (nOmega == 0) return NRG_OK;
     NRG_CUDA_TRY(cudaSetDevice(ctx->device));
+    NRG_TRY(reject_foreign(ctx, "nrg_broaden_log_gaussian", {bins, omega, A}));
     const double *dB = nullptr, *dW = nullptr;
     double* dA = nullptr;
     const size_t nbt = 2 * (size_t)numberOfBin * nMat;

@@ -213,9 +213,12 @@ void sort_basis(std::vector<int>& rec, int n, int nVar) {
     rec.swap(out);
 }
 
-// prepareBasis (prepareBasis.F90:31-114): product basis, sort, sector table
-void prepare_basis_host(const Model& M, const std::vector<int>& bo, int nb_old, std::vector<int>* rec,
-                        std::vector<int>* si) {
+// prepareBasis (prepareBasis.F90:31-114): product basis, sort, sector table.  Returns the
+// count_eigenvector the next sector would get (1 + sum of d^2 over all sectors); a value
+// above 2^31 - 1 means the reference's 32-bit field (module.F90:128) cannot hold the
+// offsets, and the stored offsets are then capped at 2^31 - 1.
+long long prepare_basis_host(const Model& M, const std::vector<int>& bo, int nb_old, std::vector<int>* rec,
+                             std::vector<int>* si) {
     const int nVar = M.nVar, rs = nVar + 3, nOps = M.nOps;
     const int nb = nb_old * nOps;
     rec->assign((size_t)nb * rs, 0);
@@ -246,6 +249,7 @@ void prepare_basis_host(const Model& M, const std::vector<int>& bo, int nb_old, 
             s0 = i;
         }
     }
+    return ce;
 }
 
 // sortWithIndex + truncation + sortByIndex (postprocess.F90:71-140).  E is indexed by
@@ -844,6 +848,7 @@ int run_drop_in(nrg_context* ctx, const nrg_run_input* in, nrg_run_output* out, 
         nrg_set_error_message("restart.dat belongs to the CFS spectrum phase: the run has no spectrum");
         return NRG_ERR_INVALID;
     }
+    ctx->host_pageable = in->host_arrays_pageable != 0;
     if (load) return resume_drop_in(ctx, out, ev, rpath, save);
     if (out && out->thermo)   // thermodynamics are the caller's part of postprocess here
         for (int k = 0; k < 3 * (M.nIter - M.first + 1); ++k) out->thermo[k] = std::nan("");
@@ -884,7 +889,11 @@ int run_drop_in(nrg_context* ctx, const nrg_run_input* in, nrg_run_output* out, 
     for (int it = first; it <= nIter; ++it) {
         const int idx = it - first;
         std::vector<int> bi, si;
-        prepare_basis_host(M, bo, nb_old, &bi, &si);
+        if (prepare_basis_host(M, bo, nb_old, &bi, &si) - 1 > 0x7fffffffLL) {
+            nrg_set_error_message("drop-in replay: iteration %d has more eigenvector entries than the 32-bit "
+                                  "count_eigenvector of subspaceInfo holds", it);
+            return NRG_ERR_TOO_LARGE;
+        }
         const int nb = nb_old * M.nOps;
         const int nsub = (int)(si.size() / rs);
         long long sizeV = 0;
@@ -1076,9 +1085,15 @@ extern "C" int nrg_prepare_basis(int32_t numberOfVariation, int32_t numberOfOper
     M.nChain = numberOfChain;
     M.operation.assign(operation, operation + (size_t)nOps * (nVar + numberOfChain));
     std::vector<int> bo(basis_output, basis_output + (size_t)numberOfBasis_old * rs), rec, si;
-    prepare_basis_host(M, bo, numberOfBasis_old, &rec, &si);
+    const long long ce_end = prepare_basis_host(M, bo, numberOfBasis_old, &rec, &si);
     const int nsub = (int)(si.size() / rs);
     *numberOfSubspace = nsub;
+    if (ce_end - 1 > 0x7fffffffLL) {
+        // the last sector's block would start beyond 2^31 - 1 or end there
+        nrg_set_error_message("nrg_prepare_basis: the eigenvector blocks hold %lld entries, more than the 32-bit "
+                              "count_eigenvector of subspaceInfo addresses", ce_end - 1);
+        return NRG_ERR_TOO_LARGE;
+    }
     if (nsub > subspaceCapacity) {
         nrg_set_error_message("nrg_prepare_basis: %d sectors, subspaceInfo holds %d", nsub, subspaceCapacity);
         return NRG_ERR_INVALID;

@@ -160,6 +160,18 @@ __global__ void __launch_bounds__(kThreads) k_syev(const SyevSector* __restrict_
     const int tid = threadIdx.x, T = blockDim.x;
     double* A = eigbuf + sec.a_off;
     double* ev = evals + sec.e_off;
+    {
+        // a block holding NaN or Inf is reported and left undiagonalised (its eigenvalues
+        // become NaN): the iterations below have fixed bounds, but their results would
+        // be meaningless
+        bool bad = false;
+        for (long long e = tid; e < (long long)n * n; e += T) bad |= !isfinite(A[e]);
+        if (__syncthreads_or(bad)) {
+            if (tid == 0) atomicOr(status, NRG_DEV_NONFINITE);
+            for (int i = tid; i < n; i += T) ev[i] = __longlong_as_double(0x7ff8000000000000LL);
+            return;
+        }
+    }
     if (n == 1) {
         if (tid == 0) { ev[0] = A[0]; A[0] = 1.0; }
         return;

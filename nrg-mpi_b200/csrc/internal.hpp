@@ -26,6 +26,8 @@ struct DevBuf {
 struct HostBuf {
     void* p = nullptr;
     size_t bytes = 0;
+    bool pageable = false;         // the next allocation: plain malloc instead of page-locked
+    bool alloc_pageable = false;   // how p was allocated
     int ensure(size_t want, bool keep = false);
     void release();
     template <class T> T* as() const { return static_cast<T*>(p); }
@@ -148,10 +150,13 @@ struct nrg_context {
         if (store.size() <= i) store.resize(i + 1);
         return store[i];
     }
-    // pinned host arrays of the host-array driver, reused across runs
+    // host module arrays of the host-array driver, reused across runs: page-locked, or
+    // pageable like a Fortran allocatable when host_pageable is set
     std::deque<nrg::HostBuf> host_store;
+    bool host_pageable = false;
     nrg::HostBuf& hslot(size_t i) {
         if (host_store.size() <= i) host_store.resize(i + 1);
+        host_store[i].pageable = host_pageable;
         return host_store[i];
     }
     ~nrg_context();

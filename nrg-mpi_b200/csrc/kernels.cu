@@ -18,7 +18,7 @@ struct AsmParams {
     double cbcs[kMaxChain];    // chain_BCS(iteration+1, c)
 };
 
-// Block Hamiltonian of diagonalization.F90:272-381.  One block per column of one sector.
+// Block Hamiltonian of diagonalization.F90:162-262.  One block per column of one sector.
 // Products are rounded one at a time (no fused multiply-add) in the reference's order.
 __global__ void k_assemble(const SyevSector* __restrict__ secs, const long long* __restrict__ colPrefix,
                            const int* __restrict__ secStart, const int* __restrict__ bi,
@@ -41,40 +41,55 @@ __global__ void k_assemble(const SyevSector* __restrict__ secs, const long long*
     const int row0 = secStart[s];
     const int R = P.rec;
     const size_t nbo = (size_t)P.nb_old;
+    // An entry whose indices fall outside their tables, or whose value is NaN or Inf (from
+    // the previous eigenvalues, invariant matrices or chain), is reported in the status
+    // word and stored as 0: the eigensolver then runs on a finite matrix (its result is
+    // discarded by the caller, which reads the status).  The reference passes such input
+    // to dsyev unchecked.
     for (int i = threadIdx.x; i < d; i += blockDim.x) {
-        double v;
+        double v = 0.0;
+        int bad = 0;
         if (i == j) {
             const int* r = bi + (size_t)(row0 + i) * R;
             const int op = r[P.nVar + 2] - 1, ref = r[P.nVar] - 1;
-            if (ref < 0 || ref >= P.nb_old || op < 0 || op >= P.nOps) { atomicOr(status, NRG_DEV_BAD_INDEX); continue; }
-            v = __dmul_rn(Eold[ref], P.sqrtL);
-            for (int c = 0; c < P.nChain; ++c)
-                v = __dadd_rn(v, __dmul_rn((double)operation[op + (size_t)(P.nVar + c) * P.nOps], P.cdiag[c]));
+            if (ref < 0 || ref >= P.nb_old || op < 0 || op >= P.nOps) {
+                bad = NRG_DEV_BAD_INDEX;
+            } else {
+                v = __dmul_rn(Eold[ref], P.sqrtL);
+                for (int c = 0; c < P.nChain; ++c)
+                    v = __dadd_rn(v, __dmul_rn((double)operation[op + (size_t)(P.nVar + c) * P.nOps], P.cdiag[c]));
+            }
         } else {
             const int p = i < j ? i : j, q = i < j ? j : i;
             const int* rp = bi + (size_t)(row0 + p) * R;
             const int* rq = bi + (size_t)(row0 + q) * R;
             const int a = rp[P.nVar + 2] - 1, b = rq[P.nVar + 2] - 1;
             const int refp = rp[P.nVar] - 1, refq = rq[P.nVar] - 1;
-            if (a < 0 || a >= P.nOps || b < 0 || b >= P.nOps) { atomicOr(status, NRG_DEV_BAD_INDEX); continue; }
-            const int idx = a * P.nOps + b;
-            const bool sw = dswp[idx] != 0;
-            const int ir = sw ? refq : refp, jr = sw ? refp : refq;
-            v = 0.0;
-            if (dflag[idx]) {
-                const int t = dtype[idx] - 1, ch = dch[idx] - 1;
-                if (ir < 0 || jr < 0 || ir >= P.nb_old || jr >= P.nb_old || t < 0 || t >= P.nCM ||
-                    ch < 0 || ch >= P.nChain) {
-                    atomicOr(status, NRG_DEV_BAD_INDEX);
-                    continue;
+            if (a < 0 || a >= P.nOps || b < 0 || b >= P.nOps) {
+                bad = NRG_DEV_BAD_INDEX;
+            } else {
+                const int idx = a * P.nOps + b;
+                const bool sw = dswp[idx] != 0;
+                const int ir = sw ? refq : refp, jr = sw ? refp : refq;
+                if (dflag[idx]) {
+                    const int t = dtype[idx] - 1, ch = dch[idx] - 1;
+                    if (ir < 0 || jr < 0 || ir >= P.nb_old || jr >= P.nb_old || t < 0 || t >= P.nCM ||
+                        ch < 0 || ch >= P.nChain)
+                        bad = NRG_DEV_BAD_INDEX;
+                    else
+                        v = __dmul_rn(__dmul_rn(P.cnond[ch], dcoef[idx]),
+                                      IMold[(size_t)jr + (size_t)ir * nbo + (size_t)t * nbo * nbo]);
                 }
-                v = __dmul_rn(__dmul_rn(P.cnond[ch], dcoef[idx]),
-                              IMold[(size_t)jr + (size_t)ir * nbo + (size_t)t * nbo * nbo]);
+                if (!bad && P.flag_BCS && bflag[idx] && ir == jr) {
+                    const int ch = bch[idx] - 1;
+                    if (ch >= 0 && ch < P.nChain) v = P.cbcs[ch];
+                }
             }
-            if (P.flag_BCS && bflag[idx] && ir == jr) {
-                const int ch = bch[idx] - 1;
-                if (ch >= 0 && ch < P.nChain) v = P.cbcs[ch];
-            }
+        }
+        if (!bad && !isfinite(v)) bad = NRG_DEV_NONFINITE;
+        if (bad) {
+            atomicOr(status, bad);
+            v = 0.0;
         }
         V[sec.a_off + (size_t)i + (size_t)j * d] = v;
     }
@@ -96,7 +111,7 @@ __global__ void k_min(const double* __restrict__ E, int n, double* out) {
     }
 }
 
-// diagonalization.F90:472-475
+// diagonalization.F90:353-356
 __global__ void k_shift(double* __restrict__ E, int n, const double* __restrict__ mn) {
     const double m = mn[0];
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
@@ -106,7 +121,7 @@ __global__ void k_shift(double* __restrict__ E, int n, const double* __restrict_
     }
 }
 
-// diagonalization.F90:392-399
+// diagonalization.F90:273-280
 __global__ void k_chop(double* __restrict__ V, long long n) {
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
         if (fabs(V[i]) < 1.0e-14) V[i] = 0.0;

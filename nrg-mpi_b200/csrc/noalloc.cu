@@ -4,6 +4,8 @@
 // held until the process exits); the call itself allocates nothing.
 #include "common.cuh"
 
+#include <cuda.h>   // CUcontext and CUresult only: driver calls go through cudaGetDriverEntryPoint
+
 #include <mutex>
 
 namespace {
@@ -28,32 +30,79 @@ namespace {
 
 constexpr int kMaxDevices = 64;
 std::mutex g_mu;
-double* g_scratch_ptr[kMaxDevices] = {nullptr};
 
-// device address of the static array on the current device (set up once per device)
+// The array's device address, looked up once per device and CUDA context.  The address
+// belongs to the context the library's device code was loaded into: after the application
+// resets the device (cudaDeviceReset) a new primary context loads the module again, and
+// the old address is stale.  The context is told apart by its process-unique id
+// (cuCtxGetId, through the runtime's driver entry points: no link against libcuda).
+struct ScratchEntry {
+    unsigned long long ctx_id;   // 0: unknown, look up again on the next call
+    double* ptr;
+};
+ScratchEntry g_scratch[kMaxDevices] = {};
+
+typedef CUresult (*CtxGetCurrentFn)(CUcontext*);
+typedef CUresult (*CtxGetIdFn)(CUcontext, unsigned long long*);
+
+// id of the calling thread's current context; 0 when there is none or it cannot be told
+unsigned long long current_context_id() {
+    static CtxGetCurrentFn get_current = nullptr;
+    static CtxGetIdFn get_id = nullptr;
+    static bool resolved = false;
+    if (!resolved) {   // under g_mu
+        resolved = true;
+        void* f = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            get_current = reinterpret_cast<CtxGetCurrentFn>(f);
+        f = nullptr;
+        if (cudaGetDriverEntryPoint("cuCtxGetId", &f, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            get_id = reinterpret_cast<CtxGetIdFn>(f);
+        cudaGetLastError();
+    }
+    if (!get_current || !get_id) return 0;
+    CUcontext c = nullptr;
+    unsigned long long id = 0;
+    if (get_current(&c) != CUDA_SUCCESS || !c || get_id(c, &id) != CUDA_SUCCESS) return 0;
+    return id;
+}
+
+// device address of the static array on the current device
 int scratch_address(int device, double** out) {
     std::lock_guard<std::mutex> lk(g_mu);
     if (device < 0 || device >= kMaxDevices) return NRG_ERR_DEVICE;
-    if (!g_scratch_ptr[device]) {
-        void* p = nullptr;
-        const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-        if (e != cudaSuccess) {
-            nrg_set_error_message("cudaGetSymbolAddress of the static workspace failed: %s", cudaGetErrorString(e));
-            return NRG_ERR_CUDA;
-        }
-        g_scratch_ptr[device] = static_cast<double*>(p);
+    ScratchEntry& e = g_scratch[device];
+    unsigned long long id = current_context_id();
+    if (e.ptr && id != 0 && id == e.ctx_id) {
+        *out = e.ptr;
+        return NRG_OK;
     }
-    *out = g_scratch_ptr[device];
+    void* p = nullptr;
+    const cudaError_t err = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (err != cudaSuccess) {
+        nrg_set_error_message("cudaGetSymbolAddress of the static workspace failed: %s", cudaGetErrorString(err));
+        return NRG_ERR_CUDA;
+    }
+    if (id == 0) id = current_context_id();   // the lookup made the primary context current
+    e.ptr = static_cast<double*>(p);
+    e.ctx_id = id;
+    *out = e.ptr;
     return NRG_OK;
 }
 
-bool on_device(const void* p) {
+// memory this device's kernels may read and write: device memory of the current device,
+// or managed memory; a device pointer of another GPU is refused (no peer access is set up)
+bool on_device(const void* p, int device) {
     cudaPointerAttributes a;
     if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
         cudaGetLastError();
         return false;
     }
-    return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
+    if (a.type == cudaMemoryTypeManaged) return true;
+    return a.type == cudaMemoryTypeDevice && a.device == device;
 }
 
 }  // namespace
@@ -65,13 +114,14 @@ extern "C" int nrg_block_eigh_noalloc(const double* H, int32_t n, double* eigenv
                               n, kMaxN);
         return NRG_ERR_TOO_LARGE;
     }
-    if (!H || !eigenvalues || !eigenvectors || !on_device(H) || !on_device(eigenvalues) ||
-        !on_device(eigenvectors)) {
-        nrg_set_error_message("nrg_block_eigh_noalloc: H, eigenvalues and eigenvectors must be device arrays");
-        return NRG_ERR_INVALID;
-    }
     int device = 0;
     NRG_CUDA_TRY(cudaGetDevice(&device));
+    if (!H || !eigenvalues || !eigenvectors || !on_device(H, device) || !on_device(eigenvalues, device) ||
+        !on_device(eigenvectors, device)) {
+        nrg_set_error_message("nrg_block_eigh_noalloc: H, eigenvalues and eigenvectors must be device arrays "
+                              "of the current device (%d) or managed memory", device);
+        return NRG_ERR_INVALID;
+    }
     double* base = nullptr;
     NRG_TRY(scratch_address(device, &base));
     cudaStream_t st = static_cast<cudaStream_t>(stream);

@@ -7,6 +7,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 #include <numeric>
 #include <unordered_set>
@@ -39,24 +40,36 @@ void DevBuf::release() {
 }
 
 int HostBuf::ensure(size_t want, bool keep) {
-    if (want <= bytes && p) return NRG_OK;
+    if (want <= bytes && p && alloc_pageable == pageable) return NRG_OK;
     size_t sz = want < 4096 ? 4096 : want;
     if (keep) sz = std::max(sz, bytes + bytes / 2);
     sz = (sz + 4095) & ~size_t(4095);
     void* q = nullptr;
-    cudaError_t e = cudaHostAlloc(&q, sz, cudaHostAllocPortable);
-    if (e != cudaSuccess) {
-        nrg_set_error_message("cudaHostAlloc(%zu) failed: %s", sz, cudaGetErrorString(e));
-        return NRG_ERR_NOMEM;
+    if (pageable) {
+        q = std::malloc(sz);
+        if (!q) {
+            nrg_set_error_message("malloc(%zu) failed", sz);
+            return NRG_ERR_NOMEM;
+        }
+    } else {
+        cudaError_t e = cudaHostAlloc(&q, sz, cudaHostAllocPortable);
+        if (e != cudaSuccess) {
+            nrg_set_error_message("cudaHostAlloc(%zu) failed: %s", sz, cudaGetErrorString(e));
+            return NRG_ERR_NOMEM;
+        }
     }
-    if (keep && p && bytes) std::memcpy(q, p, bytes);
-    if (p) cudaFreeHost(p);
+    if (keep && p && bytes) std::memcpy(q, p, std::min(bytes, sz));
+    release();
     p = q;
     bytes = sz;
+    alloc_pageable = pageable;
     return NRG_OK;
 }
 void HostBuf::release() {
-    if (p) cudaFreeHost(p);
+    if (p) {
+        if (alloc_pageable) std::free(p);
+        else cudaFreeHost(p);
+    }
     p = nullptr;
     bytes = 0;
 }
@@ -277,14 +290,15 @@ int check_device_status(nrg_context* ctx) {
     NRG_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
     if (st != 0) {
         NRG_CUDA_TRY(cudaMemsetAsync(ctx->d_status.p, 0, sizeof(int), ctx->stream));
-        nrg_set_error_message("device status flags 0x%x (1: index out of range, 4: secular root)", st);
-        return (st & NRG_DEV_SECULAR) ? NRG_ERR_NUMERIC : NRG_ERR_INVALID;
+        nrg_set_error_message("device status flags 0x%x (1: index out of range, 4: secular root, 8: NaN or Inf "
+                              "in a block)", st);
+        return (st & (NRG_DEV_SECULAR | NRG_DEV_NONFINITE)) ? NRG_ERR_NUMERIC : NRG_ERR_INVALID;
     }
     return NRG_OK;
 }
 
 // ------------------------------------------------------------------------------------
-// diagonalization (diagonalization.F90:185-528)
+// diagonalization (diagonalization.F90:1-410)
 // ------------------------------------------------------------------------------------
 int diag_device(nrg_context* ctx, int iteration, Sectors& S, const double* d_Eold, int nb_old,
                 const double* d_IMold, double* d_V, double* d_E, DiagOut* out, double* h_E) {

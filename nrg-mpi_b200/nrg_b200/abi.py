@@ -127,6 +127,7 @@ class RunInput(ctypes.Structure):
         ("invariant_matrix", _pf64), ("invariant_matrix_spectrum", _pf64),
         ("spectrum", c_int32), ("host_drop_in", c_int32), ("temperature", c_double),
         ("restart_file", ctypes.c_char_p), ("save_restart", c_int32), ("load_restart", c_int32),
+        ("host_arrays_pageable", c_int32),
     ]
 
 
@@ -501,7 +502,7 @@ class Context:
     # ------------------------------------------------------------------
     def run(self, spectrum: bool = True, flow_stride: int = 8, final_capacity: int = 0,
             host_drop_in: bool = False, temperature: float = 0.0, restart_file: Optional[str] = None,
-            save_restart: bool = False, load_restart: bool = False):
+            save_restart: bool = False, load_restart: bool = False, host_pageable: bool = False):
         """main.F90:142-252; returns bins and per-iteration statistics.
 
         ``host_drop_in=True`` drives every routine through its drop-in entry point with
@@ -512,14 +513,16 @@ class Context:
         reference's param%saveRestart / param%loadRestart: the file (``restart_file``,
         default "restart.dat") is rewritten before every CFS step, or the run resumes the
         CFS loop from it (module.F90:1710-1890, main.F90:165-224).
+        ``host_pageable=True`` (drop-in replay) keeps the emulated caller's large module
+        arrays in pageable memory, as a Fortran allocatable is, instead of page-locked memory.
         """
         args = self._run_args(spectrum, flow_stride, final_capacity, host_drop_in, temperature,
-                              restart_file, save_restart, load_restart)
+                              restart_file, save_restart, load_restart, host_pageable)
         self._check(self.lib.nrg_run(self._h, ctypes.byref(args["ri"]), ctypes.byref(args["ro"])), "nrg_run")
         return self._run_result(args)
 
     def _run_args(self, spectrum, flow_stride, final_capacity, host_drop_in, temperature=0.0,
-                  restart_file=None, save_restart=False, load_restart=False):
+                  restart_file=None, save_restart=False, load_restart=False, host_pageable=False):
         """Input and output records of nrg_run for this context (arrays kept alive here)."""
         inp = self.inp
         nb = inp.numberOfBasis
@@ -529,7 +532,8 @@ class Context:
                  path=os.fsencode(restart_file) if restart_file else None)
         a["ri"] = RunInput(nb, _p(a["bo"], c_int32), _p(a["E"], c_double), _p(a["im"], c_double),
                            _p(a["ims"], c_double), int(bool(spectrum)), int(bool(host_drop_in)),
-                           float(temperature), a["path"], int(bool(save_restart)), int(bool(load_restart)))
+                           float(temperature), a["path"], int(bool(save_restart)), int(bool(load_restart)),
+                           int(bool(host_pageable)))
         nit = inp.numberOfIteration - inp.indexOfFirstIteration + 1
         nmat = max(inp.numberOfMatrix, 1)
         nbin_cap = 20001

@@ -380,10 +380,10 @@ def prepare_basis(st: State, iteration: int) -> None:
 
 
 # ------------------------------------------------------------------------------------
-# diagonalization (diagonalization.F90:185-528)
+# diagonalization (diagonalization.F90:1-410)
 # ------------------------------------------------------------------------------------
 def assemble_block(st: State, iteration: int, isub: int, tables=None) -> np.ndarray:
-    """Sector Hamiltonian of diagonalization.F90:272-381 (full symmetric matrix)."""
+    """Sector Hamiltonian of diagonalization.F90:162-262 (full symmetric matrix)."""
     nVar = st.nVar
     if tables is None:
         tables = (diag_coef_table(st), bcs_table(st))
@@ -433,19 +433,19 @@ def diagonalization(st: State, iteration: int) -> None:
     for isub in range(st.numberOfSubspace):
         d = int(dims[isub])
         H = assemble_block(st, iteration, isub, tables)
-        w, V = scipy.linalg.eigh(H, lower=False, driver="ev", check_finite=False)  # :386
-        V[np.abs(V) < EIGENVECTOR_THRESHOLD] = 0.0                        # :392-399
+        w, V = scipy.linalg.eigh(H, lower=False, driver="ev", check_finite=False)  # :267
+        V[np.abs(V) < EIGENVECTOR_THRESHOLD] = 0.0                        # :273-280
         s0 = int(st.subspaceInfo[isub, nVar + 2]) - 1
         c0 = int(st.subspaceInfo[isub, nVar + 1]) - 1
         E[s0:s0 + d] = w
         ev[c0:c0 + d * d] = V.ravel(order="F")
-    st.ground_state_energy[iteration] = float(E[0])                       # :470
+    st.ground_state_energy[iteration] = float(E[0])                       # :351
     st.emin[iteration] = float(np.min(E))
-    E = E - np.min(E)                                                    # :472
-    E[E <= NUMERICAL_THRESHOLD] = 0.0                                     # :473-475
+    E = E - np.min(E)                                                    # :353
+    E[E <= NUMERICAL_THRESHOLD] = 0.0                                     # :354-356
     st.eigenvalue = E
     st.eigenvector = ev
-    bo = np.zeros((st.nb, nVar + 3), dtype=np.int32)                      # :514-526
+    bo = np.zeros((st.nb, nVar + 3), dtype=np.int32)                      # :394-407
     for isub in range(st.numberOfSubspace):
         d = int(dims[isub])
         s0 = int(st.subspaceInfo[isub, nVar + 2]) - 1

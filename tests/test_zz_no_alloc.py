@@ -6,13 +6,17 @@ calls it through the C ABI on device arrays the test owns, twice in a row (the s
 workspace keeps the previous call's contents), and checks each result against the
 existing entry point nrg_diagonalization on the same sector Hamiltonian, within the
 tolerances of the other parity tests (eigenvalues 1e-12 relative, eigenvector
-projectors 1e-9).  This file is collected last so a failure here comes after every other
-test has run.
+projectors 1e-9), and with the oracle's LAPACK dsyev on the same blocks.  A second test
+covers the edges: orders 1 and the static limit, the in-place call, a block holding NaN,
+orders beyond the limit and host arrays (rejected), and that repeated calls leave the
+device's free memory unchanged.  This file is collected last so a failure here comes after
+every other test has run.
 """
 import ctypes
 
 import numpy as np
 import pytest
+import scipy.linalg
 
 from oracle import nrg_oracle as O
 from nrg_b200 import model, load_library
@@ -59,28 +63,87 @@ def _sectors(ctx_factory):
     raise AssertionError("no suitable sector")
 
 
-def test_block_eigh_noalloc_matches_diagonalization(ctx_factory):
-    torch = pytest.importorskip("torch")
+def _entry():
     lib = load_library()
     fn = lib.nrg_block_eigh_noalloc
     fn.argtypes = [ctypes.c_void_p, ctypes.c_int32, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
     fn.restype = ctypes.c_int
+    return lib, fn
+
+
+def _solve(fn, torch, H, in_place=False):
+    """One call on device copies of H; returns (status, eigenvalues, eigenvectors)."""
+    n = H.shape[0]
+    dev = torch.device("cuda", 0)
+    dH = torch.tensor(np.asfortranarray(H).ravel(order="F"), dtype=torch.float64, device=dev)
+    dw = torch.zeros(n, dtype=torch.float64, device=dev)
+    dV = dH if in_place else torch.zeros(n * n, dtype=torch.float64, device=dev)
+    rc = fn(dH.data_ptr(), n, dw.data_ptr(), dV.data_ptr(), None)
+    return rc, dw.cpu().numpy(), dV.cpu().numpy().reshape((n, n), order="F")
+
+
+def _check(H, w, V, w_ref, V_ref):
+    assert eig_rel_err(w, w_ref) <= 1e-12
+    assert subspace_err(V, V_ref, w) <= 1e-9
+    assert np.allclose(H @ V, V * w, atol=1e-12 * max(1.0, np.max(np.abs(w))))
+
+
+def test_block_eigh_noalloc_matches_diagonalization(ctx_factory):
+    torch = pytest.importorskip("torch")
+    lib, fn = _entry()
     cases = _sectors(ctx_factory)
     assert len(cases) == 2
-    dev = torch.device("cuda", 0)
     for H, E_ref, V_ref in cases:            # two calls in a row, different orders
-        n = H.shape[0]
-        dH = torch.tensor(np.asfortranarray(H).ravel(order="F"), dtype=torch.float64, device=dev)
-        dw = torch.zeros(n, dtype=torch.float64, device=dev)
-        dV = torch.zeros(n * n, dtype=torch.float64, device=dev)
-        rc = fn(dH.data_ptr(), n, dw.data_ptr(), dV.data_ptr(), None)
+        rc, w, V = _solve(fn, torch, H)
         assert rc == 0, lib.nrg_last_error()
-        w = dw.cpu().numpy()
-        V = dV.cpu().numpy().reshape((n, n), order="F")
-        V[np.abs(V) < 1e-14] = 0.0       # nrg_diagonalization chops (diagonalization.F90:392-399)
-        assert eig_rel_err(w, E_ref) <= 1e-12
-        assert subspace_err(V, V_ref, w) <= 1e-9
-        assert np.allclose(H @ V, V * w, atol=1e-12 * max(1.0, np.max(np.abs(w))))
-    # orders beyond the static workspace are rejected without touching the device arrays
-    rc = fn(dH.data_ptr(), MAX_ORDER + 1, dw.data_ptr(), dV.data_ptr(), None)
-    assert rc == 4
+        V[np.abs(V) < 1e-14] = 0.0       # nrg_diagonalization chops (diagonalization.F90:273-280)
+        _check(H, w, V, E_ref, V_ref)
+        # and the oracle's dsyev('V', 'U') on the same block
+        w_o, V_o = scipy.linalg.eigh(H, lower=False, driver="ev")
+        _check(H, w, V, w_o, V_o)
+
+
+def test_block_eigh_noalloc_edges():
+    torch = pytest.importorskip("torch")
+    lib, fn = _entry()
+    rng = np.random.default_rng(20261204)
+    for n in (1, 2, 127, MAX_ORDER):        # the one-element path, and the static limit itself
+        A = rng.standard_normal((n, n))
+        H = 0.5 * (A + A.T)
+        w_o, V_o = np.linalg.eigh(H)
+        rc, w, V = _solve(fn, torch, H)
+        assert rc == 0, lib.nrg_last_error()
+        _check(H, w, V, w_o, V_o)
+    # in place: the eigenvectors overwrite H
+    A = rng.standard_normal((96, 96))
+    H = 0.5 * (A + A.T)
+    rc, w, V = _solve(fn, torch, H, in_place=True)
+    assert rc == 0, lib.nrg_last_error()
+    w_o, V_o = np.linalg.eigh(H)
+    _check(H, w, V, w_o, V_o)
+    # a block with a NaN is reported, and the next call works again
+    Hn = H.copy()
+    Hn[3, 5] = Hn[5, 3] = np.nan
+    rc, _, _ = _solve(fn, torch, Hn)
+    assert rc == 8, lib.nrg_last_error()                # NRG_ERR_NUMERIC
+    rc, w, V = _solve(fn, torch, H)
+    assert rc == 0, lib.nrg_last_error()
+    _check(H, w, V, w_o, V_o)
+    # orders beyond the static workspace, and host arrays, are rejected without a launch
+    dev = torch.device("cuda", 0)
+    d = torch.zeros((MAX_ORDER + 1) ** 2, dtype=torch.float64, device=dev)
+    assert fn(d.data_ptr(), MAX_ORDER + 1, d.data_ptr(), d.data_ptr(), None) == 4   # NRG_ERR_TOO_LARGE
+    h = np.zeros(16)
+    assert fn(h.ctypes.data, 4, d.data_ptr(), d.data_ptr(), None) == 1              # NRG_ERR_INVALID
+    # the call allocates nothing: the device's free memory is the same after two more calls
+    torch.cuda.synchronize()
+    free0 = torch.cuda.mem_get_info(0)[0]
+    dH = torch.tensor(np.asfortranarray(H).ravel(order="F"), dtype=torch.float64, device=dev)
+    dw = torch.zeros(96, dtype=torch.float64, device=dev)
+    dV = torch.zeros(96 * 96, dtype=torch.float64, device=dev)
+    torch.cuda.synchronize()
+    free1 = torch.cuda.mem_get_info(0)[0]
+    for _ in range(2):
+        assert fn(dH.data_ptr(), 96, dw.data_ptr(), dV.data_ptr(), None) == 0
+    torch.cuda.synchronize()
+    assert torch.cuda.mem_get_info(0)[0] == free1, (free0, free1)
