@@ -7,11 +7,11 @@ library's whole runs with these files instead of re-running the oracle at full s
 Workloads (``nrg_b200.model.config``):
 
 * ``siam_nkeep2048.npz``  SIAM Lambda=2.0 U=0.2 Gamma=0.02 eps_d=-0.1, N_keep=2048, all 60
-  iterations, backward reduced density matrices and the T = 0 CFS spectrum;
+  iterations (-1..58), backward reduced density matrices and the T = 0 CFS spectrum;
 * ``siam_nkeep4096_n14.npz`` SIAM Lambda=2.0 U=0.3 Gamma=0.03 eps_d=-0.15, N_keep=4096, a
-  window of the chain: iterations -1..14 (the model cut at 14 sites, so iteration 14 is
-  the last one: no truncation there, the density matrices start from its ground states)
-  with the spectrum over that window.
+  window of the chain: its first 14 iterations, -1..12 (the model cut there, so iteration
+  12 is the last one: no truncation there, the density matrices start from its ground
+  states), with the spectrum over that window.
 
 Stored per iteration: the kept count, the number of states before truncation, the
 ground-state energy (eigenvalue(1) before the shift), the lowest ``FLOW`` kept energies

@@ -7,7 +7,8 @@ density-matrix trace of every backward step, and the nonzero spectral bins:
 
 * the N_keep = 2048 SIAM workload, all 60 iterations with density matrices and the T = 0
   CFS spectrum (the second bench object);
-* the N_keep = 4096 SIAM workload (the bench headline's model) cut at iteration 14.
+* the N_keep = 4096 SIAM workload (the bench headline's model), its first 14 iterations
+  (-1..12), the model cut there.
 
 Both the device-resident run and the drop-in replay (every routine through its entry point
 with host arrays) are compared.  Tolerances: kept counts and state counts equal (the
