@@ -525,6 +525,349 @@ __global__ void __launch_bounds__(TT, 1) k_tri_cluster(const LSec* __restrict__ 
     cluster.sync();   // no block leaves while another may still write its shared memory
 }
 
+// ---------------------------------------------------------------------------------
+// the same cluster tridiagonalisation on the lower triangle only
+// ---------------------------------------------------------------------------------
+// k_tri_cluster streams every own column of the trailing matrix in full for each column
+// step's product y = A v, and updates full columns after each panel.  The matrix is
+// symmetric, so this variant keeps and reads only the lower triangle: the product of own
+// column l takes rows i >= l,
+//   y(l) += sum_{i >= l} A(i, l) v(i)        (the column's own dot product)
+//   z(i) += A(i, l) v(l)       for i > l     (row i's share of A(i, :) v, i.e. the upper
+//                                             triangle read as the transpose)
+// and every block sends the z of each row to the block that owns the row, in the same
+// cluster exchange that carries the panel dot products; y(l) = dot(l) + the received z.
+// Half the bytes of the product and of the panel update cross from L2.  The panel rows of
+// column p+q (needed as own rows of the column) are read from the column itself (rows at
+// stride CL), since the upper triangle is stale.  The product is split into work items of
+// 256 rows x CRW own columns; each item leaves its column dot products in ysp (per row
+// batch) and its row sums in zsp (per column range), and both are added in a fixed order,
+// so results do not depend on the schedule.
+constexpr int SRB = 256;   // rows per work item of the symmetric product
+
+struct TriLayoutS {
+    int MM, PN, NRB, NCR, CRW;   // own indices per block, rows (even), row batches, column ranges
+    __host__ __device__ long long doubles(int CL) const {
+        const long long stage = (long long)NB * MM > 2LL * NB * 64 ? (long long)NB * MM : 2LL * NB * 64;
+        return 2LL * NB * MM + PN + MM + (long long)CL * P2W + CL + 2 + 2LL * NB + 2LL * NB + P2W + 32 +
+               stage + (long long)NRB * MM + (long long)NCR * PN + (long long)CL * MM + 3LL * NB;
+    }
+};
+
+template <int CL>
+__global__ void __launch_bounds__(TT, 1) k_tri_csym(const LSec* __restrict__ secs, TriLayoutS lay,
+                                                   double* eigbuf, double* wsd, int* wsi) {
+    constexpr int TRS = 64;   // rows per staged chunk of the panel update
+    extern __shared__ double sm[];
+    cg::cluster_group cluster = cg::this_cluster();
+    const int rank = (int)cluster.block_rank();
+    const LSec sec = secs[blockIdx.x / CL];
+    LView L = lview(sec, eigbuf, wsd, wsi);
+    const int n = L.n, MM = lay.MM, PN = lay.PN, CRW = lay.CRW;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    constexpr int NW = TT / 32;
+    double* VO = sm;                       // NB x MM: V(own row m, q) at q*MM + m
+    double* WO = VO + (size_t)NB * MM;     // NB x MM
+    double* cv = WO + (size_t)NB * MM;     // column k (rows > k), then v, by row
+    double* ys = cv + PN;                  // y of the own columns
+    double* P2 = ys + MM;                  // CL x P2W partials, by source block
+    double* redA = P2 + CL * P2W;          // CL partial |x|^2
+    double* Y1 = redA + CL;                // y(k+1) from its owner
+    double* pivn = Y1 + 2;                 // 2 NB: V(k+1, q) | W(k+1, q) from its owner
+    double* piv = pivn + 2 * NB;           // 2 NB: W(k, q) | V(k, q) of the current pivot row
+    double* tsum = piv + 2 * NB;           // t1 | t2 | y.v
+    double* red = tsum + P2W;              // 32
+    double* AR = red + 32;                 // NB x MM: A(own row m, p + q), during the columns
+    double* stV = AR;                      // NB x TRS staged rows of V (transposed), panel update
+    double* stW = stV + NB * TRS;          // NB x TRS
+    double* ysp = AR + ((size_t)NB * MM > 2 * NB * TRS ? (size_t)NB * MM : 2 * NB * TRS);   // NRB x MM
+    double* zsp = ysp + (size_t)lay.NRB * MM;   // NCR x PN row sums per column range
+    double* zr = zsp + (size_t)lay.NCR * PN;    // CL x MM: z of the own rows, by source block
+    double* pan = zr + (size_t)CL * MM;         // D | E | tau of the panel's columns
+    double* Vg = L.VW;
+    double* Wg = L.VW + (size_t)NB * n;
+    double* A = L.A;
+    const int cnt = (n - rank + CL - 1) / CL;                           // own indices rank + CL*m
+    auto first_own = [&](int i0) { return (i0 - rank + CL - 1) / CL; };  // i0 >= 0
+
+    for (int p = 0; p < n - 1; p += NB) {
+        const int last = min(p + NB - 1, n - 2);
+        const int jn = last - p + 1;
+        // own rows i >= p + q of the panel's columns p + q (lower triangle, stride CL)
+        for (int q = 0; q < jn; ++q) {
+            const int m0 = first_own(p + q);
+            for (int m = m0 + tid; m < cnt; m += TT)
+                AR[q * MM + m] = __ldcg(A + (size_t)(rank + CL * m) + (size_t)(p + q) * n);
+        }
+        __syncthreads();
+        for (int k = p; k <= last; ++k) {
+            const int j = k - p;
+            // ---- A: own rows of column k, broadcast ----
+            const int m = first_own(k) + tid;
+            const bool act = m < cnt;
+            const int i = rank + CL * m;
+            double c = 0.0, ss = 0.0;
+            if (act) {
+                double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
+                int q = 0;
+                for (; q + 1 < j; q += 2) {
+                    s0 = fma(VO[q * MM + m], piv[q], s0);
+                    s1 = fma(WO[q * MM + m], piv[NB + q], s1);
+                    s2 = fma(VO[(q + 1) * MM + m], piv[q + 1], s2);
+                    s3 = fma(WO[(q + 1) * MM + m], piv[NB + q + 1], s3);
+                }
+                if (q < j) {
+                    s0 = fma(VO[q * MM + m], piv[q], s0);
+                    s1 = fma(WO[q * MM + m], piv[NB + q], s1);
+                }
+                c = AR[j * MM + m] - ((s0 + s2) + (s1 + s3));
+                if (i == k) pan[j] = c;
+                if (i >= k + 2) ss = c * c;
+                if (i >= k + 1)
+                    for (int r = 0; r < CL; ++r) cluster.map_shared_rank(cv, r)[i] = c;
+            }
+            const double ssb = block_sum(ss, red);
+            if (tid < CL) cluster.map_shared_rank(redA, tid)[rank] = ssb;
+            cluster.sync();
+            double xn2 = 0.0;
+            for (int r = 0; r < CL; ++r) xn2 += redA[r];
+            const double alpha = cv[k + 1];
+            double beta = alpha, tau = 0.0, scal = 0.0;
+            if (xn2 != 0.0) {
+                beta = -copysign(sqrt(alpha * alpha + xn2), alpha);
+                tau = (beta - alpha) / beta;
+                scal = 1.0 / (alpha - beta);
+            }
+            for (int r = k + 2 + tid; r < n; r += TT) cv[r] = xn2 == 0.0 ? 0.0 : cv[r] * scal;
+            if (act && i >= k + 1) VO[j * MM + m] = (i == k + 1) ? 1.0 : (xn2 == 0.0 ? 0.0 : c * scal);
+            if (tid == 0) { pan[NB + j] = beta; pan[2 * NB + j] = tau; }
+            __syncthreads();
+            // ---- B: partial W^T v, V^T v over the own rows, the next pivot row, the
+            // lower-triangle product, z to the row owners, partial y.v ----
+            const int mB = first_own(k + 1);
+            const double* vj = VO + j * MM;
+            for (int o = warp; o < 2 * j; o += NW) {
+                const double* colp = (o < j) ? WO + o * MM : VO + (o - j) * MM;
+                double s = 0.0;
+                for (int mm = mB + lane; mm < cnt; mm += 32) s = fma(colp[mm], vj[mm], s);
+                s = warp_sum(s);
+                if (lane < CL) cluster.map_shared_rank(P2, lane)[rank * P2W + (o < j ? o : NB + (o - j))] = s;
+            }
+            const bool pivot_owner = (rank == (k + 1) % CL);
+            if (pivot_owner && k + 1 <= last) {
+                for (int e = tid; e < 2 * j * CL; e += TT) {
+                    const int q = e / CL, r = e % CL;
+                    const double val = q < j ? VO[q * MM + mB] : WO[(q - j) * MM + mB];
+                    cluster.map_shared_rank(pivn, r)[q < j ? q : NB + (q - j)] = val;
+                }
+            }
+            const int nrows = n - k - 1;
+            const int nrb = (nrows + SRB - 1) / SRB;
+            const int ncr = (cnt - mB + CRW - 1) / CRW;
+            // an item (row batch rb, column range cr) holds work when the range's first
+            // column is not below the batch's last row
+            auto item_live = [&](int rb, int cr) {
+                const int lastrow = min(k + 1 + (rb + 1) * SRB, n) - 1;
+                return rank + CL * (mB + cr * CRW) <= lastrow;
+            };
+            for (int item = warp; item < nrb * ncr; item += NW) {
+                const int rb = item / ncr, cr = item % ncr;
+                if (!item_live(rb, cr)) continue;
+                const int rbase = k + 1 + rb * SRB;
+                const int mEnd = min(cnt, mB + (cr + 1) * CRW);
+                const int row0 = rbase + lane;
+                double xv[8], z[8];
+#pragma unroll
+                for (int u = 0; u < 8; ++u) {
+                    const int r = row0 + 32 * u;
+                    xv[u] = r < n ? (r == k + 1 ? 1.0 : cv[r]) : 0.0;
+                    z[u] = 0.0;
+                }
+                for (int m0 = mB + cr * CRW; m0 < mEnd; m0 += 4) {
+                    int col[4];
+                    double vc[4];
+#pragma unroll
+                    for (int c = 0; c < 4; ++c) {
+                        col[c] = (m0 + c < mEnd) ? rank + CL * (m0 + c) : n;   // n: no column
+                        vc[c] = (m0 + c < mEnd) ? (col[c] == k + 1 ? 1.0 : cv[col[c]]) : 0.0;
+                    }
+                    double x[4][8];
+#pragma unroll
+                    for (int u = 0; u < 8; ++u)
+#pragma unroll
+                        for (int c = 0; c < 4; ++c) {
+                            const int r = row0 + 32 * u;
+                            x[c][u] = (r < n && r >= col[c]) ? A[(size_t)col[c] * n + r] : 0.0;
+                        }
+                    double sc[4] = {0.0, 0.0, 0.0, 0.0};
+#pragma unroll
+                    for (int u = 0; u < 8; ++u)
+#pragma unroll
+                        for (int c = 0; c < 4; ++c) {
+                            sc[c] = fma(x[c][u], xv[u], sc[c]);
+                            if (row0 + 32 * u > col[c]) z[u] = fma(x[c][u], vc[c], z[u]);
+                        }
+#pragma unroll
+                    for (int c = 0; c < 4; ++c) sc[c] = warp_sum(sc[c]);
+                    if (lane == 0)
+#pragma unroll
+                        for (int c = 0; c < 4; ++c)
+                            if (m0 + c < mEnd) ysp[rb * MM + m0 + c] = sc[c];
+                }
+#pragma unroll
+                for (int u = 0; u < 8; ++u)
+                    if (row0 + 32 * u < n) zsp[cr * PN + row0 + 32 * u] = z[u];
+            }
+            __syncthreads();
+            // row sums of z (fixed order over the live ranges) to the rows' owners, and this
+            // block's part of v^T A v: sum over own columns of v(l) dot(l) plus sum over all
+            // rows of v(i) z(i)
+            double yvp = 0.0;
+            for (int r = k + 1 + tid; r < n; r += TT) {
+                const int rb = (r - k - 1) / SRB;
+                double zt = 0.0;
+                for (int cr = 0; cr < ncr; ++cr)
+                    if (item_live(rb, cr)) zt += zsp[cr * PN + r];
+                cluster.map_shared_rank(zr, r % CL)[rank * MM + r / CL] = zt;
+                yvp = fma(r == k + 1 ? 1.0 : cv[r], zt, yvp);
+            }
+            const int mc = mB + tid;
+            const bool own_c = mc < cnt;
+            double dot = 0.0;
+            if (own_c) {
+                const int l = rank + CL * mc;
+                for (int rb = (l - k - 1) / SRB; rb < nrb; ++rb) dot += ysp[rb * MM + mc];
+                ys[mc] = dot;
+                yvp = fma(vj[mc], dot, yvp);
+                // y(k+1) has no z part (no own column lies left of it in the trailing block)
+                if (pivot_owner && k + 1 <= last && l == k + 1)
+                    for (int r = 0; r < CL; ++r) cluster.map_shared_rank(Y1, r)[0] = dot;
+            }
+            yvp = block_sum(yvp, red);
+            if (tid < CL) cluster.map_shared_rank(P2, tid)[rank * P2W + 2 * NB] = yvp;
+            cluster.sync();
+            // ---- C: totals, y of the own columns, w of the own rows and of the next pivot row ----
+            if (own_c) {
+                double zz = 0.0;
+                for (int r = 0; r < CL; ++r) zz += zr[r * MM + mc];
+                ys[mc] += zz;
+            }
+            if (tid < 2 * j) {
+                const int o = tid < j ? tid : NB + (tid - j);
+                double s = 0.0;
+                for (int r = 0; r < CL; ++r) s += P2[r * P2W + o];
+                tsum[o] = s;
+            } else if (tid == TT - 1) {
+                double s = 0.0;
+                for (int r = 0; r < CL; ++r) s += P2[r * P2W + 2 * NB];
+                tsum[2 * NB] = s;
+            }
+            __syncthreads();
+            double t12 = 0.0, t12b = 0.0;
+            for (int q = 0; q + 1 < j; q += 2) {
+                t12 = fma(tsum[q], tsum[NB + q], t12);
+                t12b = fma(tsum[q + 1], tsum[NB + q + 1], t12b);
+            }
+            if (j & 1) t12 = fma(tsum[j - 1], tsum[NB + j - 1], t12);
+            const double wv = tau * (tsum[2 * NB] - 2.0 * (t12 + t12b));
+            const double al = -0.5 * tau * wv;
+            if (own_c) WO[j * MM + mc] = w_entry(ys[mc], VO + mc, WO + mc, MM, tsum, tsum + NB, j, tau, al, vj[mc]);
+            if (k + 1 <= last) {
+                if (tid < j) {
+                    piv[tid] = pivn[NB + tid];        // W(k+1, q)
+                    piv[NB + tid] = pivn[tid];        // V(k+1, q)
+                } else if (tid == TT - 1) {
+                    piv[j] = w_entry(Y1[0], pivn, pivn + NB, 1, tsum, tsum + NB, j, tau, al, 1.0);
+                    piv[NB + j] = 1.0;
+                }
+            }
+            __syncthreads();
+        }
+        // ---- the panel's V, W, reflectors, D, E, tau to global memory ----
+        const int m1 = first_own(p + 1), nm1 = cnt - m1;
+        for (int e = tid; e < jn * nm1; e += TT) {
+            const int mm = m1 + e % nm1, q = e / nm1;
+            const int i = rank + CL * mm, kq = p + q;
+            if (i >= kq + 1) {
+                const double v = VO[q * MM + mm];
+                Vg[(size_t)i + (size_t)q * n] = v;
+                Wg[(size_t)i + (size_t)q * n] = WO[q * MM + mm];
+                if (i > kq + 1) A[(size_t)i + (size_t)kq * n] = v;
+            }
+        }
+        if (tid < jn) {
+            const int kq = p + tid;
+            if (kq % CL == rank) L.D[kq] = pan[tid];
+            if (rank == 0) { L.E[kq] = pan[NB + tid]; L.TAU[kq] = pan[2 * NB + tid]; }
+        }
+        // ---- lower-triangle update of the own columns l >= r0: rows >= l ----
+        const int r0 = last + 1, jc = last - p + 1;
+        cluster.sync();
+        const int mR = first_own(r0);
+        const int tr = tid & 31, tc = tid >> 5;
+        for (int ib = r0; ib < n; ib += TRS) {
+            // own columns that reach this chunk: rank + CL*m <= ib + TRS - 1
+            const int lastrow = min(ib + TRS, n) - 1;
+            const int mLim = lastrow >= rank ? min(cnt, (lastrow - rank) / CL + 1) : 0;
+            if (mLim <= mR) continue;   // no own column reaches this chunk yet (uniform in the block)
+            for (int e = tid; e < jc * TRS; e += TT) {
+                const int q = e / TRS, r = e % TRS, row = ib + r;
+                stV[q * TRS + r] = row < n ? __ldcg(Vg + row + (size_t)q * n) : 0.0;
+                stW[q * TRS + r] = row < n ? __ldcg(Wg + row + (size_t)q * n) : 0.0;
+            }
+            __syncthreads();
+            for (int mc = mR; mc < mLim; mc += 4 * (TT / 32)) {
+                const int m0 = mc + 4 * tc;
+                if (m0 < mLim) {
+                    int mcol[4];
+#pragma unroll
+                    for (int c = 0; c < 4; ++c) mcol[c] = min(m0 + c, mLim - 1);
+                    double acc[2][4];
+#pragma unroll
+                    for (int u = 0; u < 2; ++u)
+#pragma unroll
+                        for (int c = 0; c < 4; ++c) acc[u][c] = 0.0;
+                    for (int q = 0; q < jc; ++q) {
+                        double av[2], aw[2], bw[4], bv[4];
+#pragma unroll
+                        for (int u = 0; u < 2; ++u) {
+                            av[u] = stV[q * TRS + tr + 32 * u];
+                            aw[u] = stW[q * TRS + tr + 32 * u];
+                        }
+#pragma unroll
+                        for (int c = 0; c < 4; ++c) {
+                            bw[c] = WO[q * MM + mcol[c]];
+                            bv[c] = VO[q * MM + mcol[c]];
+                        }
+#pragma unroll
+                        for (int u = 0; u < 2; ++u)
+#pragma unroll
+                            for (int c = 0; c < 4; ++c) acc[u][c] = fma(av[u], bw[c], fma(aw[u], bv[c], acc[u][c]));
+                    }
+#pragma unroll
+                    for (int c = 0; c < 4; ++c) {
+                        if (m0 + c >= mLim) continue;
+                        const int l = rank + CL * (m0 + c);
+                        double* colp = A + (size_t)l * n;
+#pragma unroll
+                        for (int u = 0; u < 2; ++u) {
+                            const int row = ib + tr + 32 * u;
+                            if (row < n && row >= l) colp[row] -= acc[u][c];
+                        }
+                    }
+                }
+            }
+            __syncthreads();
+        }
+        // the next panel reads its columns' own rows from columns that other blocks own
+        // and have just updated: their stores are visible after this barrier
+        cluster.sync();
+    }
+    if ((n - 1) % CL == rank && tid == 0) L.D[n - 1] = A[(size_t)(n - 1) + (size_t)(n - 1) * n];
+    if (rank == 0 && tid == 0) L.E[n - 1] = 0.0;
+    cluster.sync();   // no block leaves while another may still write its shared memory
+}
+
 __global__ void k_tri_end(const LSec* __restrict__ secs, double* eigbuf, double* wsd, int* wsi) {
     const LSec sec = secs[blockIdx.x];
     if (threadIdx.x != 0) return;
@@ -952,11 +1295,60 @@ static int tri_cluster_cl(nrg_context* ctx, const LSec* dsec, int ns, int maxn, 
     return NRG_OK;
 }
 
+// The lower-triangle variant, when its layout fits in shared memory: the column ranges
+// of its product are as narrow as the space allows (more work items to balance).
+template <int CL>
+static int tri_csym_cl(nrg_context* ctx, const LSec* dsec, int ns, int maxn, double* d_V, double* wsd,
+                       int* wsi, bool* done) {
+    *done = false;
+    int dev = 0, optin = 0;
+    NRG_CUDA_TRY(cudaGetDevice(&dev));
+    NRG_CUDA_TRY(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+    TriLayoutS lay;
+    lay.MM = (maxn + CL - 1) / CL;
+    lay.PN = maxn + (maxn & 1);
+    lay.NRB = (maxn + SRB - 1) / SRB;
+    if (lay.MM > TT) return NRG_OK;
+    size_t smem = 0;
+    bool fits = false;
+    for (int crw : {32, 48, 64, 96, 128}) {
+        lay.CRW = crw;
+        lay.NCR = (lay.MM + crw - 1) / crw;
+        smem = sizeof(double) * (size_t)lay.doubles(CL);
+        if (smem <= (size_t)optin) { fits = true; break; }
+    }
+    if (!fits) return NRG_OK;
+    NRG_TRY(raise_smem_limit((const void*)k_tri_csym<CL>, smem));
+    if (CL > 8) NRG_CUDA_TRY(cudaFuncSetAttribute(k_tri_csym<CL>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((unsigned)(CL * ns));
+    cfg.blockDim = dim3(TT);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = ctx->stream;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeClusterDimension;
+    at[0].val.clusterDim.x = CL;
+    at[0].val.clusterDim.y = 1;
+    at[0].val.clusterDim.z = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    int clusters = 0;
+    if (cudaOccupancyMaxActiveClusters(&clusters, k_tri_csym<CL>, &cfg) != cudaSuccess || clusters < 1) {
+        cudaGetLastError();
+        return NRG_OK;
+    }
+    NRG_CUDA_TRY(cudaLaunchKernelEx(&cfg, k_tri_csym<CL>, dsec, lay, d_V, wsd, wsi));
+    ctx->launches++;
+    *done = true;
+    return NRG_OK;
+}
+
 // Cluster size of the one-launch tridiagonalisation: 8 blocks per sector (16 for the
 // largest size class alone halves its per-block product but costs as much in the wider
 // exchanges: no net gain measured); a size that cannot be placed falls back to the next
 // smaller one.  The environment variable NRG_TRI_CLUSTER forces 4, 8 or 16, or 0 for the
-// multi-kernel path.
+// multi-kernel path.  The lower-triangle kernel is taken for 8 or 16 blocks when its
+// layout fits; NRG_TRI_SYM=0 keeps the full-column kernel.
 static int tri_cluster(nrg_context* ctx, const LSec* dsec, int ns, int maxn, double* d_V, double* wsd,
                        int* wsi, bool* done) {
     static const int forced = [] {
@@ -965,8 +1357,20 @@ static int tri_cluster(nrg_context* ctx, const LSec* dsec, int ns, int maxn, dou
         const int v = atoi(e);
         return (v == 0 || v == 4 || v == 8 || v == 16) ? v : -1;
     }();
+    static const bool sym = [] {
+        const char* e = getenv("NRG_TRI_SYM");
+        return !(e && e[0] == '0');
+    }();
     *done = false;
     const int cl = forced >= 0 ? forced : kTriCL;
+    if (sym && cl == 16) {
+        NRG_TRY(tri_csym_cl<16>(ctx, dsec, ns, maxn, d_V, wsd, wsi, done));
+        if (*done) return NRG_OK;
+    }
+    if (sym && cl == 8) {
+        NRG_TRY(tri_csym_cl<8>(ctx, dsec, ns, maxn, d_V, wsd, wsi, done));
+        if (*done) return NRG_OK;
+    }
     if (cl == 16) {
         NRG_TRY(tri_cluster_cl<16>(ctx, dsec, ns, maxn, d_V, wsd, wsi, done));
         if (*done || forced == 16) return NRG_OK;

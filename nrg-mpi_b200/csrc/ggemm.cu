@@ -10,17 +10,20 @@
 //   B(k,j) = B[ki(k)*b_sk + ji(j)*b_sj]          ki = b_ki ? b_ki[k] : k, ji likewise
 //   C(i,j) = C[ci(i)*c_si + cj(j)*c_sj]          ci = c_ri ? c_ri[i] : i, cj likewise
 //
-// 64x64 output tiles, 128 threads (four warps of 32x32), FP64 tensor-core MMA
-// (mma.sync m8n8k4 f64); k slabs of 16 staged in shared memory, the next slab's global
-// loads held in registers while the current slab is multiplied.  Loads are coalesced
-// along whichever index of each operand has unit stride.
+// Output tiles of 32x32 per warp (64x64 with four warps, 32x32 with one, 128x64 and
+// 64x128 with eight), FP64 tensor-core MMA (mma.sync m8n8k4 f64); k slabs of 16 staged in
+// shared memory, the next slab's global loads held in registers while the current slab is
+// multiplied.  Loads are coalesced along whichever index of each operand has unit stride.
+// The tile shape of each launch is chosen by the context's tuner (GemmTuner below).
 #include "internal.hpp"
+
+#include <algorithm>
+#include <cstdlib>
 
 namespace nrg {
 namespace {
 
-constexpr int TM = 64, TN = 64, TK = 16, NT = 128;
-constexpr int LDA = TM + 4, LDB = TN + 4;   // [k][i] and [k][j] rows, padded against bank conflicts
+constexpr int TK = 16;
 
 __device__ __forceinline__ void dmma(double& d0, double& d1, double a, double b) {
     asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};\n"
@@ -28,18 +31,32 @@ __device__ __forceinline__ void dmma(double& d0, double& d1, double a, double b)
                  : "d"(a), "d"(b));
 }
 
-struct Slab {
-    double a[(TM * TK) / NT], b[(TN * TK) / NT];
+// WM x WN warps per block, each computing a 32 x 32 piece of the (32 WM) x (32 WN) output
+// tile.  Every variant accumulates each output element over k in the same order (slabs of
+// 16, then the k = 4 steps of the MMA), so all variants give bit-identical results and the
+// tile choice is free to change between launches.
+template <int WM, int WN>
+struct Tile {
+    static constexpr int TM = 32 * WM, TN = 32 * WN, NT = 32 * WM * WN;
+    static constexpr int LDA = TM + 4, LDB = TN + 4;   // [k][i] and [k][j] rows, padded
+    static constexpr int EA = (TM * TK) / NT, EB = (TN * TK) / NT;
+    static constexpr size_t smem_bytes() { return sizeof(double) * 2 * TK * (LDA + LDB); }
 };
 
-__device__ __forceinline__ void fetch_slab(const GemmProblem& P, int i0, int j0, int k0, Slab& r, bool a_kfast,
+template <class T>
+struct Slab {
+    double a[T::EA], b[T::EB];
+};
+
+template <class T>
+__device__ __forceinline__ void fetch_slab(const GemmProblem& P, int i0, int j0, int k0, Slab<T>& r, bool a_kfast,
                                            bool b_kfast) {
     const int tid = threadIdx.x;
 #pragma unroll
-    for (int u = 0; u < (TM * TK) / NT; ++u) {
-        const int e = tid + u * NT;
+    for (int u = 0; u < T::EA; ++u) {
+        const int e = tid + u * T::NT;
         int ii, kk;
-        if (a_kfast) { kk = e % TK; ii = e / TK; } else { ii = e % TM; kk = e / TM; }
+        if (a_kfast) { kk = e % TK; ii = e / TK; } else { ii = e % T::TM; kk = e / T::TM; }
         const int gi = i0 + ii, gk = k0 + kk;
         double v = 0.0;
         if (gi < P.M && gk < P.K) {
@@ -50,10 +67,10 @@ __device__ __forceinline__ void fetch_slab(const GemmProblem& P, int i0, int j0,
         r.a[u] = v;
     }
 #pragma unroll
-    for (int u = 0; u < (TN * TK) / NT; ++u) {
-        const int e = tid + u * NT;
+    for (int u = 0; u < T::EB; ++u) {
+        const int e = tid + u * T::NT;
         int jj, kk;
-        if (b_kfast) { kk = e % TK; jj = e / TK; } else { jj = e % TN; kk = e / TN; }
+        if (b_kfast) { kk = e % TK; jj = e / TK; } else { jj = e % T::TN; kk = e / T::TN; }
         const int gj = j0 + jj, gk = k0 + kk;
         double v = 0.0;
         if (gj < P.N && gk < P.K) {
@@ -65,28 +82,33 @@ __device__ __forceinline__ void fetch_slab(const GemmProblem& P, int i0, int j0,
     }
 }
 
-__device__ __forceinline__ void store_slab(const Slab& r, double* As, double* Bs, bool a_kfast, bool b_kfast) {
+template <class T>
+__device__ __forceinline__ void store_slab(const Slab<T>& r, double* As, double* Bs, bool a_kfast, bool b_kfast) {
     const int tid = threadIdx.x;
 #pragma unroll
-    for (int u = 0; u < (TM * TK) / NT; ++u) {
-        const int e = tid + u * NT;
+    for (int u = 0; u < T::EA; ++u) {
+        const int e = tid + u * T::NT;
         int ii, kk;
-        if (a_kfast) { kk = e % TK; ii = e / TK; } else { ii = e % TM; kk = e / TM; }
-        As[kk * LDA + ii] = r.a[u];
+        if (a_kfast) { kk = e % TK; ii = e / TK; } else { ii = e % T::TM; kk = e / T::TM; }
+        As[kk * T::LDA + ii] = r.a[u];
     }
 #pragma unroll
-    for (int u = 0; u < (TN * TK) / NT; ++u) {
-        const int e = tid + u * NT;
+    for (int u = 0; u < T::EB; ++u) {
+        const int e = tid + u * T::NT;
         int jj, kk;
-        if (b_kfast) { kk = e % TK; jj = e / TK; } else { jj = e % TN; kk = e / TN; }
-        Bs[kk * LDB + jj] = r.b[u];
+        if (b_kfast) { kk = e % TK; jj = e / TK; } else { jj = e % T::TN; kk = e / T::TN; }
+        Bs[kk * T::LDB + jj] = r.b[u];
     }
 }
 
-__global__ void __launch_bounds__(NT) k_ggemm(const GemmProblem* __restrict__ probs,
-                                              const int* __restrict__ tilePrefix, int nprob) {
-    __shared__ double As[2][TK * LDA];
-    __shared__ double Bs[2][TK * LDB];
+template <int WM, int WN>
+__global__ void __launch_bounds__(32 * WM * WN) k_ggemm(const GemmProblem* __restrict__ probs,
+                                                        const int* __restrict__ tilePrefix, int nprob) {
+    using T = Tile<WM, WN>;
+    extern __shared__ double gsm[];
+    // two A slabs, then two B slabs
+    auto As = [&](int x) { return gsm + x * (TK * T::LDA); };
+    auto Bs = [&](int x) { return gsm + 2 * TK * T::LDA + x * (TK * T::LDB); };
     const int bid = blockIdx.x;
     int lo = 0, hi = nprob - 1;
     while (lo < hi) {
@@ -95,8 +117,8 @@ __global__ void __launch_bounds__(NT) k_ggemm(const GemmProblem* __restrict__ pr
     }
     GemmProblem P = probs[lo];
     const int t = bid - tilePrefix[lo];
-    const int tilesN = (P.N + TN - 1) / TN;
-    const int i0 = (t / tilesN) * TM, j0 = (t % tilesN) * TN;
+    const int tilesN = (P.N + T::TN - 1) / T::TN;
+    const int i0 = (t / tilesN) * T::TM, j0 = (t % tilesN) * T::TN;
     if (P.dyn_nk) {
         const int v = *P.dyn_nk;
         P.N = min(P.N, v);
@@ -106,7 +128,7 @@ __global__ void __launch_bounds__(NT) k_ggemm(const GemmProblem* __restrict__ pr
     const bool a_kfast = (P.a_sk == 1 && P.a_si != 1);
     const bool b_kfast = (P.b_sk == 1 && P.b_sj != 1);
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const int wi = (warp >> 1) * 32, wj = (warp & 1) * 32;   // warp tile origin
+    const int wi = (warp / WN) * 32, wj = (warp % WN) * 32;   // warp tile origin
     const int g = lane >> 2, q4 = lane & 3;
     double acc[4][4][2];
 #pragma unroll
@@ -114,30 +136,30 @@ __global__ void __launch_bounds__(NT) k_ggemm(const GemmProblem* __restrict__ pr
 #pragma unroll
         for (int c = 0; c < 4; ++c) acc[r][c][0] = acc[r][c][1] = 0.0;
     const int nslab = (P.K + TK - 1) / TK;
-    Slab reg;
+    Slab<T> reg;
     if (nslab > 0) {
-        fetch_slab(P, i0, j0, 0, reg, a_kfast, b_kfast);
-        store_slab(reg, As[0], Bs[0], a_kfast, b_kfast);
+        fetch_slab<T>(P, i0, j0, 0, reg, a_kfast, b_kfast);
+        store_slab<T>(reg, As(0), Bs(0), a_kfast, b_kfast);
     }
     __syncthreads();
     for (int s = 0; s < nslab; ++s) {
         const int cur = s & 1;
-        if (s + 1 < nslab) fetch_slab(P, i0, j0, (s + 1) * TK, reg, a_kfast, b_kfast);
-        const double* as = As[cur];
-        const double* bs = Bs[cur];
+        if (s + 1 < nslab) fetch_slab<T>(P, i0, j0, (s + 1) * TK, reg, a_kfast, b_kfast);
+        const double* as = As(cur);
+        const double* bs = Bs(cur);
 #pragma unroll
         for (int ks = 0; ks < TK; ks += 4) {
             double af[4], bf[4];
 #pragma unroll
-            for (int r = 0; r < 4; ++r) af[r] = as[(ks + q4) * LDA + wi + r * 8 + g];
+            for (int r = 0; r < 4; ++r) af[r] = as[(ks + q4) * T::LDA + wi + r * 8 + g];
 #pragma unroll
-            for (int c = 0; c < 4; ++c) bf[c] = bs[(ks + q4) * LDB + wj + c * 8 + g];
+            for (int c = 0; c < 4; ++c) bf[c] = bs[(ks + q4) * T::LDB + wj + c * 8 + g];
 #pragma unroll
             for (int r = 0; r < 4; ++r)
 #pragma unroll
                 for (int c = 0; c < 4; ++c) dmma(acc[r][c][0], acc[r][c][1], af[r], bf[c]);
         }
-        if (s + 1 < nslab) store_slab(reg, As[cur ^ 1], Bs[cur ^ 1], a_kfast, b_kfast);
+        if (s + 1 < nslab) store_slab<T>(reg, As(cur ^ 1), Bs(cur ^ 1), a_kfast, b_kfast);
         __syncthreads();
     }
 #pragma unroll
@@ -160,7 +182,96 @@ __global__ void __launch_bounds__(NT) k_ggemm(const GemmProblem* __restrict__ pr
     }
 }
 
+// the tile variants, in the order of GemmTuner's slots
+constexpr int kVariants = 4;
+constexpr int kWM[kVariants] = {2, 1, 4, 2};
+constexpr int kWN[kVariants] = {2, 1, 2, 4};
+
+template <int WM, int WN>
+int launch_variant(nrg_context* ctx, long long total_blocks_hint, const GemmProblem* dp, const int* dq, int np,
+                   const std::vector<GemmProblem>& live, std::vector<int>& prefix, DevBuf& prefixBuf) {
+    using T = Tile<WM, WN>;
+    long long total = 0;
+    for (int i = 0; i < np; ++i) {
+        prefix[i] = (int)total;
+        total += (long long)((live[i].M + T::TM - 1) / T::TM) * ((live[i].N + T::TN - 1) / T::TN);
+    }
+    (void)total_blocks_hint;
+    if (total > 0x7fffffffLL) return NRG_ERR_TOO_LARGE;
+    NRG_TRY(h2d_async(ctx, prefixBuf.p, prefix.data(), sizeof(int) * np));
+    const size_t smem = T::smem_bytes();
+    if (smem > 48 * 1024) NRG_TRY(raise_smem_limit((const void*)k_ggemm<WM, WN>, smem));
+    k_ggemm<WM, WN><<<(unsigned)total, T::NT, smem, ctx->stream>>>(dp, dq, np);
+    ctx->launches++;
+    NRG_CUDA_TRY(cudaGetLastError());
+    return NRG_OK;
+}
+
+int log2_bucket(long long v) {
+    int b = 0;
+    while (v > 1 && b < 15) { v >>= 1; ++b; }
+    return b;
+}
+
 }  // namespace
+
+// Online tuning of the tile shape.  Launches are keyed by their problem mix (log2 buckets
+// of the median M, N, K and of the problem count); the first launches of a key try each
+// tile variant in turn, timed by events on the context's stream, and later launches of
+// the key take the variant with the least time per flop.  Timings are read without
+// waiting: a pending measurement is collected by a later launch once its events have
+// completed.  The variants give bit-identical results, so the choice never changes a
+// result.  NRG_GGEMM_VARIANT=0..3 fixes one variant (no tuning).
+int GemmTuner::pick(unsigned key) {
+    static const int forced = [] {
+        const char* e = getenv("NRG_GGEMM_VARIANT");
+        if (!e || !*e) return -1;
+        const int v = atoi(e);
+        return (v >= 0 && v < kTunedVariants) ? v : -1;
+    }();
+    if (forced >= 0) return forced;
+    Entry& e = table[key];
+    for (int v = 0; v < kTunedVariants; ++v)
+        if (e.samples[v] < kSamples && e.inflight[v] == 0) return v;
+    int best = 0;
+    for (int v = 1; v < kTunedVariants; ++v)
+        if (e.samples[v] > 0 && (e.samples[best] == 0 || e.ms_per_gflop[v] < e.ms_per_gflop[best])) best = v;
+    return best;
+}
+
+void GemmTuner::collect(bool wait) {
+    for (size_t i = 0; i < pending.size();) {
+        Pending& q = pending[i];
+        cudaError_t st = wait ? cudaEventSynchronize(q.b) : cudaEventQuery(q.b);
+        if (st == cudaErrorNotReady) { ++i; continue; }
+        float ms = 0.0f;
+        if (st == cudaSuccess && cudaEventElapsedTime(&ms, q.a, q.b) == cudaSuccess && q.gflop > 0.0) {
+            Entry& e = table[q.key];
+            const double r = ms / q.gflop;
+            e.ms_per_gflop[q.variant] = e.samples[q.variant] == 0 ? r : std::min(e.ms_per_gflop[q.variant], r);
+            e.samples[q.variant]++;
+            e.inflight[q.variant]--;
+        } else {
+            cudaGetLastError();
+            table[q.key].inflight[q.variant]--;
+        }
+        free_events.push_back(q.a);
+        free_events.push_back(q.b);
+        pending[i] = pending.back();
+        pending.pop_back();
+    }
+}
+
+void GemmTuner::release() {
+    for (auto& q : pending) {
+        cudaEventSynchronize(q.b);
+        cudaEventDestroy(q.a);
+        cudaEventDestroy(q.b);
+    }
+    pending.clear();
+    for (cudaEvent_t e : free_events) cudaEventDestroy(e);
+    free_events.clear();
+}
 
 int launch_ggemm(nrg_context* ctx, std::vector<GemmProblem>& probs, int scratch_slot) {
     // drop empty problems
@@ -170,23 +281,65 @@ int launch_ggemm(nrg_context* ctx, std::vector<GemmProblem>& probs, int scratch_
         if (p.M > 0 && p.N > 0 && p.K > 0) live.push_back(p);
     const int np = (int)live.size();
     if (np == 0) return NRG_OK;
-    std::vector<int> prefix(np);
-    long long total = 0;
+    // problem-mix key and algorithmic flops
+    std::vector<int> ms(np), ns(np), ks(np);
+    double gflop = 0.0;
     for (int i = 0; i < np; ++i) {
-        live[i].tiles = ((live[i].M + TM - 1) / TM) * ((live[i].N + TN - 1) / TN);
-        prefix[i] = (int)total;
-        total += live[i].tiles;
+        ms[i] = live[i].M;
+        ns[i] = live[i].N;
+        ks[i] = live[i].K;
+        gflop += 2e-9 * live[i].M * (double)live[i].N * live[i].K;
     }
-    if (total > 0x7fffffffLL) return NRG_ERR_TOO_LARGE;
+    auto med = [](std::vector<int>& v) {
+        std::nth_element(v.begin(), v.begin() + v.size() / 2, v.end());
+        return (long long)v[v.size() / 2];
+    };
+    const unsigned key = (unsigned)(log2_bucket(med(ms)) | log2_bucket(med(ns)) << 4 | log2_bucket(med(ks)) << 8 |
+                                    log2_bucket(np) << 12);
+    GemmTuner& tu = ctx->gemm_tuner;
+    tu.collect(false);
+    const int v = tu.pick(key);
     DevBuf& dp = ctx->scratch.b[scratch_slot];
     DevBuf& dq = ctx->scratch.b[scratch_slot + 1];
     NRG_TRY(dp.ensure(sizeof(GemmProblem) * np));
     NRG_TRY(dq.ensure(sizeof(int) * np));
+    for (auto& p : live) p.tiles = 0;   // unused by the kernels (the prefix carries the tiling)
     NRG_TRY(h2d_async(ctx, dp.p, live.data(), sizeof(GemmProblem) * np));
-    NRG_TRY(h2d_async(ctx, dq.p, prefix.data(), sizeof(int) * np));
-    k_ggemm<<<(unsigned)total, NT, 0, ctx->stream>>>(dp.as<GemmProblem>(), dq.as<int>(), np);
-    ctx->launches++;
-    NRG_CUDA_TRY(cudaGetLastError());
+    std::vector<int> prefix(np);
+    const bool timed = tu.table[key].samples[v] < GemmTuner::kSamples && tu.table[key].inflight[v] == 0;
+    cudaEvent_t ea = nullptr, eb = nullptr;
+    if (timed) {
+        NRG_TRY(tu.event(&ea));
+        NRG_TRY(tu.event(&eb));
+        NRG_CUDA_TRY(cudaEventRecord(ea, ctx->stream));
+    }
+    int rc = NRG_OK;
+    switch (v) {
+        case 0: rc = launch_variant<kWM[0], kWN[0]>(ctx, 0, dp.as<GemmProblem>(), dq.as<int>(), np, live, prefix, dq); break;
+        case 1: rc = launch_variant<kWM[1], kWN[1]>(ctx, 0, dp.as<GemmProblem>(), dq.as<int>(), np, live, prefix, dq); break;
+        case 2: rc = launch_variant<kWM[2], kWN[2]>(ctx, 0, dp.as<GemmProblem>(), dq.as<int>(), np, live, prefix, dq); break;
+        default: rc = launch_variant<kWM[3], kWN[3]>(ctx, 0, dp.as<GemmProblem>(), dq.as<int>(), np, live, prefix, dq); break;
+    }
+    if (timed) {
+        if (rc == NRG_OK) {
+            NRG_CUDA_TRY(cudaEventRecord(eb, ctx->stream));
+            tu.table[key].inflight[v]++;
+            tu.pending.push_back({key, v, ea, eb, gflop});
+        } else {
+            tu.free_events.push_back(ea);
+            tu.free_events.push_back(eb);
+        }
+    }
+    return rc;
+}
+
+int GemmTuner::event(cudaEvent_t* e) {
+    if (!free_events.empty()) {
+        *e = free_events.back();
+        free_events.pop_back();
+        return NRG_OK;
+    }
+    NRG_CUDA_TRY(cudaEventCreate(e));
     return NRG_OK;
 }
 

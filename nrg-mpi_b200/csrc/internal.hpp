@@ -7,6 +7,7 @@
 #include <vector>
 #include <map>
 #include <deque>
+#include <unordered_map>
 
 namespace nrg {
 
@@ -97,6 +98,31 @@ struct Scratch {
 
 }  // namespace nrg
 
+namespace nrg {
+// per-context choice of the grouped GEMM's tile shape (ggemm.cu)
+struct GemmTuner {
+    static constexpr int kTunedVariants = 4, kSamples = 2;
+    struct Entry {
+        double ms_per_gflop[kTunedVariants] = {0.0, 0.0, 0.0, 0.0};
+        int samples[kTunedVariants] = {0, 0, 0, 0};
+        int inflight[kTunedVariants] = {0, 0, 0, 0};
+    };
+    struct Pending {
+        unsigned key;
+        int variant;
+        cudaEvent_t a, b;
+        double gflop;
+    };
+    std::unordered_map<unsigned, Entry> table;
+    std::vector<Pending> pending;
+    std::vector<cudaEvent_t> free_events;
+    int pick(unsigned key);
+    void collect(bool wait);
+    void release();
+    int event(cudaEvent_t* e);
+};
+}  // namespace nrg
+
 struct nrg_context {
     int device = 0;
     cudaStream_t stream = nullptr;
@@ -106,6 +132,7 @@ struct nrg_context {
     long long launches = 0;
     // measurement counters (nrg_context_get_stats)
     bool profiling = false;
+    nrg::GemmTuner gemm_tuner;   // tile shape of the grouped GEMM per problem mix
     long long syev_launches = 0;
     double syev_ms = 0.0, syev_flops = 0.0;
     long long h2d = 0, d2h = 0;
@@ -199,6 +226,8 @@ struct GemmProblem {
     const int* dyn_nk;
 };
 int launch_ggemm(nrg_context* ctx, std::vector<GemmProblem>& probs, int scratch_slot);
+
+
 
 // eigensolver for sectors of order > 128 across the whole GPU (eig_large.cu); the
 // descriptors use a_off / e_off / n only

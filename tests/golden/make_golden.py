@@ -11,7 +11,10 @@ Workloads (``nrg_b200.model.config``):
 * ``siam_nkeep4096_n14.npz`` SIAM Lambda=2.0 U=0.3 Gamma=0.03 eps_d=-0.15, N_keep=4096, a
   window of the chain: its first 14 iterations, -1..12 (the model cut there, so iteration
   12 is the last one: no truncation there, the density matrices start from its ground
-  states), with the spectrum over that window.
+  states), with the spectrum over that window;
+* ``two_orbital_nkeep8192_n5.npz`` the two-orbital Hund model (U=0.2, J=0.02, Gamma=0.015
+  per orbital, Lambda=3, 16 local states, N_keep=8192), its first 5 iterations (-1..3),
+  forward sweep only (no spectrum): sectors of order up to ~8,800, tied sort keys.
 
 Stored per iteration: the kept count, the number of states before truncation, the
 ground-state energy (eigenvalue(1) before the shift), the lowest ``FLOW`` kept energies
@@ -37,16 +40,33 @@ from oracle import nrg_oracle as O  # noqa: E402
 
 FLOW = 64
 
+def _two_orbital_window():
+    inp = model.config(4, n_iterations=5)
+    inp.flag_spectrum = False       # forward sweep only
+    return inp
+
+
 CASES = {
     "siam_nkeep2048": lambda: model.config(2),
     "siam_nkeep4096_n14": lambda: model.config(3, n_iterations=14),
+    "two_orbital_nkeep8192_n5": _two_orbital_window,
 }
 
 
 def golden(inp) -> dict:
     d = tempfile.mkdtemp(prefix="nrg_golden_")
     model.write_inputs(inp, d)
-    st = O.run(d)
+    st = O.State(d)
+    nfull = {}
+    for it in range(st.first, st.nIter + 1):        # main.F90:175-177, as nrg_oracle.run
+        O.nrg_iteration(st, it)
+        nfull[it] = st.numberOfBasis_full
+    if st.flag_spectrum:
+        if st.flag_truncation:                        # main.F90:188-201
+            O.initialize_reduced_density(st)
+            O.reduced_density_matrix_calculation(st)
+        for it in range(st.startTrancation, st.nIter + 1):
+            O.cfs_spectrum_calculation(st, it)
     its = list(range(st.first, st.nIter + 1))
     flow = np.full((len(its), FLOW), np.nan)
     for k, i in enumerate(its):
@@ -59,7 +79,7 @@ def golden(inp) -> dict:
         first=st.first, nIter=st.nIter, startTrancation=st.startTrancation, numberOfBin=st.numberOfBin,
         nMat=st.nMat,
         kept=np.array([st.kept[i] for i in its], dtype=np.int32),
-        numberOfBasisFull=np.array([st.restore[i]["numberOfBasis_full"] for i in its], dtype=np.int32),
+        numberOfBasisFull=np.array([nfull[i] for i in its], dtype=np.int32),
         groundStateEnergy=np.array([st.ground_state_energy[i] for i in its]),
         flow=flow,
         thermo=np.array([st.thermo[i] for i in its]),

@@ -1,8 +1,11 @@
-"""The multi-kernel tridiagonalisation (two launches per column, then grouped-GEMM panel
-updates), which sectors too large for the one-launch cluster kernel's shared memory
-take (order above ~1500): the large-sector parity test re-run in a child process with
-NRG_TRI_CLUSTER=0, which sends every sector of order > 128 down that path (the variable
-is read once per process)."""
+"""The tridiagonalisation paths other than the default one (the lower-triangle cluster
+kernel on 8-block clusters), each through the large-sector parity test re-run in a child
+process with the environment variable that selects it (read once per process):
+* the multi-kernel path (two launches per column, then grouped-GEMM panel updates), which
+  sectors too large for the cluster kernels' shared memory take: NRG_TRI_CLUSTER=0;
+* the full-column cluster kernel, taken where the lower-triangle layout does not fit:
+  NRG_TRI_SYM=0;
+* the lower-triangle kernel on 16-block clusters: NRG_TRI_CLUSTER=16."""
 import os
 import subprocess
 import sys
@@ -19,5 +22,20 @@ def test_large_sectors_through_the_multi_kernel_tridiagonalisation():
     cmd = [sys.executable, "-m", "pytest", "-q", "-x", "-p", "no:cacheprovider",
            os.path.join(HERE, "test_gpu_parity.py") + "::test_large_sector_diagonalization[nkeep512]"]
     r = subprocess.run(cmd, env=env, cwd=os.path.dirname(HERE), capture_output=True, text=True, timeout=900)
+    assert r.returncode == 0, r.stdout[-3000:] + r.stderr[-3000:]
+    assert "1 passed" in r.stdout
+
+
+@pytest.mark.parametrize("env,case", [
+    ({"NRG_TRI_SYM": "0"}, "nkeep4096"),        # the full-column cluster kernel, 8 blocks
+    ({"NRG_TRI_CLUSTER": "16"}, "nkeep4096"),   # the lower-triangle kernel on 16-block clusters
+])
+def test_large_sectors_through_the_other_cluster_kernels(env, case):
+    # the default is the lower-triangle kernel on 8-block clusters; the N_keep = 4096 case
+    # reaches orders 1225 and 1308
+    cmd = [sys.executable, "-m", "pytest", "-q", "-x", "-p", "no:cacheprovider",
+           os.path.join(HERE, "test_gpu_parity.py") + f"::test_large_sector_diagonalization[{case}]"]
+    r = subprocess.run(cmd, env=dict(os.environ, **env), cwd=os.path.dirname(HERE), capture_output=True,
+                       text=True, timeout=900)
     assert r.returncode == 0, r.stdout[-3000:] + r.stderr[-3000:]
     assert "1 passed" in r.stdout
