@@ -33,6 +33,8 @@ second (60 per step), whole job.
 * fdm: that workload with the full-density-matrix spectrum and density matrices at
   T = 1e-6 (the workload table's temperature; no reference counterpart: the reference's
   spectrum is the T = 0 CFS one), one warm-up and two event-timed sweeps.
+* two_orbital_window: the two-orbital Hund model at N_keep = 8192 (16 local states),
+  iterations -1..3 of its chain (sectors of order up to ~8,800), forward sweep only.
 * many_instance: independent impurity models side by side (nrg_run_batch): the 27 draws
   with N_keep <= 1024 of the seeded 64-SIAM sweep (50 iterations each, T=0 CFS), run one
   at a time and then 8 in flight; wall clock around each batch with the device
@@ -79,6 +81,7 @@ def parse():
     p.add_argument("--no-fdm", action="store_true")
     p.add_argument("--no-nk2048", action="store_true")
     p.add_argument("--no-pageable", action="store_true")
+    p.add_argument("--no-two-orbital", action="store_true")
     p.add_argument("--e2e-steps", type=int, default=3)
     # profiling helpers: a shorter sweep of the same model (not the headline workload)
     p.add_argument("--iterations", type=int, default=None)
@@ -242,6 +245,36 @@ def second_workload(torch, dev, local, stream, fdm_temperature=None):
             out["temperature"] = T
             out["shell_trace_max_dev"] = float(np.nanmax(np.abs(r["rdmTrace"] - 1.0)))
         return out
+    finally:
+        c.close()
+
+
+def two_orbital_window(torch, dev, local, stream):
+    """The two-orbital Hund model at N_keep = 8192 (16 local states, sectors of order up to
+    ~8,800), its first 5 iterations (-1..3), forward sweep only: one warm-up and one
+    event-timed sweep; the context's storage is released afterwards."""
+    from nrg_b200 import Context, model
+    inp = model.config(4, n_iterations=5)
+    inp.flag_spectrum = False
+    n_it = inp.numberOfIteration - inp.indexOfFirstIteration + 1
+    c = Context(local)
+    try:
+        c.set_model(inp)
+        c.set_stream(stream.cuda_stream)
+        c.run(spectrum=False)
+        torch.cuda.synchronize(dev)
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s.record(stream)
+        r = c.run(spectrum=False)
+        e.record(stream)
+        torch.cuda.synchronize(dev)
+        ms = s.elapsed_time(e)
+        return {"workload": "two-orbital Hund model U=0.2 J=0.02 Gamma=0.015 Lambda=3 N_keep=8192, iterations "
+                            "-1..3 (a window of the 40-iteration chain), forward sweep only",
+                "ms_per_window": ms, "iterations_per_s": n_it * 1e3 / ms,
+                "kept": [int(k) for k in r["kept"]],
+                "states_before_truncation": [int(k) for k in r["numberOfBasisFull"]],
+                "timing": "CUDA events on the library's stream, 1 window after 1 warm-up"}
     finally:
         c.close()
 
@@ -428,6 +461,7 @@ def main():
     nk2048 = None if args.no_nk2048 else second_workload(torch, dev, local, stream)
     fdm = None if args.no_fdm else second_workload(torch, dev, local, stream, fdm_temperature=1e-6)
     many = None if args.no_many else many_instance(torch, dev, rank, world, dist)
+    two = None if args.no_two_orbital else two_orbital_window(torch, dev, local, stream)
     if rank == 0:
         clocks = clk.summary()
         nbin = res["numberOfBin"]
@@ -484,6 +518,7 @@ def main():
             "n_keep_2048": nk2048,
             "fdm": fdm,
             "many_instance": many,
+            "two_orbital_window": two,
         }
         print(json.dumps(line), flush=True)
     ctx.close()

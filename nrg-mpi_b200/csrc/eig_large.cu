@@ -537,33 +537,50 @@ __global__ void __launch_bounds__(TT, 1) k_tri_cluster(const LSec* __restrict__ 
 //                                             triangle read as the transpose)
 // and every block sends the z of each row to the block that owns the row, in the same
 // cluster exchange that carries the panel dot products; y(l) = dot(l) + the received z.
-// Half the bytes of the product and of the panel update cross from L2.  The panel rows of
-// column p+q (needed as own rows of the column) are read from the column itself (rows at
-// stride CL), since the upper triangle is stale.  The product is split into work items of
-// 256 rows x CRW own columns; each item leaves its column dot products in ysp (per row
-// batch) and its row sums in zsp (per column range), and both are added in a fixed order,
-// so results do not depend on the schedule.
-constexpr int SRB = 256;   // rows per work item of the symmetric product
-
+// Half the bytes of the product and of the panel update cross from L2.
+// Work split of the product: the trailing rows form blocks of 32; each warp takes whole
+// row blocks (dealt heaviest first, in snake order, so the warps' loads balance), one row
+// per lane, and walks the own columns that reach the block in tiles of 32: the loads are
+// coalesced along the rows, z of the lane's row stays in a register across the tiles, and
+// the 32 column dot products of a tile are summed over the lanes by a transposed
+// butterfly (31 shuffles; lane j ends with column j).  Each warp adds its column partials
+// into its own row of ysp, and the warps' partials are added in warp order, so results do
+// not depend on the schedule.
+// The panel rows of column p+q (needed as own rows of the column) are read from the column
+// itself (rows at stride CL), since the upper triangle is stale.
 struct TriLayoutS {
-    int MM, PN, NRB, NCR, CRW;   // own indices per block, rows (even), row batches, column ranges
+    int MM, PN;   // own indices per block, rows (even)
     __host__ __device__ long long doubles(int CL) const {
-        const long long stage = (long long)NB * MM > 2LL * NB * 64 ? (long long)NB * MM : 2LL * NB * 64;
+        const long long stage = (long long)NB * MM > 2LL * NB * TRW ? (long long)NB * MM : 2LL * NB * TRW;
         return 2LL * NB * MM + PN + MM + (long long)CL * P2W + CL + 2 + 2LL * NB + 2LL * NB + P2W + 32 +
-               stage + (long long)NRB * MM + (long long)NCR * PN + (long long)CL * MM + 3LL * NB;
+               stage + (long long)(TT / 32) * MM + (long long)CL * MM + 3LL * NB;
     }
 };
+
+// v[0..31] of every lane summed over the warp: lane j returns the sum of v[j]
+__device__ __forceinline__ double transpose_sum32(double (&v)[32], int lane) {
+#pragma unroll
+    for (int o = 16; o >= 1; o >>= 1) {
+        const bool upper = (lane & o) != 0;
+#pragma unroll
+        for (int i = 0; i < o; ++i) {
+            const double send = upper ? v[i] : v[i + o];
+            const double keep = upper ? v[i + o] : v[i];
+            v[i] = keep + __shfl_xor_sync(0xffffffffu, send, o);
+        }
+    }
+    return v[0];
+}
 
 template <int CL>
 __global__ void __launch_bounds__(TT, 1) k_tri_csym(const LSec* __restrict__ secs, TriLayoutS lay,
                                                    double* eigbuf, double* wsd, int* wsi) {
-    constexpr int TRS = 64;   // rows per staged chunk of the panel update
     extern __shared__ double sm[];
     cg::cluster_group cluster = cg::this_cluster();
     const int rank = (int)cluster.block_rank();
     const LSec sec = secs[blockIdx.x / CL];
     LView L = lview(sec, eigbuf, wsd, wsi);
-    const int n = L.n, MM = lay.MM, PN = lay.PN, CRW = lay.CRW;
+    const int n = L.n, MM = lay.MM, PN = lay.PN;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     constexpr int NW = TT / 32;
     double* VO = sm;                       // NB x MM: V(own row m, q) at q*MM + m
@@ -578,26 +595,29 @@ __global__ void __launch_bounds__(TT, 1) k_tri_csym(const LSec* __restrict__ sec
     double* tsum = piv + 2 * NB;           // t1 | t2 | y.v
     double* red = tsum + P2W;              // 32
     double* AR = red + 32;                 // NB x MM: A(own row m, p + q), during the columns
-    double* stV = AR;                      // NB x TRS staged rows of V (transposed), panel update
-    double* stW = stV + NB * TRS;          // NB x TRS
-    double* ysp = AR + ((size_t)NB * MM > 2 * NB * TRS ? (size_t)NB * MM : 2 * NB * TRS);   // NRB x MM
-    double* zsp = ysp + (size_t)lay.NRB * MM;   // NCR x PN row sums per column range
-    double* zr = zsp + (size_t)lay.NCR * PN;    // CL x MM: z of the own rows, by source block
+    double* stV = AR;                      // NB x TRW staged rows of V (transposed), panel update
+    double* stW = stV + NB * TRW;          // NB x TRW
+    double* ysp = AR + ((size_t)NB * MM > 2 * NB * TRW ? (size_t)NB * MM : 2 * NB * TRW);   // NW x MM
+    double* zr = ysp + (size_t)NW * MM;         // CL x MM: z of the own rows, by source block
     double* pan = zr + (size_t)CL * MM;         // D | E | tau of the panel's columns
     double* Vg = L.VW;
     double* Wg = L.VW + (size_t)NB * n;
     double* A = L.A;
     const int cnt = (n - rank + CL - 1) / CL;                           // own indices rank + CL*m
     auto first_own = [&](int i0) { return (i0 - rank + CL - 1) / CL; };  // i0 >= 0
+    (void)PN;
 
     for (int p = 0; p < n - 1; p += NB) {
         const int last = min(p + NB - 1, n - 2);
         const int jn = last - p + 1;
         // own rows i >= p + q of the panel's columns p + q (lower triangle, stride CL)
-        for (int q = 0; q < jn; ++q) {
-            const int m0 = first_own(p + q);
-            for (int m = m0 + tid; m < cnt; m += TT)
-                AR[q * MM + m] = __ldcg(A + (size_t)(rank + CL * m) + (size_t)(p + q) * n);
+        {
+            const int m0 = first_own(p);
+            const int nm = cnt - m0;
+            for (int e = tid; e < jn * nm; e += TT) {
+                const int q = e / nm, m = m0 + e % nm, i = rank + CL * m;
+                if (i >= p + q) AR[q * MM + m] = __ldcg(A + (size_t)i + (size_t)(p + q) * n);
+            }
         }
         __syncthreads();
         for (int k = p; k <= last; ++k) {
@@ -641,10 +661,11 @@ __global__ void __launch_bounds__(TT, 1) k_tri_csym(const LSec* __restrict__ sec
             for (int r = k + 2 + tid; r < n; r += TT) cv[r] = xn2 == 0.0 ? 0.0 : cv[r] * scal;
             if (act && i >= k + 1) VO[j * MM + m] = (i == k + 1) ? 1.0 : (xn2 == 0.0 ? 0.0 : c * scal);
             if (tid == 0) { pan[NB + j] = beta; pan[2 * NB + j] = tau; }
+            const int mB = first_own(k + 1);
+            for (int mm = mB + lane; mm < cnt; mm += 32) ysp[warp * MM + mm] = 0.0;
             __syncthreads();
             // ---- B: partial W^T v, V^T v over the own rows, the next pivot row, the
             // lower-triangle product, z to the row owners, partial y.v ----
-            const int mB = first_own(k + 1);
             const double* vj = VO + j * MM;
             for (int o = warp; o < 2 * j; o += NW) {
                 const double* colp = (o < j) ? WO + o * MM : VO + (o - j) * MM;
@@ -661,86 +682,56 @@ __global__ void __launch_bounds__(TT, 1) k_tri_csym(const LSec* __restrict__ sec
                     cluster.map_shared_rank(pivn, r)[q < j ? q : NB + (q - j)] = val;
                 }
             }
-            const int nrows = n - k - 1;
-            const int nrb = (nrows + SRB - 1) / SRB;
-            const int ncr = (cnt - mB + CRW - 1) / CRW;
-            // an item (row batch rb, column range cr) holds work when the range's first
-            // column is not below the batch's last row
-            auto item_live = [&](int rb, int cr) {
-                const int lastrow = min(k + 1 + (rb + 1) * SRB, n) - 1;
-                return rank + CL * (mB + cr * CRW) <= lastrow;
-            };
-            for (int item = warp; item < nrb * ncr; item += NW) {
-                const int rb = item / ncr, cr = item % ncr;
-                if (!item_live(rb, cr)) continue;
-                const int rbase = k + 1 + rb * SRB;
-                const int mEnd = min(cnt, mB + (cr + 1) * CRW);
-                const int row0 = rbase + lane;
-                double xv[8], z[8];
+            double yvp = 0.0;   // this block's part of v^T A v
+            {
+                const int nblk = (n - k - 1 + 31) / 32;
+                double* yw = ysp + (size_t)warp * MM;
+                for (int pass = 0; pass * NW < nblk; ++pass) {
+                    const int slot = (pass & 1) ? NW - 1 - warp : warp;
+                    const int qi = pass * NW + slot;
+                    if (qi >= nblk) continue;
+                    const int b = nblk - 1 - qi;            // heaviest (lowest) blocks first
+                    const int r0b = k + 1 + 32 * b;
+                    const int r = r0b + lane;
+                    const double vr = r < n ? (r == k + 1 ? 1.0 : cv[r]) : 0.0;   // v(k+1) = 1
+                    const int lastrow = min(r0b + 31, n - 1);
+                    const int mLim = min(cnt, (lastrow - rank) / CL + 1);   // own columns l <= lastrow
+                    double z = 0.0;
+                    for (int t0 = mB; t0 < mLim; t0 += 32) {
+                        double d[32];
 #pragma unroll
-                for (int u = 0; u < 8; ++u) {
-                    const int r = row0 + 32 * u;
-                    xv[u] = r < n ? (r == k + 1 ? 1.0 : cv[r]) : 0.0;
-                    z[u] = 0.0;
-                }
-                for (int m0 = mB + cr * CRW; m0 < mEnd; m0 += 4) {
-                    int col[4];
-                    double vc[4];
+                        for (int jj = 0; jj < 32; ++jj) {
+                            const int mc = t0 + jj;
+                            const int l = rank + CL * mc;
+                            d[jj] = (mc < mLim && r < n && r >= l) ? A[(size_t)l * n + r] : 0.0;
+                        }
 #pragma unroll
-                    for (int c = 0; c < 4; ++c) {
-                        col[c] = (m0 + c < mEnd) ? rank + CL * (m0 + c) : n;   // n: no column
-                        vc[c] = (m0 + c < mEnd) ? (col[c] == k + 1 ? 1.0 : cv[col[c]]) : 0.0;
+                        for (int jj = 0; jj < 32; ++jj) {
+                            const int mc = t0 + jj;
+                            const int l = rank + CL * mc;
+                            const double x = d[jj];
+                            if (mc < mLim && r > l) z = fma(x, l == k + 1 ? 1.0 : cv[l], z);
+                            d[jj] = x * vr;
+                        }
+                        const double dsum = transpose_sum32(d, lane);
+                        if (t0 + lane < mLim) yw[t0 + lane] += dsum;
                     }
-                    double x[4][8];
-#pragma unroll
-                    for (int u = 0; u < 8; ++u)
-#pragma unroll
-                        for (int c = 0; c < 4; ++c) {
-                            const int r = row0 + 32 * u;
-                            x[c][u] = (r < n && r >= col[c]) ? A[(size_t)col[c] * n + r] : 0.0;
-                        }
-                    double sc[4] = {0.0, 0.0, 0.0, 0.0};
-#pragma unroll
-                    for (int u = 0; u < 8; ++u)
-#pragma unroll
-                        for (int c = 0; c < 4; ++c) {
-                            sc[c] = fma(x[c][u], xv[u], sc[c]);
-                            if (row0 + 32 * u > col[c]) z[u] = fma(x[c][u], vc[c], z[u]);
-                        }
-#pragma unroll
-                    for (int c = 0; c < 4; ++c) sc[c] = warp_sum(sc[c]);
-                    if (lane == 0)
-#pragma unroll
-                        for (int c = 0; c < 4; ++c)
-                            if (m0 + c < mEnd) ysp[rb * MM + m0 + c] = sc[c];
+                    if (r < n) {
+                        cluster.map_shared_rank(zr, r % CL)[rank * MM + r / CL] = z;
+                        yvp = fma(vr, z, yvp);
+                    }
                 }
-#pragma unroll
-                for (int u = 0; u < 8; ++u)
-                    if (row0 + 32 * u < n) zsp[cr * PN + row0 + 32 * u] = z[u];
             }
             __syncthreads();
-            // row sums of z (fixed order over the live ranges) to the rows' owners, and this
-            // block's part of v^T A v: sum over own columns of v(l) dot(l) plus sum over all
-            // rows of v(i) z(i)
-            double yvp = 0.0;
-            for (int r = k + 1 + tid; r < n; r += TT) {
-                const int rb = (r - k - 1) / SRB;
-                double zt = 0.0;
-                for (int cr = 0; cr < ncr; ++cr)
-                    if (item_live(rb, cr)) zt += zsp[cr * PN + r];
-                cluster.map_shared_rank(zr, r % CL)[rank * MM + r / CL] = zt;
-                yvp = fma(r == k + 1 ? 1.0 : cv[r], zt, yvp);
-            }
             const int mc = mB + tid;
             const bool own_c = mc < cnt;
-            double dot = 0.0;
             if (own_c) {
-                const int l = rank + CL * mc;
-                for (int rb = (l - k - 1) / SRB; rb < nrb; ++rb) dot += ysp[rb * MM + mc];
+                double dot = 0.0;
+                for (int w = 0; w < NW; ++w) dot += ysp[w * MM + mc];
                 ys[mc] = dot;
                 yvp = fma(vj[mc], dot, yvp);
                 // y(k+1) has no z part (no own column lies left of it in the trailing block)
-                if (pivot_owner && k + 1 <= last && l == k + 1)
+                if (pivot_owner && k + 1 <= last && rank + CL * mc == k + 1)
                     for (int r = 0; r < CL; ++r) cluster.map_shared_rank(Y1, r)[0] = dot;
             }
             yvp = block_sum(yvp, red);
@@ -805,54 +796,55 @@ __global__ void __launch_bounds__(TT, 1) k_tri_csym(const LSec* __restrict__ sec
         cluster.sync();
         const int mR = first_own(r0);
         const int tr = tid & 31, tc = tid >> 5;
-        for (int ib = r0; ib < n; ib += TRS) {
-            // own columns that reach this chunk: rank + CL*m <= ib + TRS - 1
-            const int lastrow = min(ib + TRS, n) - 1;
+        for (int ib = r0; ib < n; ib += TRW) {
+            // own columns that reach this chunk: rank + CL*m <= its last row
+            const int lastrow = min(ib + TRW, n) - 1;
             const int mLim = lastrow >= rank ? min(cnt, (lastrow - rank) / CL + 1) : 0;
             if (mLim <= mR) continue;   // no own column reaches this chunk yet (uniform in the block)
-            for (int e = tid; e < jc * TRS; e += TT) {
-                const int q = e / TRS, r = e % TRS, row = ib + r;
-                stV[q * TRS + r] = row < n ? __ldcg(Vg + row + (size_t)q * n) : 0.0;
-                stW[q * TRS + r] = row < n ? __ldcg(Wg + row + (size_t)q * n) : 0.0;
+            for (int e = tid; e < jc * TRW; e += TT) {
+                const int q = e / TRW, rr = e % TRW, row = ib + rr;
+                stV[q * TRW + rr] = row < n ? __ldcg(Vg + row + (size_t)q * n) : 0.0;
+                stW[q * TRW + rr] = row < n ? __ldcg(Wg + row + (size_t)q * n) : 0.0;
             }
             __syncthreads();
-            for (int mc = mR; mc < mLim; mc += 4 * (TT / 32)) {
-                const int m0 = mc + 4 * tc;
+            for (int mc2 = mR; mc2 < mLim; mc2 += 4 * (TT / 32)) {
+                const int m0 = mc2 + 4 * tc;
                 if (m0 < mLim) {
                     int mcol[4];
 #pragma unroll
-                    for (int c = 0; c < 4; ++c) mcol[c] = min(m0 + c, mLim - 1);
-                    double acc[2][4];
+                    for (int cc = 0; cc < 4; ++cc) mcol[cc] = min(m0 + cc, mLim - 1);
+                    double acc[4][4];
 #pragma unroll
-                    for (int u = 0; u < 2; ++u)
+                    for (int u = 0; u < 4; ++u)
 #pragma unroll
-                        for (int c = 0; c < 4; ++c) acc[u][c] = 0.0;
+                        for (int cc = 0; cc < 4; ++cc) acc[u][cc] = 0.0;
                     for (int q = 0; q < jc; ++q) {
-                        double av[2], aw[2], bw[4], bv[4];
+                        double av[4], aw[4], bw[4], bv[4];
 #pragma unroll
-                        for (int u = 0; u < 2; ++u) {
-                            av[u] = stV[q * TRS + tr + 32 * u];
-                            aw[u] = stW[q * TRS + tr + 32 * u];
+                        for (int u = 0; u < 4; ++u) {
+                            av[u] = stV[q * TRW + tr + 32 * u];
+                            aw[u] = stW[q * TRW + tr + 32 * u];
                         }
 #pragma unroll
-                        for (int c = 0; c < 4; ++c) {
-                            bw[c] = WO[q * MM + mcol[c]];
-                            bv[c] = VO[q * MM + mcol[c]];
+                        for (int cc = 0; cc < 4; ++cc) {
+                            bw[cc] = WO[q * MM + mcol[cc]];
+                            bv[cc] = VO[q * MM + mcol[cc]];
                         }
 #pragma unroll
-                        for (int u = 0; u < 2; ++u)
+                        for (int u = 0; u < 4; ++u)
 #pragma unroll
-                            for (int c = 0; c < 4; ++c) acc[u][c] = fma(av[u], bw[c], fma(aw[u], bv[c], acc[u][c]));
+                            for (int cc = 0; cc < 4; ++cc)
+                                acc[u][cc] = fma(av[u], bw[cc], fma(aw[u], bv[cc], acc[u][cc]));
                     }
 #pragma unroll
-                    for (int c = 0; c < 4; ++c) {
-                        if (m0 + c >= mLim) continue;
-                        const int l = rank + CL * (m0 + c);
+                    for (int cc = 0; cc < 4; ++cc) {
+                        if (m0 + cc >= mLim) continue;
+                        const int l = rank + CL * (m0 + cc);
                         double* colp = A + (size_t)l * n;
 #pragma unroll
-                        for (int u = 0; u < 2; ++u) {
+                        for (int u = 0; u < 4; ++u) {
                             const int row = ib + tr + 32 * u;
-                            if (row < n && row >= l) colp[row] -= acc[u][c];
+                            if (row < n && row >= l) colp[row] -= acc[u][cc];
                         }
                     }
                 }
@@ -1307,17 +1299,9 @@ static int tri_csym_cl(nrg_context* ctx, const LSec* dsec, int ns, int maxn, dou
     TriLayoutS lay;
     lay.MM = (maxn + CL - 1) / CL;
     lay.PN = maxn + (maxn & 1);
-    lay.NRB = (maxn + SRB - 1) / SRB;
     if (lay.MM > TT) return NRG_OK;
-    size_t smem = 0;
-    bool fits = false;
-    for (int crw : {32, 48, 64, 96, 128}) {
-        lay.CRW = crw;
-        lay.NCR = (lay.MM + crw - 1) / crw;
-        smem = sizeof(double) * (size_t)lay.doubles(CL);
-        if (smem <= (size_t)optin) { fits = true; break; }
-    }
-    if (!fits) return NRG_OK;
+    const size_t smem = sizeof(double) * (size_t)lay.doubles(CL);
+    if (smem > (size_t)optin) return NRG_OK;
     NRG_TRY(raise_smem_limit((const void*)k_tri_csym<CL>, smem));
     if (CL > 8) NRG_CUDA_TRY(cudaFuncSetAttribute(k_tri_csym<CL>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
     cudaLaunchConfig_t cfg = {};
@@ -1370,6 +1354,12 @@ static int tri_cluster(nrg_context* ctx, const LSec* dsec, int ns, int maxn, dou
     if (sym && cl == 8) {
         NRG_TRY(tri_csym_cl<8>(ctx, dsec, ns, maxn, d_V, wsd, wsi, done));
         if (*done) return NRG_OK;
+        // orders whose 8-block layout does not fit (above ~1,500) fit on 16-block clusters
+        // up to ~2,300
+        if (forced < 0) {
+            NRG_TRY(tri_csym_cl<16>(ctx, dsec, ns, maxn, d_V, wsd, wsi, done));
+            if (*done) return NRG_OK;
+        }
     }
     if (cl == 16) {
         NRG_TRY(tri_cluster_cl<16>(ctx, dsec, ns, maxn, d_V, wsd, wsi, done));
