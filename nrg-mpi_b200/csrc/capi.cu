@@ -94,7 +94,6 @@ nrg_context::~nrg_context() {
             cudaEventDestroy(t.b);
         }
     if (stage_host) cudaFreeHost(stage_host);
-    gemm_tuner.release();
 }
 
 using namespace nrg;

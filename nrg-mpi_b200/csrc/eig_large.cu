@@ -1331,8 +1331,10 @@ static int tri_csym_cl(nrg_context* ctx, const LSec* dsec, int ns, int maxn, dou
 // largest size class alone halves its per-block product but costs as much in the wider
 // exchanges: no net gain measured); a size that cannot be placed falls back to the next
 // smaller one.  The environment variable NRG_TRI_CLUSTER forces 4, 8 or 16, or 0 for the
-// multi-kernel path.  The lower-triangle kernel is taken for 8 or 16 blocks when its
-// layout fits; NRG_TRI_SYM=0 keeps the full-column kernel.
+// multi-kernel path.  NRG_TRI_SYM=1 takes the lower-triangle kernel (8 or 16 blocks) when
+// its layout fits: it moves half the bytes but measured slower on the bench workloads
+// (23.8 against 16.3 ms per launch at N_keep = 4096: more time at the barriers per column),
+// so the full-column kernel is the default.
 static int tri_cluster(nrg_context* ctx, const LSec* dsec, int ns, int maxn, double* d_V, double* wsd,
                        int* wsi, bool* done) {
     static const int forced = [] {
@@ -1343,7 +1345,7 @@ static int tri_cluster(nrg_context* ctx, const LSec* dsec, int ns, int maxn, dou
     }();
     static const bool sym = [] {
         const char* e = getenv("NRG_TRI_SYM");
-        return !(e && e[0] == '0');
+        return e && e[0] == '1';
     }();
     *done = false;
     const int cl = forced >= 0 ? forced : kTriCL;

@@ -19,6 +19,8 @@
 
 #include <algorithm>
 #include <cstdlib>
+#include <map>
+#include <mutex>
 
 namespace nrg {
 namespace {
@@ -215,10 +217,10 @@ int log2_bucket(long long v) {
 
 }  // namespace
 
-// Online tuning of the tile shape.  Launches are keyed by their problem mix (log2 buckets
-// of the median M, N, K and of the problem count); the first launches of a key try each
-// tile variant in turn, timed by events on the context's stream, and later launches of
-// the key take the variant with the least time per flop.  Timings are read without
+// Online tuning of the tile shape, per device.  Launches are keyed by their problem mix
+// (log2 buckets of the median M, N, K and of the problem count); the first launches of a
+// key try each tile variant in turn, timed by events on the launching stream, and later
+// launches of the key take the variant with the least time per flop.  Timings are read without
 // waiting: a pending measurement is collected by a later launch once its events have
 // completed.  The variants give bit-identical results, so the choice never changes a
 // result.  NRG_GGEMM_VARIANT=0..3 fixes one variant (no tuning).
@@ -262,15 +264,15 @@ void GemmTuner::collect(bool wait) {
     }
 }
 
-void GemmTuner::release() {
-    for (auto& q : pending) {
-        cudaEventSynchronize(q.b);
-        cudaEventDestroy(q.a);
-        cudaEventDestroy(q.b);
-    }
-    pending.clear();
-    for (cudaEvent_t e : free_events) cudaEventDestroy(e);
-    free_events.clear();
+// one tuner per device, shared by every context on it (independent instances side by side
+// tune once between them); its state is guarded by its mutex
+GemmTuner& tuner_for(int dev) {
+    static std::mutex mu;
+    static std::map<int, GemmTuner*> tuners;
+    std::lock_guard<std::mutex> lk(mu);
+    GemmTuner*& t = tuners[dev];
+    if (!t) t = new GemmTuner();   // lives until the process exits
+    return *t;
 }
 
 int launch_ggemm(nrg_context* ctx, std::vector<GemmProblem>& probs, int scratch_slot) {
@@ -296,7 +298,10 @@ int launch_ggemm(nrg_context* ctx, std::vector<GemmProblem>& probs, int scratch_
     };
     const unsigned key = (unsigned)(log2_bucket(med(ms)) | log2_bucket(med(ns)) << 4 | log2_bucket(med(ks)) << 8 |
                                     log2_bucket(np) << 12);
-    GemmTuner& tu = ctx->gemm_tuner;
+    int dev = 0;
+    NRG_CUDA_TRY(cudaGetDevice(&dev));
+    GemmTuner& tu = tuner_for(dev);
+    std::unique_lock<std::mutex> lk(tu.mu);
     tu.collect(false);
     const int v = tu.pick(key);
     DevBuf& dp = ctx->scratch.b[scratch_slot];
@@ -311,8 +316,10 @@ int launch_ggemm(nrg_context* ctx, std::vector<GemmProblem>& probs, int scratch_
     if (timed) {
         NRG_TRY(tu.event(&ea));
         NRG_TRY(tu.event(&eb));
-        NRG_CUDA_TRY(cudaEventRecord(ea, ctx->stream));
+        tu.table[key].inflight[v]++;   // claimed before the lock is released
     }
+    lk.unlock();
+    if (timed) NRG_CUDA_TRY(cudaEventRecord(ea, ctx->stream));
     int rc = NRG_OK;
     switch (v) {
         case 0: rc = launch_variant<kWM[0], kWN[0]>(ctx, 0, dp.as<GemmProblem>(), dq.as<int>(), np, live, prefix, dq); break;
@@ -321,11 +328,12 @@ int launch_ggemm(nrg_context* ctx, std::vector<GemmProblem>& probs, int scratch_
         default: rc = launch_variant<kWM[3], kWN[3]>(ctx, 0, dp.as<GemmProblem>(), dq.as<int>(), np, live, prefix, dq); break;
     }
     if (timed) {
-        if (rc == NRG_OK) {
-            NRG_CUDA_TRY(cudaEventRecord(eb, ctx->stream));
-            tu.table[key].inflight[v]++;
+        const bool rec = rc == NRG_OK && cudaEventRecord(eb, ctx->stream) == cudaSuccess;
+        lk.lock();
+        if (rec) {
             tu.pending.push_back({key, v, ea, eb, gflop});
         } else {
+            tu.table[key].inflight[v]--;
             tu.free_events.push_back(ea);
             tu.free_events.push_back(eb);
         }

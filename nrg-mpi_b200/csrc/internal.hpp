@@ -7,6 +7,7 @@
 #include <vector>
 #include <map>
 #include <deque>
+#include <mutex>
 #include <unordered_map>
 
 namespace nrg {
@@ -99,7 +100,7 @@ struct Scratch {
 }  // namespace nrg
 
 namespace nrg {
-// per-context choice of the grouped GEMM's tile shape (ggemm.cu)
+// per-device choice of the grouped GEMM's tile shape (ggemm.cu)
 struct GemmTuner {
     static constexpr int kTunedVariants = 4, kSamples = 2;
     struct Entry {
@@ -113,12 +114,12 @@ struct GemmTuner {
         cudaEvent_t a, b;
         double gflop;
     };
+    std::mutex mu;
     std::unordered_map<unsigned, Entry> table;
     std::vector<Pending> pending;
     std::vector<cudaEvent_t> free_events;
     int pick(unsigned key);
     void collect(bool wait);
-    void release();
     int event(cudaEvent_t* e);
 };
 }  // namespace nrg
@@ -132,7 +133,6 @@ struct nrg_context {
     long long launches = 0;
     // measurement counters (nrg_context_get_stats)
     bool profiling = false;
-    nrg::GemmTuner gemm_tuner;   // tile shape of the grouped GEMM per problem mix
     long long syev_launches = 0;
     double syev_ms = 0.0, syev_flops = 0.0;
     long long h2d = 0, d2h = 0;

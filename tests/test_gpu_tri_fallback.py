@@ -1,11 +1,10 @@
-"""The tridiagonalisation paths other than the default one (the lower-triangle cluster
-kernel on 8-block clusters), each through the large-sector parity test re-run in a child
-process with the environment variable that selects it (read once per process):
+"""The tridiagonalisation paths other than the default one (the full-column cluster kernel
+on 8-block clusters), each through the large-sector parity test re-run in a child process
+with the environment variable that selects it (read once per process):
 * the multi-kernel path (two launches per column, then grouped-GEMM panel updates), which
   sectors too large for the cluster kernels' shared memory take: NRG_TRI_CLUSTER=0;
-* the full-column cluster kernel, taken where the lower-triangle layout does not fit:
-  NRG_TRI_SYM=0;
-* the lower-triangle kernel on 16-block clusters: NRG_TRI_CLUSTER=16."""
+* the lower-triangle cluster kernel on 8-block clusters: NRG_TRI_SYM=1;
+* the lower-triangle kernel on 16-block clusters: NRG_TRI_SYM=1 NRG_TRI_CLUSTER=16."""
 import os
 import subprocess
 import sys
@@ -27,12 +26,11 @@ def test_large_sectors_through_the_multi_kernel_tridiagonalisation():
 
 
 @pytest.mark.parametrize("env,case", [
-    ({"NRG_TRI_SYM": "0"}, "nkeep4096"),        # the full-column cluster kernel, 8 blocks
-    ({"NRG_TRI_CLUSTER": "16"}, "nkeep4096"),   # the lower-triangle kernel on 16-block clusters
+    ({"NRG_TRI_SYM": "1"}, "nkeep4096"),                            # lower triangle, 8 blocks
+    ({"NRG_TRI_SYM": "1", "NRG_TRI_CLUSTER": "16"}, "nkeep4096"),   # lower triangle, 16 blocks
 ])
 def test_large_sectors_through_the_other_cluster_kernels(env, case):
-    # the default is the lower-triangle kernel on 8-block clusters; the N_keep = 4096 case
-    # reaches orders 1225 and 1308
+    # the N_keep = 4096 case reaches orders 1225 and 1308
     cmd = [sys.executable, "-m", "pytest", "-q", "-x", "-p", "no:cacheprovider",
            os.path.join(HERE, "test_gpu_parity.py") + f"::test_large_sector_diagonalization[{case}]"]
     r = subprocess.run(cmd, env=dict(os.environ, **env), cwd=os.path.dirname(HERE), capture_output=True,
