@@ -145,9 +145,47 @@ int stage_in(nrg_context* ctx, const T* p, size_t n, size_t slot, const T** out)
     return NRG_OK;
 }
 
+constexpr size_t kSlotIO = 100000;   // drop-in staging slots
+
 // stage_in for an input of which the routine reads only the listed runs: pinned host
 // memory is read run by run by a kernel (only those bytes cross the host link, the
-// rest of the device copy is never read); pageable memory is copied whole
+// rest of the device copy is never read); from pageable memory the runs are gathered on
+// the host into a page-locked buffer, copied in one piece and scattered to their places
+// on the device (the whole array is copied instead when the runs are most of it)
+int stage_in_pageable_segs(nrg_context* ctx, const double* p, size_t n, long long ld,
+                           const std::vector<HostSeg>& segs, size_t slot, const double** out) {
+    long long total = 0;
+    for (const auto& g : segs) total += (long long)g.len * g.count;
+    if (total == 0 || 2 * total > (long long)n) return stage_in(ctx, p, n, slot, out);
+    for (const auto& g : segs)
+        if (g.len < 0 || g.count < 0 || g.off < 0 || g.off + (long long)(g.count - 1) * ld + g.len > (long long)n) {
+            nrg_set_error_message("segment outside the input array");
+            return NRG_ERR_INVALID;
+        }
+    HostBuf& h = ctx->seg_slot(slot - kSlotIO);
+    NRG_TRY(h.ensure(sizeof(double) * (size_t)total));
+    double* pk = h.as<double>();
+    long long at = 0;
+    for (const auto& g : segs)
+        for (int r = 0; r < g.count; ++r) {
+            std::memcpy(pk + at, p + g.off + (long long)r * ld, sizeof(double) * (size_t)g.len);
+            at += g.len;
+        }
+    DevBuf& b = ctx->slot(slot);
+    DevBuf& bp = ctx->slot(slot + 50000);
+    NRG_TRY(b.ensure(sizeof(double) * n));
+    NRG_TRY(bp.ensure(sizeof(double) * (size_t)total));
+    NRG_CUDA_TRY(cudaMemcpyAsync(bp.p, pk, sizeof(double) * (size_t)total, cudaMemcpyHostToDevice, ctx->stream));
+    long long bytes = 0;
+    NRG_TRY(run_gather_segs(ctx, bp.as<double>(), b.as<double>(), ld, segs, &bytes, true));
+    ctx->h2d += bytes;
+    *out = b.as<double>();
+    // the page-locked buffer is rewritten by the next call on this slot: the copy must
+    // have left it (the drop-in entries drain the stream before they return as well)
+    NRG_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+    return NRG_OK;
+}
+
 int stage_in_segs(nrg_context* ctx, const double* p, size_t n, long long ld, const std::vector<HostSeg>& segs,
                   size_t slot, const double** out) {
     if (n == 0) { *out = nullptr; return NRG_OK; }
@@ -155,10 +193,10 @@ int stage_in_segs(nrg_context* ctx, const double* p, size_t n, long long ld, con
     cudaPointerAttributes a;
     if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
         cudaGetLastError();
-        return stage_in(ctx, p, n, slot, out);
+        return stage_in_pageable_segs(ctx, p, n, ld, segs, slot, out);
     }
     if (a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged) { *out = p; return NRG_OK; }
-    if (a.type != cudaMemoryTypeHost || !a.devicePointer) return stage_in(ctx, p, n, slot, out);
+    if (a.type != cudaMemoryTypeHost || !a.devicePointer) return stage_in_pageable_segs(ctx, p, n, ld, segs, slot, out);
     DevBuf& b = ctx->slot(slot);
     NRG_TRY(b.ensure(sizeof(double) * n));
     long long bytes = 0;
@@ -214,7 +252,6 @@ int up(DevBuf& b, const std::vector<T>& v, cudaStream_t st) {
     return NRG_OK;
 }
 
-constexpr size_t kSlotIO = 100000;   // drop-in staging slots
 
 }  // namespace
 

@@ -1134,7 +1134,11 @@ __global__ void __launch_bounds__(256) k_bt_prep(const LSec* __restrict__ secs, 
 template <int CBK>
 __global__ void __launch_bounds__(256, 1) k_bt_apply(const LSec* __restrict__ secs, int nsec, double* eigbuf,
                                                      double* wsd, int* wsi) {
-    constexpr int JPT = CBK / 4;       // columns per thread
+    // The three small products of each panel, W = V^T Z, W2 = T W and Z -= V W2, on the
+    // FP64 tensor pipe (mma.sync m8n8k4): the eight warps split the panel's 64 reflectors
+    // (W, W2) or the chunk's 64 rows (the update) in slices of 8, and each warp covers the
+    // CBK columns in tiles of 8.
+    constexpr int NTJ = CBK / 8;
     extern __shared__ double asm_[];
     int bid = blockIdx.x, s = 0;
     for (; s < nsec; ++s) {
@@ -1151,21 +1155,23 @@ __global__ void __launch_bounds__(256, 1) k_bt_apply(const LSec* __restrict__ se
     double* Ws = Vs + NBB * 65;             // Ws[c * CBK + j]
     double* W2 = Ws + NBB * CBK;
     double* Ts = W2 + NBB * CBK;            // T column-major
-    const int tid = threadIdx.x, cl = tid & 63, jg = tid >> 6;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int g = lane >> 2, q4 = lane & 3;
+    const int wr = 8 * warp;                // this warp's slice of reflectors / rows
     for (int j = 0; j < CBK; ++j)
         for (int row = tid; row < n; row += 256)
             Zs[(size_t)j * n + row] = j < nc ? L.Z[(size_t)row + (size_t)(c0 + j) * n] : 0.0;
     const int qmax = (n - 2) / NBB;
     for (int q = qmax; q >= 0; --q) {
-        const int jb = q * NBB, b = min(NBB, nr - jb), r0 = jb + 1, mr = n - r0;
-        (void)b;
+        const int jb = q * NBB, r0 = jb + 1, mr = n - r0;
+        (void)nr;
         const double* Rp = L.R + bt_panel_off(n, q);
         const double* Tq = L.R + (size_t)q * NBB * NBB;
         for (int e = tid; e < NBB * NBB; e += 256) Ts[e] = Tq[e];
-        // W = V^T Z(r0:, :)
-        double acc[JPT];
+        // W = V^T Z(r0:, :): W(i, j) for the warp's reflectors i
+        double acc[NTJ][2];
 #pragma unroll
-        for (int u = 0; u < JPT; ++u) acc[u] = 0.0;
+        for (int t = 0; t < NTJ; ++t) acc[t][0] = acc[t][1] = 0.0;
         for (int i0 = 0; i0 < mr; i0 += 64) {
             const int rows = min(64, mr - i0);
             __syncthreads();
@@ -1175,26 +1181,38 @@ __global__ void __launch_bounds__(256, 1) k_bt_apply(const LSec* __restrict__ se
             }
             __syncthreads();
             const double* zr = Zs + r0 + i0;
-            for (int r = 0; r < rows; ++r) {
-                const double v = Vs[cl * 65 + r];
+#pragma unroll 4
+            for (int k0 = 0; k0 < 64; k0 += 4) {
+                const int kk = k0 + q4;
+                const double a = Vs[(wr + g) * 65 + kk];
 #pragma unroll
-                for (int u = 0; u < JPT; ++u) acc[u] = fma(v, zr[(size_t)(jg * JPT + u) * n + r], acc[u]);
+                for (int t = 0; t < NTJ; ++t) {
+                    const double b = kk < rows ? zr[(size_t)(t * 8 + g) * n + kk] : 0.0;
+                    nrg::cta_dmma(acc[t][0], acc[t][1], a, b);
+                }
             }
         }
 #pragma unroll
-        for (int u = 0; u < JPT; ++u) Ws[cl * CBK + jg * JPT + u] = acc[u];
+        for (int t = 0; t < NTJ; ++t) {
+            Ws[(wr + g) * CBK + t * 8 + 2 * q4] = acc[t][0];
+            Ws[(wr + g) * CBK + t * 8 + 2 * q4 + 1] = acc[t][1];
+        }
         __syncthreads();
-        // W2 = T W (T upper triangular)
+        // W2 = T W (T upper triangular, zero below the diagonal)
 #pragma unroll
-        for (int u = 0; u < JPT; ++u) acc[u] = 0.0;
-        for (int c2 = cl; c2 < NBB; ++c2) {
-            const double t = Ts[cl + c2 * NBB];
+        for (int t = 0; t < NTJ; ++t) acc[t][0] = acc[t][1] = 0.0;
+#pragma unroll 4
+        for (int k0 = 0; k0 < NBB; k0 += 4) {
+            const double a = Ts[(wr + g) + (k0 + q4) * NBB];
 #pragma unroll
-            for (int u = 0; u < JPT; ++u) acc[u] = fma(t, Ws[c2 * CBK + jg * JPT + u], acc[u]);
+            for (int t = 0; t < NTJ; ++t) nrg::cta_dmma(acc[t][0], acc[t][1], a, Ws[(k0 + q4) * CBK + t * 8 + g]);
         }
 #pragma unroll
-        for (int u = 0; u < JPT; ++u) W2[cl * CBK + jg * JPT + u] = acc[u];
-        // Z(r0:, :) -= V W2
+        for (int t = 0; t < NTJ; ++t) {
+            W2[(wr + g) * CBK + t * 8 + 2 * q4] = acc[t][0];
+            W2[(wr + g) * CBK + t * 8 + 2 * q4 + 1] = acc[t][1];
+        }
+        // Z(r0:, :) -= V W2, one chunk of 64 rows at a time
         for (int i0 = 0; i0 < mr; i0 += 64) {
             const int rows = min(64, mr - i0);
             __syncthreads();
@@ -1203,17 +1221,22 @@ __global__ void __launch_bounds__(256, 1) k_bt_apply(const LSec* __restrict__ se
                 Vs[c * 65 + r] = r < rows ? Rp[(size_t)(i0 + r) + (size_t)c * mr] : 0.0;
             }
             __syncthreads();
-            if (cl < rows) {
 #pragma unroll
-                for (int u = 0; u < JPT; ++u) acc[u] = 0.0;
-                for (int c = 0; c < NBB; ++c) {
-                    const double v = Vs[c * 65 + cl];
+            for (int t = 0; t < NTJ; ++t) acc[t][0] = acc[t][1] = 0.0;
+#pragma unroll 4
+            for (int k0 = 0; k0 < NBB; k0 += 4) {
+                const double a = Vs[(k0 + q4) * 65 + wr + g];
 #pragma unroll
-                    for (int u = 0; u < JPT; ++u) acc[u] = fma(v, W2[c * CBK + jg * JPT + u], acc[u]);
+                for (int t = 0; t < NTJ; ++t) nrg::cta_dmma(acc[t][0], acc[t][1], a, W2[(k0 + q4) * CBK + t * 8 + g]);
+            }
+            const int row = wr + g;
+            if (row < rows) {
+                double* zr = Zs + r0 + i0 + row;
+#pragma unroll
+                for (int t = 0; t < NTJ; ++t) {
+                    zr[(size_t)(t * 8 + 2 * q4) * n] -= acc[t][0];
+                    zr[(size_t)(t * 8 + 2 * q4 + 1) * n] -= acc[t][1];
                 }
-                double* zr = Zs + r0 + i0 + cl;
-#pragma unroll
-                for (int u = 0; u < JPT; ++u) zr[(size_t)(jg * JPT + u) * n] -= acc[u];
             }
         }
         __syncthreads();

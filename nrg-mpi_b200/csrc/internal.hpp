@@ -181,6 +181,12 @@ struct nrg_context {
     // pageable like a Fortran allocatable when host_pageable is set
     std::deque<nrg::HostBuf> host_store;
     bool host_pageable = false;
+    // page-locked staging of the runs a routine reads from a caller's pageable array
+    std::deque<nrg::HostBuf> seg_stage;
+    nrg::HostBuf& seg_slot(size_t i) {
+        if (seg_stage.size() <= i) seg_stage.resize(i + 1);
+        return seg_stage[i];
+    }
     nrg::HostBuf& hslot(size_t i) {
         if (host_store.size() <= i) host_store.resize(i + 1);
         host_store[i].pageable = host_pageable;
@@ -198,9 +204,10 @@ struct HostSeg {
 };
 // copies the listed runs of src (device-accessible pinned host memory) to the same
 // positions of dst, reading them over the host link from a kernel; ld is the stride
-// between the runs of one segment
+// between the runs of one segment.  packed: src holds the runs one after another (in
+// segment order) instead of at their positions.
 int run_gather_segs(nrg_context* ctx, const double* src, double* dst, long long ld,
-                    const std::vector<HostSeg>& segs, long long* bytes);
+                    const std::vector<HostSeg>& segs, long long* bytes, bool packed = false);
 
 // raises a kernel's dynamic shared-memory limit on the current device to at least bytes
 // and never lowers it: the attribute belongs to the kernel, not to a stream, and host

@@ -362,7 +362,7 @@ __global__ void __launch_bounds__(256) k_broaden(const double* __restrict__ bins
 // then run and offset; consecutive threads read consecutive doubles of a run
 __global__ void k_gather_segs(const double* __restrict__ src, double* __restrict__ dst, long long ld,
                               const HostSeg* __restrict__ segs, const long long* __restrict__ prefix, int nseg,
-                              long long total) {
+                              long long total, int packed) {
     for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < total;
          e += (long long)gridDim.x * blockDim.x) {
         int lo = 0, hi = nseg - 1;
@@ -373,7 +373,7 @@ __global__ void k_gather_segs(const double* __restrict__ src, double* __restrict
         const HostSeg g = segs[lo];
         const long long loc = e - prefix[lo];
         const long long p = g.off + (loc / g.len) * ld + loc % g.len;
-        dst[p] = src[p];
+        dst[p] = src[packed ? e : p];
     }
 }
 
@@ -579,7 +579,7 @@ int run_broaden(nrg_context* ctx, const double* d_bins, int nbin, int nMat, doub
 }
 
 int run_gather_segs(nrg_context* ctx, const double* src, double* dst, long long ld,
-                    const std::vector<HostSeg>& segs, long long* bytes) {
+                    const std::vector<HostSeg>& segs, long long* bytes, bool packed) {
     const int ns = (int)segs.size();
     *bytes = 0;
     if (ns == 0) return NRG_OK;
@@ -598,7 +598,7 @@ int run_gather_segs(nrg_context* ctx, const double* src, double* dst, long long 
     NRG_TRY(h2d_async(ctx, bp.p, prefix.data(), sizeof(long long) * ns));
     const long long grid = std::min<long long>((total + 255) / 256, 148LL * 16);
     k_gather_segs<<<(unsigned)grid, 256, 0, ctx->stream>>>(src, dst, ld, bs.as<HostSeg>(), bp.as<long long>(), ns,
-                                                          total);
+                                                          total, packed ? 1 : 0);
     ctx->launches++;
     NRG_CUDA_TRY(cudaGetLastError());
     *bytes = total * (long long)sizeof(double);

@@ -11,7 +11,7 @@ density-matrix trace of every backward step, and the nonzero spectral bins:
   (-1..12), the model cut there.
 
 Both the device-resident run and the drop-in replay (every routine through its entry point
-with host arrays) are compared.  Tolerances: kept counts and state counts equal (the
+with host arrays, page-locked, and for the N_keep = 4096 case also pageable) are compared.  Tolerances: kept counts and state counts equal (the
 truncation edge with its degenerate multiplets, postprocess.F90:79-126, is where a
 bit-level eigenvalue difference would show); energies <= 1e-11 * max(1, |E|); thermo
 <= 1e-11 relative; density-matrix traces 1e-12; bins <= 1e-8 absolute; sum rule 1e-10.
@@ -87,6 +87,11 @@ def test_whole_run_matches_golden(ctx_factory, name):
     _compare(res, g, device_resident=True)
     res2 = ctx.run(spectrum=True, flow_stride=64, host_drop_in=True)
     _compare(res2, g, device_resident=False)
+    if name == "siam_nkeep4096_n14":
+        # the caller's module arrays in pageable memory (a Fortran allocatable): the routines
+        # gather the runs they read on the host instead of reading pinned memory directly
+        res3 = ctx.run(spectrum=True, flow_stride=64, host_drop_in=True, host_pageable=True)
+        _compare(res3, g, device_resident=False)
     ctx.release_storage()
 
 
