@@ -376,14 +376,18 @@ def main():
     from nrg_b200 import Context, model
     inp = model.siam(**WORKLOAD)
     n_it = inp.numberOfIteration - inp.indexOfFirstIteration + 1
+    peak = fp64_peak_tflops(torch, dev) if rank == 0 else None
+    torch.cuda.empty_cache()
+    free0 = torch.cuda.mem_get_info(dev)[0]
     ctx = Context(local)
     ctx.set_model(inp)
     stream = torch.cuda.current_stream(dev)
     ctx.set_stream(stream.cuda_stream)
-    peak = fp64_peak_tflops(torch, dev) if rank == 0 else None
     for _ in range(args.warmup):
         res = ctx.run(spectrum=True)
     torch.cuda.synchronize(dev)
+    # device memory the library holds for one instance of the workload (stores and workspaces)
+    device_gb = (free0 - torch.cuda.mem_get_info(dev)[0]) / 1e9
     ctx.set_profiling(True)
     ctx.reset_stats()
     l0 = ctx.launch_count
@@ -494,6 +498,7 @@ def main():
             "phase_seconds": {"nrg_sweep": float(ph[0]), "rdm": float(ph[1]), "cfs_spectrum": float(ph[2])},
             "spectrum_seconds": float(ph[2]),
             "forward_only": forward_only,
+            "device_memory_gb": device_gb,
             "sum_rule": sums,
             "gpu_launches": int(launches),
             "roofline": {"kernel": "k_tri_cluster (FP64 Householder tridiagonalisation of the sectors of "

@@ -646,7 +646,12 @@ static int invmat_common(nrg_context* ctx, int32_t iteration, const nrg_invarian
     }
     if (rc == NRG_OK) rc = stage_out(ctx, io->invariant_matrix, nout, kSlotIO + 6, &dOut);
     if (rc == NRG_OK) {
-        if (spec) rc = invmat_spec_device(ctx, S, kept, dV, io->numberOfBasis_old, dIMSo, dOut);
+        if (spec) {
+            OpView old;
+            old.dense = dIMSo;
+            old.nb = io->numberOfBasis_old;
+            rc = invmat_spec_device(ctx, S, kept, dV, old, dOut, nullptr, nullptr);
+        }
         else rc = invmat_device(ctx, S, kept, dV, dOut);
     }
     if (rc == NRG_OK) rc = finish_out(ctx, io->invariant_matrix, dOut, nout);
@@ -918,8 +923,11 @@ static int spike_common(nrg_context* ctx, int32_t iteration, const nrg_spike_io*
     if (rc == NRG_OK) rc = run_fill(ctx, tPos, (long long)(2 * nw), 0.0);
     if (rc == NRG_OK) rc = run_fill(ctx, tot, 4LL * M.nMat, 0.0);
     if (rc == NRG_OK) {
-        if (cfs) rc = spike_cfs_device(ctx, iteration, it, io->numberOfBasis_old, dIMS, dR, tPos, tNeg, tot);
-        else rc = spike_t0_device(ctx, iteration, it, gs, io->numberOfBasis_old, dIMS, tPos, tNeg);
+        OpView old;
+        old.dense = dIMS;
+        old.nb = io->numberOfBasis_old;
+        if (cfs) rc = spike_cfs_device(ctx, iteration, it, old, dR, tPos, tNeg, tot);
+        else rc = spike_t0_device(ctx, iteration, it, gs, old, tPos, tNeg);
     }
     // add into the caller's bins (weight column = second column)
     std::vector<double> hp(nw), hn(nw);

@@ -432,14 +432,18 @@ int run_device(nrg_context* ctx, const nrg_run_input* in, nrg_run_output* out, c
     ctx->h2d += (long long)sizeof(double) * nb_old * (1 + (long long)nb_old * M.nCM);
     const double* dEold = bEold0.as<double>();
     const double* dIMold = bIM0.as<double>();
-    const double* dIMSold = nullptr;
+    // the d-dagger matrices: the initial one dense (initial.dat), those of the iterations
+    // block-sparse (only the blocks of allowed sector pairs)
+    OpView imsOld;
+    std::vector<SparseBlocks> imsTab(nIt);
     if (spectrum) {
         DevBuf& b = ctx->slot(9);
         const size_t n = (size_t)nb_old * nb_old * M.nMat;
         NRG_TRY(b.ensure(sizeof(double) * n));
         NRG_CUDA_TRY(cudaMemcpyAsync(b.p, in->invariant_matrix_spectrum, sizeof(double) * n, cudaMemcpyHostToDevice, st));
         ctx->h2d += (long long)(sizeof(double) * n);
-        dIMSold = b.as<double>();
+        imsOld.dense = b.as<double>();
+        imsOld.nb = nb_old;
     }
     if ((int)ctx->iter_sectors.size() < nIt) ctx->iter_sectors.resize(nIt);
     ctx->slot(22 + 3 * (size_t)nIt);   // size the store once: references below stay valid
@@ -521,17 +525,17 @@ int run_device(nrg_context* ctx, const nrg_run_input* in, nrg_run_output* out, c
         if (out && out->kept) out->kept[idx] = nbk;
         if (out && out->numberOfBasisFull) out->numberOfBasisFull[idx] = nb;
         const double* dIMnew = dIMold;
-        const double* dIMSnew = dIMSold;
+        OpView imsNew = imsOld;
         if (it < nIter) {   // postprocess.F90:189-204
             DevBuf& bIM = ctx->slot(1 + ((idx + 1) & 1));
             NRG_TRY(bIM.ensure(sizeof(double) * (size_t)nbk * nbk * M.nCM));
             NRG_TRY(invmat_device(ctx, S, R.kept, bV.as<double>(), bIM.as<double>()));
             dIMnew = bIM.as<double>();
             if (spectrum) {
-                DevBuf& bS = slotS(idx);
-                NRG_TRY(bS.ensure(sizeof(double) * (size_t)nbk * nbk * M.nMat));
-                NRG_TRY(invmat_spec_device(ctx, S, R.kept, bV.as<double>(), nb_old, dIMSold, bS.as<double>()));
-                dIMSnew = bS.as<double>();
+                NRG_TRY(invmat_spec_device(ctx, S, R.kept, bV.as<double>(), imsOld, nullptr, &imsTab[idx],
+                                           &slotS(idx)));
+                imsNew = OpView();
+                imsNew.sp = &imsTab[idx];
             }
         }
         DevBuf& bEo = ctx->slot(3 + ((idx + 1) & 1));
@@ -540,7 +544,7 @@ int run_device(nrg_context* ctx, const nrg_run_input* in, nrg_run_output* out, c
         ctx->h2d += (long long)sizeof(double) * nbk;
         dEold = bEo.as<double>();
         dIMold = dIMnew;
-        dIMSold = dIMSnew;
+        imsOld = imsNew;
         bo.swap(bo_new);
         nb_old = nbk;
     }
@@ -679,8 +683,9 @@ int run_device(nrg_context* ctx, const nrg_run_input* in, nrg_run_output* out, c
             V.S = &ctx->iter_sectors[idx]; V.kept = recs[idx].kept; V.d_V = slotV(idx).as<double>();
             V.d_Esec = slotE(idx).as<double>(); V.nb_kept = recs[idx].nb_kept;
             V.d_rdm = bRdm.as<double>(); V.rdm_off = recs[idx].rdm_off; V.d_P = dP(idx);
-            NRG_TRY(spike_fdm_device(ctx, N, V, recs[idx - 1].nb_kept, slotS(idx - 1).as<double>(), N == nIter,
-                                     dPos, dNeg, bTot.as<double>()));
+            OpView prev;
+            prev.sp = &imsTab[idx - 1];
+            NRG_TRY(spike_fdm_device(ctx, N, V, prev, N == nIter, dPos, dNeg, bTot.as<double>()));
         }
     }
     // ---- CFS spectrum (main.F90:204-224) ----
@@ -695,20 +700,20 @@ int run_device(nrg_context* ctx, const nrg_run_input* in, nrg_run_output* out, c
             V.S = &ctx->iter_sectors[idx]; V.kept = recs[idx].kept; V.d_V = slotV(idx).as<double>();
             V.d_Esec = slotE(idx).as<double>(); V.nb_kept = recs[idx].nb_kept;
             V.d_rdm = bRdm.as<double>(); V.rdm_off = recs[idx].rdm_off;
-            const int nbo = recs[idx - 1].nb_kept;
-            const double* dIMSprev = slotS(idx - 1).as<double>();
+            OpView prev;
+            prev.sp = &imsTab[idx - 1];
             if (N == nIter) {
                 std::vector<int> gs;
                 const Sectors& S = *V.S;
                 for (int s = 0; s < S.nsub; ++s)
                     for (int p = 0; p < S.dim[s]; ++p)
                         if (recs[idx].Esec[S.start[s] + p] < 1.0e-8) gs.push_back(s);
-                NRG_TRY(spike_t0_device(ctx, N, V, gs, nbo, dIMSprev, dPos, dNeg));
+                NRG_TRY(spike_t0_device(ctx, N, V, gs, prev, dPos, dNeg));
             } else {
                 double* tPos = bTmp.as<double>();
                 double* tNeg = tPos + nw;
                 NRG_TRY(run_fill(ctx, tPos, (long long)(2 * nw), 0.0));
-                NRG_TRY(spike_cfs_device(ctx, N, V, nbo, dIMSprev, bRdm.as<double>(), tPos, tNeg, bTot.as<double>()));
+                NRG_TRY(spike_cfs_device(ctx, N, V, prev, bRdm.as<double>(), tPos, tNeg, bTot.as<double>()));
                 NRG_TRY(run_add(ctx, dPos, tPos, (long long)(2 * nw)));
             }
         }

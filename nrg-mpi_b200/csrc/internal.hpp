@@ -346,8 +346,37 @@ std::vector<int> kept_per_sector(const Sectors& S, int nb_kept, const int* basis
 
 int invmat_device(nrg_context* ctx, const Sectors& S, const std::vector<int>& kept,
                   const double* d_V, double* d_IM);
+
+// The d-dagger matrices <l| d^dagger_m |r> of the kept states of one iteration, stored as
+// blocks: only the (sector L, sector R, m) blocks whose quantum numbers differ by the
+// operator's (invariantMatrixForSpectrumDGEMM.F90:166-170) are kept, each column-major
+// kept[R] x kept[L] (element (r, l) at off + r + l * kept[R]); the others are zero.
+struct SparseBlocks {
+    int nsub = 0, nMat = 0;
+    std::vector<long long> kst;   // kept-state prefix per sector (nsub + 1)
+    std::vector<int> kept;        // kept states per sector
+    std::vector<long long> off;   // ((L * nsub) + R) * nMat + m -> offset, -1 when absent
+    long long total = 0;          // doubles
+    const double* data = nullptr;
+    int sector_of(long long i) const;   // sector holding kept index i, or -1
+};
+// read access to a d-dagger matrix of the kept states of one iteration: dense
+// (nb, nb, nMat) column-major as the reference stores it, or block-sparse
+struct OpView {
+    const double* dense = nullptr;
+    long long nb = 0;
+    const SparseBlocks* sp = nullptr;
+    // element (r0, l0, m) of a cr x cl range and its strides along r and l; nullptr when
+    // the range lies in an absent (zero) block; *bad when the range leaves the matrix or
+    // crosses a block boundary
+    const double* at(long long r0, long long l0, int m, long long cr, long long cl, long long* sr,
+                     long long* sl, bool* bad) const;
+};
+// invariantMatrixForSpectrumDGEMM: the new matrix, dense into d_dense (nb_kept^2 x nMat) or,
+// with d_dense null, block-sparse into *sp_out with its data in *sp_buf
 int invmat_spec_device(nrg_context* ctx, const Sectors& S, const std::vector<int>& kept,
-                       const double* d_V, int nb_old, const double* d_IMSold, double* d_IMS);
+                       const double* d_V, const OpView& old, double* d_dense, SparseBlocks* sp_out,
+                       DevBuf* sp_buf);
 
 // rdm / spectrum inputs for one iteration (device resident)
 struct IterView {
@@ -367,16 +396,15 @@ int rdm_step_device(nrg_context* ctx, const IterView& present, const IterView& c
 // T = 0 jobs when gs_sectors is given, CFS jobs otherwise
 std::vector<HostSeg> spike_ims_segs(const Model& M, const IterView& it, const std::vector<int>* gs_sectors,
                                     int nb_old);
-int spike_cfs_device(nrg_context* ctx, int iteration, const IterView& it, int nb_old,
-                     const double* d_IMSold, const double* d_rdm, double* d_binPos,
-                     double* d_binNeg, double* d_tot);
+int spike_cfs_device(nrg_context* ctx, int iteration, const IterView& it, const OpView& old,
+                     const double* d_rdm, double* d_binPos, double* d_binNeg, double* d_tot);
 int spike_t0_device(nrg_context* ctx, int iteration, const IterView& it,
-                    const std::vector<int>& gs_sectors, int nb_old, const double* d_IMSold,
+                    const std::vector<int>& gs_sectors, const OpView& old,
                     double* d_binPos, double* d_binNeg);
 // full-density-matrix spectrum of one shell: the kept-discarded terms (the CFS products,
 // with the discarded states' weights added) and the discarded-discarded terms, each
 // spike in the bins of the sign of its frequency; last: every state is discarded
-int spike_fdm_device(nrg_context* ctx, int iteration, const IterView& it, int nb_old, const double* d_IMSold,
+int spike_fdm_device(nrg_context* ctx, int iteration, const IterView& it, const OpView& old,
                      bool last, double* d_binPos, double* d_binNeg, double* d_tot);
 
 int check_device_status(nrg_context* ctx);

@@ -557,16 +557,44 @@ int invmat_device(nrg_context* ctx, const Sectors& S, const std::vector<int>& ke
     return launch_ggemm(ctx, probs, 8);
 }
 
+int SparseBlocks::sector_of(long long i) const {
+    if (i < 0 || nsub == 0 || i >= kst[nsub]) return -1;
+    const int s = (int)(std::upper_bound(kst.begin(), kst.end(), i) - kst.begin()) - 1;
+    return (s >= 0 && s < nsub && kept[s] > 0) ? s : -1;
+}
+
+const double* OpView::at(long long r0, long long l0, int m, long long cr, long long cl, long long* sr,
+                         long long* sl, bool* bad) const {
+    *bad = false;
+    if (dense) {
+        if (r0 < 0 || l0 < 0 || r0 + cr > nb || l0 + cl > nb) { *bad = true; return nullptr; }
+        *sr = 1;
+        *sl = nb;
+        return dense + r0 + l0 * nb + (long long)m * nb * nb;
+    }
+    if (!sp) { *bad = true; return nullptr; }
+    const int R = sp->sector_of(r0), L = sp->sector_of(l0);
+    if (R < 0 || L < 0 || r0 + cr > sp->kst[R] + sp->kept[R] || l0 + cl > sp->kst[L] + sp->kept[L]) {
+        *bad = true;
+        return nullptr;
+    }
+    const long long o = sp->off[((size_t)L * sp->nsub + R) * sp->nMat + m];
+    if (o < 0) return nullptr;
+    *sr = 1;
+    *sl = sp->kept[R];
+    return sp->data + o + (r0 - sp->kst[R]) + (l0 - sp->kst[L]) * sp->kept[R];
+}
+
 int invmat_spec_device(nrg_context* ctx, const Sectors& S, const std::vector<int>& kept,
-                       const double* d_V, int nb_old, const double* d_IMSold, double* d_IMS) {
+                       const double* d_V, const OpView& old, double* d_dense, SparseBlocks* sp_out,
+                       DevBuf* sp_buf) {
     // invariantMatrixForSpectrumDGEMM.F90:71-370
     const Model& M = ctx->model;
     const int nsub = S.nsub, nVar = S.nVar, nOps = S.nOps;
     std::vector<long long> kst(nsub + 1, 0);
     for (int s = 0; s < nsub; ++s) kst[s + 1] = kst[s] + kept[s];
     const long long nbk = kst[nsub];
-    const long long nbo = nb_old;
-    NRG_TRY(run_fill(ctx, d_IMS, nbk * nbk * M.nMat, 0.0));
+    if (d_dense) NRG_TRY(run_fill(ctx, d_dense, nbk * nbk * M.nMat, 0.0));
     struct Pair { int L, R, m; long long t_off; };
     std::vector<Pair> pairs;
     long long toff = 0;
@@ -585,6 +613,22 @@ int invmat_spec_device(nrg_context* ctx, const Sectors& S, const std::vector<int
             }
         }
     }
+    if (!d_dense) {
+        // the block table of the new matrix: one block per allowed pair
+        sp_out->nsub = nsub;
+        sp_out->nMat = M.nMat;
+        sp_out->kst = kst;
+        sp_out->kept = kept;
+        sp_out->off.assign((size_t)nsub * nsub * M.nMat, -1);
+        long long tot = 0;
+        for (const auto& pr : pairs) {
+            sp_out->off[((size_t)pr.L * nsub + pr.R) * M.nMat + pr.m] = tot;
+            tot += (long long)kept[pr.L] * kept[pr.R];
+        }
+        sp_out->total = tot;
+        NRG_TRY(sp_buf->ensure(sizeof(double) * (size_t)std::max(tot, 1LL)));
+        sp_out->data = sp_buf->as<double>();
+    }
     if (pairs.empty()) return NRG_OK;
     DevBuf& T = ctx->scratch.b[6];
     NRG_TRY(T.ensure(sizeof(double) * (size_t)toff));
@@ -596,17 +640,21 @@ int invmat_spec_device(nrg_context* ctx, const Sectors& S, const std::vector<int
         for (int a = 0; a < nOps; ++a) {
             const int cL = S.cnt(L, a), cR = S.cnt(R, a);
             if (cL == 0 || cR == 0) continue;
-            if (S.refBase[(size_t)L * nOps + a] + cL > nb_old || S.refBase[(size_t)R * nOps + a] + cR > nb_old) {
-                nrg_set_error_message("basis_input references exceed numberOfBasis_old=%d", nb_old);
+            // C(i in L, j in R) = cspec(m, a) IMS_old(ref_j, ref_i, m): rows ref_j, columns ref_i
+            long long sr = 0, sl = 0;
+            bool bad = false;
+            const double* a0 = old.at(S.refBase[(size_t)R * nOps + a], S.refBase[(size_t)L * nOps + a], m, cR, cL,
+                                      &sr, &sl, &bad);
+            if (bad) {
+                nrg_set_error_message("basis_input references outside the previous d-dagger matrix");
                 return NRG_ERR_INVALID;
             }
+            if (!a0) continue;   // a zero block of the previous matrix
             GemmProblem P;
             std::memset(&P, 0, sizeof(P));
             P.M = cL; P.N = kept[R]; P.K = cR;
             P.alpha = M.cspec[(size_t)m + (size_t)a * M.nMat]; P.beta = 0.0;
-            P.A = d_IMSold + S.refBase[(size_t)R * nOps + a] + (long long)S.refBase[(size_t)L * nOps + a] * nbo +
-                  (long long)m * nbo * nbo;
-            P.a_si = nbo; P.a_sk = 1;
+            P.A = a0; P.a_si = sl; P.a_sk = sr;
             P.B = d_V + S.ce[R]; P.b_ki = dl + S.lstOff[(size_t)R * nOps + a]; P.b_sk = 1; P.b_sj = S.dim[R];
             P.C = T.as<double>() + pr.t_off; P.c_ri = dl + S.lstOff[(size_t)L * nOps + a];
             P.c_si = 1; P.c_sj = S.dim[L];
@@ -618,7 +666,12 @@ int invmat_spec_device(nrg_context* ctx, const Sectors& S, const std::vector<int
         Q.alpha = 1.0; Q.beta = 0.0;
         Q.A = d_V + S.ce[L]; Q.a_si = S.dim[L]; Q.a_sk = 1;
         Q.B = T.as<double>() + pr.t_off; Q.b_sk = 1; Q.b_sj = S.dim[L];
-        Q.C = d_IMS + kst[R] + kst[L] * nbk + (long long)m * nbk * nbk; Q.c_si = nbk; Q.c_sj = 1;
+        if (d_dense) {
+            Q.C = d_dense + kst[R] + kst[L] * nbk + (long long)m * nbk * nbk; Q.c_si = nbk; Q.c_sj = 1;
+        } else {
+            Q.C = sp_buf->as<double>() + sp_out->off[((size_t)L * nsub + R) * M.nMat + m];
+            Q.c_si = kept[R]; Q.c_sj = 1;
+        }
         p2.push_back(Q);
     }
     NRG_TRY(launch_ggemm(ctx, p1, 8));
@@ -752,13 +805,11 @@ struct SpecJob {
     int fdm = 0;       // full-density-matrix weights
 };
 
-int run_spec_jobs(nrg_context* ctx, const IterView& it, std::vector<SpecJob>& jobs, int nb_old,
-                  const double* d_IMSold, double sc, int nbin, double* d_binPos, double* d_binNeg,
-                  double* d_tot) {
+int run_spec_jobs(nrg_context* ctx, const IterView& it, std::vector<SpecJob>& jobs, const OpView& old,
+                  double sc, int nbin, double* d_binPos, double* d_binNeg, double* d_tot) {
     const Model& M = ctx->model;
     const Sectors& S = *it.S;
     const int nOps = S.nOps;
-    const long long nbo = nb_old;
     long long ttot = 0, stot = 0;
     for (auto& j : jobs) {
         j.t_off = ttot;
@@ -780,22 +831,24 @@ int run_spec_jobs(nrg_context* ctx, const IterView& it, std::vector<SpecJob>& jo
         for (int a = 0; a < nOps; ++a) {
             const int ck = S.cnt(k, a), cl = S.cnt(l, a);
             if (ck == 0 || cl == 0) continue;
-            if (S.refBase[(size_t)k * nOps + a] + ck > nb_old || S.refBase[(size_t)l * nOps + a] + cl > nb_old) {
-                nrg_set_error_message("basis_input references exceed numberOfBasis_old=%d", nb_old);
+            const long long rk = S.refBase[(size_t)k * nOps + a], rl = S.refBase[(size_t)l * nOps + a];
+            long long sr = 0, sc2 = 0;
+            bool bad = false;
+            // part 0: C(i in k, j in l) = cspec(m, a) IMS(ref_j, ref_i, m), rows ref_j (l);
+            // part 1: C'(j in k, i in l)^T = IMS(ref_j(k), ref_i(l), m), rows ref_j (k)
+            const double* a0 = j.part == 0 ? old.at(rl, rk, m, cl, ck, &sr, &sc2, &bad)
+                                           : old.at(rk, rl, m, ck, cl, &sr, &sc2, &bad);
+            if (bad) {
+                nrg_set_error_message("basis_input references outside the previous d-dagger matrix");
                 return NRG_ERR_INVALID;
             }
+            if (!a0) continue;   // a zero block of the previous matrix
             GemmProblem P;
             std::memset(&P, 0, sizeof(P));
             P.M = ck; P.N = j.nl; P.K = cl;
             P.alpha = M.cspec[(size_t)m + (size_t)a * M.nMat]; P.beta = 0.0;
-            const long long rk = S.refBase[(size_t)k * nOps + a], rl = S.refBase[(size_t)l * nOps + a];
-            if (j.part == 0) {
-                // C(i in k, j in l) = cspec(m, a) IMS(ref_j, ref_i, m)
-                P.A = d_IMSold + rl + rk * nbo + (long long)m * nbo * nbo; P.a_si = nbo; P.a_sk = 1;
-            } else {
-                // C'(j in k, i in l)^T: IMS(ref_j(k), ref_i(l), m)
-                P.A = d_IMSold + rk + rl * nbo + (long long)m * nbo * nbo; P.a_si = 1; P.a_sk = nbo;
-            }
+            P.A = a0;
+            if (j.part == 0) { P.a_si = sc2; P.a_sk = sr; } else { P.a_si = sr; P.a_sk = sc2; }
             P.B = it.d_V + S.ce[l] + (long long)j.c0 * S.dim[l];
             P.b_ki = dl + S.lstOff[(size_t)l * nOps + a]; P.b_sk = 1; P.b_sj = S.dim[l];
             P.C = T.as<double>() + j.t_off; P.c_ri = dl + S.lstOff[(size_t)k * nOps + a];
@@ -927,17 +980,15 @@ std::vector<HostSeg> spike_ims_segs(const Model& M, const IterView& it, const st
     return segs;
 }
 
-int spike_cfs_device(nrg_context* ctx, int iteration, const IterView& it, int nb_old,
-                     const double* d_IMSold, const double* d_rdm, double* d_binPos,
-                     double* d_binNeg, double* d_tot) {
+int spike_cfs_device(nrg_context* ctx, int iteration, const IterView& it, const OpView& old,
+                     const double* d_rdm, double* d_binPos, double* d_binNeg, double* d_tot) {
     const Model& M = ctx->model;
     (void)d_rdm;
     std::vector<SpecJob> jobs = cfs_jobs(M, it);
-    return run_spec_jobs(ctx, it, jobs, nb_old, d_IMSold, M.scale(iteration), M.numberOfBin(),
-                         d_binPos, d_binNeg, d_tot);
+    return run_spec_jobs(ctx, it, jobs, old, M.scale(iteration), M.numberOfBin(), d_binPos, d_binNeg, d_tot);
 }
 
-int spike_fdm_device(nrg_context* ctx, int iteration, const IterView& it, int nb_old, const double* d_IMSold,
+int spike_fdm_device(nrg_context* ctx, int iteration, const IterView& it, const OpView& old,
                      bool last, double* d_binPos, double* d_binNeg, double* d_tot) {
     const Model& M = ctx->model;
     const Sectors& S = *it.S;
@@ -975,19 +1026,18 @@ int spike_fdm_device(nrg_context* ctx, int iteration, const IterView& it, int nb
             }
         }
     }
-    return run_spec_jobs(ctx, it, jobs, nb_old, d_IMSold, M.scale(iteration), M.numberOfBin(),
-                         d_binPos, d_binNeg, d_tot);
+    return run_spec_jobs(ctx, it, jobs, old, M.scale(iteration), M.numberOfBin(), d_binPos, d_binNeg, d_tot);
 }
 
 int spike_t0_device(nrg_context* ctx, int iteration, const IterView& it,
-                    const std::vector<int>& gs_sectors, int nb_old, const double* d_IMSold,
+                    const std::vector<int>& gs_sectors, const OpView& old,
                     double* d_binPos, double* d_binNeg) {
     const Model& M = ctx->model;
     std::vector<SpecJob> jobs = t0_jobs(M, it, gs_sectors);
     DevBuf& tot = ctx->scratch.b[22];
     NRG_TRY(tot.ensure(sizeof(double) * 2 * std::max(M.nMat, 1)));
-    return run_spec_jobs(ctx, it, jobs, nb_old, d_IMSold, M.scale(iteration), M.numberOfBin(),
-                         d_binPos, d_binNeg, tot.as<double>());
+    return run_spec_jobs(ctx, it, jobs, old, M.scale(iteration), M.numberOfBin(), d_binPos, d_binNeg,
+                         tot.as<double>());
 }
 
 }  // namespace nrg
