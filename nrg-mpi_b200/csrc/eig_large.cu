@@ -31,6 +31,7 @@ constexpr int DC_LOW = 128;   // merges of up to this many rows run inside one b
 constexpr int TPB = 256;
 constexpr int CB = 32;        // columns per block in the symmetric matrix-vector product
 constexpr int kTriCL = 8;     // blocks per cluster of the one-launch tridiagonalisation
+constexpr int kTriCL16Min = 1 << 30;   // order from which a launch takes 16-block clusters
 
 struct LSec {
     long long a_off, e_off, w_off, i_off;
@@ -1370,8 +1371,14 @@ static int tri_cluster(nrg_context* ctx, const LSec* dsec, int ns, int maxn, dou
         const char* e = getenv("NRG_TRI_SYM");
         return e && e[0] == '1';
     }();
+    // launches whose largest sector reaches this order take 16-block clusters: their
+    // column product (the trailing matrix streamed from L2) outweighs the wider exchanges
+    static const int cl16_min = [] {
+        const char* e = getenv("NRG_TRI_CL16_MIN");
+        return (e && *e) ? atoi(e) : kTriCL16Min;
+    }();
     *done = false;
-    const int cl = forced >= 0 ? forced : kTriCL;
+    const int cl = forced >= 0 ? forced : (maxn >= cl16_min ? 16 : kTriCL);
     if (sym && cl == 16) {
         NRG_TRY(tri_csym_cl<16>(ctx, dsec, ns, maxn, d_V, wsd, wsi, done));
         if (*done) return NRG_OK;
@@ -1389,6 +1396,10 @@ static int tri_cluster(nrg_context* ctx, const LSec* dsec, int ns, int maxn, dou
     if (cl == 16) {
         NRG_TRY(tri_cluster_cl<16>(ctx, dsec, ns, maxn, d_V, wsd, wsi, done));
         if (*done || forced == 16) return NRG_OK;
+    }
+    if (cl == 16 && !*done) {   // 16 could not be placed: the 8-block kernel
+        NRG_TRY(tri_cluster_cl<8>(ctx, dsec, ns, maxn, d_V, wsd, wsi, done));
+        if (*done) return NRG_OK;
     }
     if (cl >= 8) {
         NRG_TRY(tri_cluster_cl<8>(ctx, dsec, ns, maxn, d_V, wsd, wsi, done));
