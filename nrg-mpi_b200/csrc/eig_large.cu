@@ -229,14 +229,13 @@ __global__ void __launch_bounds__(TPB) k_tri_finish(const LSec* __restrict__ sec
 // other's data.
 constexpr int TT = 512;     // threads per block of the cluster kernel
 constexpr int TRW = 128;    // rows per staged chunk of the trailing update
-constexpr int TRL = TRW + 4;   // their stride in shared memory (spreads the MMA fragment loads over banks)
 constexpr int P2W = 2 * NB + 2;   // partials per block: W^T v | V^T v | y.v
 
 struct TriLayout {
     int MM, PN, NRB;   // own indices per block, rows (even), row batches of 256
     __host__ __device__ long long doubles(int CL) const {
         // the panel rows AR share their space with the staging of the trailing update
-        const long long stage = (long long)NB * MM > 2LL * NB * TRL ? (long long)NB * MM : 2LL * NB * TRL;
+        const long long stage = (long long)NB * MM > 2LL * NB * TRW ? (long long)NB * MM : 2LL * NB * TRW;
         return 2LL * NB * MM + PN + MM + (long long)CL * P2W + CL + 2 + 2LL * NB + 2LL * NB + P2W + 32 +
                stage + (long long)NRB * MM + 3LL * NB;
     }
@@ -283,9 +282,9 @@ __global__ void __launch_bounds__(TT, 1) k_tri_cluster(const LSec* __restrict__ 
     double* tsum = piv + 2 * NB;           // t1 | t2 | y.v
     double* red = tsum + P2W;              // 32
     double* AR = red + 32;                 // NB x MM: A(p + q, own column m), during the columns
-    double* stV = AR;                      // NB x TRL staged rows of V (transposed), during the
-    double* stW = stV + NB * TRL;          // trailing update; NB x TRL
-    double* ysp = AR + ((size_t)NB * MM > 2 * NB * TRL ? (size_t)NB * MM : 2 * NB * TRL);   // NRB x MM
+    double* stV = AR;                      // NB x TRW staged rows of V (transposed), during the
+    double* stW = stV + NB * TRW;          // trailing update; NB x TRW
+    double* ysp = AR + ((size_t)NB * MM > 2 * NB * TRW ? (size_t)NB * MM : 2 * NB * TRW);   // NRB x MM
     double* pan = ysp + (size_t)lay.NRB * MM;   // D | E | tau of the panel's columns
     double* Vg = L.VW;
     double* Wg = L.VW + (size_t)NB * n;
@@ -466,58 +465,58 @@ __global__ void __launch_bounds__(TT, 1) k_tri_cluster(const LSec* __restrict__ 
             if (kq % CL == rank) L.D[kq] = pan[tid];
             if (rank == 0) { L.E[kq] = pan[NB + tid]; L.TAU[kq] = pan[2 * NB + tid]; }
         }
-        // ---- trailing update of the own columns l >= r0, rows >= r0, on the FP64 tensor
-        // pipe: A(rows, own columns) -= [V W](rows, :) [W V](own columns, :)^T, K = 2 jc;
-        // the 16 warps cover 128 rows x 128 own columns per pass in 32 x 32 tiles of 4 x 4
-        // MMAs (m8n8k4) ----
+        // ---- trailing update of the own columns l >= r0, rows >= r0 ----
         const int r0 = last + 1, jc = last - p + 1;
         cluster.sync();
         const int mR = first_own(r0);
-        const int g = lane >> 2, q4 = lane & 3;
-        const int wr = (warp >> 2) * 32, wc = (warp & 3) * 32;
-        const int K2 = 2 * jc, Kp = (K2 + 3) & ~3;
+        // register tiles of 4 rows (tr + 32 u) x 4 own columns (4 tc + c), K = 2 jc
+        const int tr = tid & 31, tc = tid >> 5;
         for (int ib = r0; ib < n; ib += TRW) {
             for (int e = tid; e < jc * TRW; e += TT) {
                 const int q = e / TRW, r = e % TRW, row = ib + r;
-                stV[q * TRL + r] = row < n ? __ldcg(Vg + row + (size_t)q * n) : 0.0;
-                stW[q * TRL + r] = row < n ? __ldcg(Wg + row + (size_t)q * n) : 0.0;
+                stV[q * TRW + r] = row < n ? __ldcg(Vg + row + (size_t)q * n) : 0.0;
+                stW[q * TRW + r] = row < n ? __ldcg(Wg + row + (size_t)q * n) : 0.0;
             }
             __syncthreads();
-            for (int mc = mR; mc < cnt; mc += 128) {
-                const int m0 = mc + wc;   // this warp's first own column (uniform in the warp)
-                if (m0 >= cnt) continue;
-                double acc[4][4][2];
+            for (int mc = mR; mc < cnt; mc += 4 * (TT / 32)) {
+                const int m0 = mc + 4 * tc;
+                if (m0 < cnt) {
+                    int mcol[4];
 #pragma unroll
-                for (int r = 0; r < 4; ++r)
+                    for (int c = 0; c < 4; ++c) mcol[c] = min(m0 + c, cnt - 1);
+                    double acc[4][4];
 #pragma unroll
-                    for (int c = 0; c < 4; ++c) acc[r][c][0] = acc[r][c][1] = 0.0;
-                for (int k0 = 0; k0 < Kp; k0 += 4) {
-                    const int k = k0 + q4;
-                    const double* sa = k < jc ? stV + (size_t)k * TRL : stW + (size_t)(k - jc) * TRL;
-                    const double* sb = k < jc ? WO + (size_t)k * MM : VO + (size_t)(k - jc) * MM;
-                    double af[4], bf[4];
+                    for (int u = 0; u < 4; ++u)
 #pragma unroll
-                    for (int r = 0; r < 4; ++r) af[r] = k < K2 ? sa[wr + r * 8 + g] : 0.0;
+                        for (int c = 0; c < 4; ++c) acc[u][c] = 0.0;
+                    for (int q = 0; q < jc; ++q) {
+                        double av[4], aw[4], bw[4], bv[4];
 #pragma unroll
-                    for (int c = 0; c < 4; ++c) bf[c] = k < K2 ? sb[min(m0 + c * 8 + g, cnt - 1)] : 0.0;
+                        for (int u = 0; u < 4; ++u) {
+                            av[u] = stV[q * TRW + tr + 32 * u];
+                            aw[u] = stW[q * TRW + tr + 32 * u];
+                        }
 #pragma unroll
-                    for (int r = 0; r < 4; ++r)
+                        for (int c = 0; c < 4; ++c) {
+                            bw[c] = WO[q * MM + mcol[c]];
+                            bv[c] = VO[q * MM + mcol[c]];
+                        }
 #pragma unroll
-                        for (int c = 0; c < 4; ++c) nrg::cta_dmma(acc[r][c][0], acc[r][c][1], af[r], bf[c]);
-                }
+                        for (int u = 0; u < 4; ++u)
 #pragma unroll
-                for (int c = 0; c < 4; ++c)
+                            for (int c = 0; c < 4; ++c) acc[u][c] = fma(av[u], bw[c], fma(aw[u], bv[c], acc[u][c]));
+                    }
 #pragma unroll
-                    for (int h = 0; h < 2; ++h) {
-                        const int m = m0 + c * 8 + 2 * q4 + h;
-                        if (m >= cnt) continue;
-                        double* colp = A + (size_t)(rank + CL * m) * n;
+                    for (int c = 0; c < 4; ++c) {
+                        if (m0 + c >= cnt) continue;
+                        double* colp = A + (size_t)(rank + CL * (m0 + c)) * n;
 #pragma unroll
-                        for (int r = 0; r < 4; ++r) {
-                            const int row = ib + wr + r * 8 + g;
-                            if (row < n) colp[row] -= acc[r][c][h];
+                        for (int u = 0; u < 4; ++u) {
+                            const int row = ib + tr + 32 * u;
+                            if (row < n) colp[row] -= acc[u][c];
                         }
                     }
+                }
             }
             __syncthreads();
         }
