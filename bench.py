@@ -494,6 +494,18 @@ def main():
                        "arrays in page-locked host memory allocated in one untimed run; host<->device "
                        "copies inside the timed region")
         e2e["timing"] = "wall clock around the runs, device synchronised, max over ranks"
+        # where the drop-in time goes: one more run with the parts timed apart (the stream
+        # is drained between them, so they do not overlap; not part of the timed runs)
+        ctx.reset_stats()
+        ctx.set_profiling(True)
+        ctx.run(spectrum=True, host_drop_in=True)
+        ctx.set_profiling(False)
+        sb = ctx.stats()
+        e2e["breakdown_seconds"] = {
+            "entry_staging_in": sb["entry_in_s"], "entry_device": sb["entry_compute_s"],
+            "entry_copy_out": sb["entry_out_s"], "replay_host": sb["replay_host_s"],
+            "entry_calls": int(sb["entry_calls"]),
+            "timing": "one untimed sweep with profiling on, host wall clock, stream drained between parts"}
         if not args.no_pageable:
             pg = drop_in(True, 1)
             pg["path"] = "the same with the module arrays in pageable memory (a Fortran allocatable)"

@@ -116,6 +116,15 @@ typedef struct nrg_stats {
     double tri_ms;           /* their summed device time                              */
     double tri_flops;        /* their algorithmic flops, sum over sectors of 4/3 n^3  */
     double tri_bytes;        /* their algorithmic matrix reads, sum of 8 n^3 / 3      */
+    /* drop-in entry points (profiling on: the stream is drained between the parts, so
+     * the parts do not overlap), host wall-clock seconds summed over calls:            */
+    double entry_in_s;       /* host tables, sector build, host-to-device staging     */
+    double entry_compute_s;  /* the device work                                       */
+    double entry_out_s;      /* device-to-host results, host-side output work         */
+    int64_t entry_calls;     /* drop-in entry calls timed                             */
+    double replay_host_s;    /* nrg_run's host drop-in replay: its own host work, the
+                                caller's part (truncation, module-array stock) outside
+                                the entry calls                                       */
 } nrg_stats;
 NRG_API int nrg_context_get_stats(const nrg_context* ctx, nrg_stats* out);
 NRG_API int nrg_context_reset_stats(nrg_context* ctx);

@@ -4,6 +4,7 @@
 #include "internal.hpp"
 
 #include <algorithm>
+#include <chrono>
 #include <cstdarg>
 #include <cstdlib>
 #include <cstring>
@@ -131,6 +132,27 @@ int reject_foreign(const nrg_context* ctx, const char* who, std::initializer_lis
     }
     return NRG_OK;
 }
+
+// Host wall-clock parts of one drop-in entry call with profiling on: the stream is drained
+// at each mark, so the staging copies, the device work and the copies out are timed apart
+struct EntryClock {
+    nrg_context* ctx;
+    bool on;
+    std::chrono::steady_clock::time_point t;
+    explicit EntryClock(nrg_context* c) : ctx(c), on(c->profiling) {
+        if (!on) return;
+        cudaStreamSynchronize(ctx->stream);
+        t = std::chrono::steady_clock::now();
+        ++ctx->entry_calls;
+    }
+    void mark(int part) {
+        if (!on) return;
+        cudaStreamSynchronize(ctx->stream);
+        const auto n = std::chrono::steady_clock::now();
+        ctx->entry_s[part] += std::chrono::duration<double>(n - t).count();
+        t = n;
+    }
+};
 
 template <class T>
 int stage_in(nrg_context* ctx, const T* p, size_t n, size_t slot, const T** out) {
@@ -330,6 +352,11 @@ int nrg_context_get_stats(const nrg_context* ctx, nrg_stats* out) {
     out->tri_ms = ctx->tri_ms;
     out->tri_flops = ctx->tri_flops;
     out->tri_bytes = ctx->tri_bytes;
+    out->entry_in_s = ctx->entry_s[0];
+    out->entry_compute_s = ctx->entry_s[1];
+    out->entry_out_s = ctx->entry_s[2];
+    out->entry_calls = ctx->entry_calls;
+    out->replay_host_s = ctx->replay_host_s;
     return NRG_OK;
 }
 
@@ -343,6 +370,9 @@ int nrg_context_reset_stats(nrg_context* ctx) {
     ctx->d2h = 0;
     ctx->tri_launches = 0;
     ctx->tri_ms = ctx->tri_flops = ctx->tri_bytes = 0.0;
+    ctx->entry_s[0] = ctx->entry_s[1] = ctx->entry_s[2] = 0.0;
+    ctx->entry_calls = 0;
+    ctx->replay_host_s = 0.0;
     return NRG_OK;
 }
 
@@ -491,6 +521,7 @@ int nrg_diagonalization(nrg_context* ctx, int32_t iteration, const nrg_diagonali
     NRG_TRY(reject_foreign(ctx, "nrg_diagonalization",
                            {io->subspaceInfo, io->basis_input, io->eigenvalue_old, io->invariant_matrix, io->eigenvalue,
                             io->eigenvector, io->basis_output, io->groundStateEnergy}));
+    EntryClock clk(ctx);
     const Model& M = ctx->model;
     if (iteration < M.first || iteration > M.nIter) {
         nrg_set_error_message("iteration %d outside [%d, %d]", iteration, M.first, M.nIter);
@@ -546,7 +577,9 @@ int nrg_diagonalization(nrg_context* ctx, int32_t iteration, const nrg_diagonali
     if (rc == NRG_OK) rc = stage_out(ctx, io->eigenvector, (size_t)S.sizeV, kSlotIO + 2, &dV);
     if (rc == NRG_OK) rc = stage_out(ctx, io->eigenvalue, (size_t)S.nb, kSlotIO + 3, &dE);
     DiagOut out;
+    clk.mark(0);
     if (rc == NRG_OK) rc = diag_device(ctx, iteration, S, dEo, nbo, dIM, dV, dE, &out);
+    clk.mark(1);
     if (rc == NRG_OK) rc = finish_out(ctx, io->eigenvector, dV, (size_t)S.sizeV);
     if (rc == NRG_OK) rc = finish_out(ctx, io->eigenvalue, dE, (size_t)S.nb);
     if (rc == NRG_OK && io->basis_output) {
@@ -564,6 +597,7 @@ int nrg_diagonalization(nrg_context* ctx, int32_t iteration, const nrg_diagonali
     }
     if (rc == NRG_OK && io->groundStateEnergy) *io->groundStateEnergy = out.groundStateEnergy;
     if (cudaStreamSynchronize(ctx->stream) != cudaSuccess && rc == NRG_OK) rc = NRG_ERR_CUDA;
+    clk.mark(2);
     S.d_bi.release(); S.d_lst.release(); S.d_lstOff.release();
     return rc;
 }
@@ -575,6 +609,7 @@ static int invmat_common(nrg_context* ctx, int32_t iteration, const nrg_invarian
     NRG_TRY(reject_foreign(ctx, spec ? "nrg_invariant_matrix_for_spectrum_dgemm" : "nrg_invariant_matrix_dgemm",
                            {io->subspaceInfo, io->basis_input, io->basis_output, io->eigenvector,
                             io->invariant_matrix_spectrum_old, io->invariant_matrix}));
+    EntryClock clk(ctx);
     const Model& M = ctx->model;
     (void)iteration;
     if (spec && M.nMat == 0) { nrg_set_error_message("model has no spectrum tables"); return NRG_ERR_STATE; }
@@ -645,6 +680,7 @@ static int invmat_common(nrg_context* ctx, int32_t iteration, const nrg_invarian
                            kSlotIO + 5, &dIMSo);
     }
     if (rc == NRG_OK) rc = stage_out(ctx, io->invariant_matrix, nout, kSlotIO + 6, &dOut);
+    clk.mark(0);
     if (rc == NRG_OK) {
         if (spec) {
             OpView old;
@@ -654,8 +690,10 @@ static int invmat_common(nrg_context* ctx, int32_t iteration, const nrg_invarian
         }
         else rc = invmat_device(ctx, S, kept, dV, dOut);
     }
+    clk.mark(1);
     if (rc == NRG_OK) rc = finish_out(ctx, io->invariant_matrix, dOut, nout);
     if (cudaStreamSynchronize(ctx->stream) != cudaSuccess && rc == NRG_OK) rc = NRG_ERR_CUDA;
+    clk.mark(2);
     if (rc == NRG_OK) rc = check_device_status(ctx);
     S.d_bi.release(); S.d_lst.release(); S.d_lstOff.release();
     return rc;
@@ -748,6 +786,7 @@ int nrg_reduced_density_matrix(nrg_context* ctx, const nrg_reduced_density_io* i
     NRG_TRY(reject_foreign(ctx, "nrg_reduced_density_matrix",
                            {io->mapFullSubspaceInfo, io->fullSubspaceInfo, io->fullBasisInput, io->fullBasisOutput,
                             io->fullEigenvector, io->reducedDensityMatrix, io->pointReducedDensity, io->trace}));
+    EntryClock clk(ctx);
     const Model& M = ctx->model;
     const int nVar = M.nVar, rsf = nVar + 6, rs = nVar + 3;
     const int nIter = io->numberOfIteration, start = io->startTrancation;
@@ -772,6 +811,7 @@ int nrg_reduced_density_matrix(nrg_context* ctx, const nrg_reduced_density_io* i
     FullIter child, present;
     int rc = NRG_OK;
     int r0, r1;
+    clk.mark(0);
     rc = full_range(map.data(), nIter, M.first, io->elementNumFullSubspace, nIter, &r0, &r1);
     if (rc == NRG_OK) rc = build_full_iter(ctx, fsi.data(), r0, r1, fbi.data(), io->numFullBasisInput, &child);
     for (int i = 1; rc == NRG_OK && i <= nIter - start; ++i) {
@@ -796,6 +836,7 @@ int nrg_reduced_density_matrix(nrg_context* ctx, const nrg_reduced_density_io* i
     }
     release(child);
     release(present);
+    clk.mark(1);
     if (rc == NRG_OK) rc = finish_out(ctx, io->reducedDensityMatrix, dR, (size_t)io->sizeOfReducedDensity);
     if (rc == NRG_OK && io->trace) {
         std::vector<double> t(nIter - start);
@@ -812,6 +853,7 @@ int nrg_reduced_density_matrix(nrg_context* ctx, const nrg_reduced_density_io* i
         *io->pointReducedDensity = point;
         rc = check_device_status(ctx);
     }
+    clk.mark(2);
     return rc;
 }
 
@@ -824,6 +866,7 @@ static int spike_common(nrg_context* ctx, int32_t iteration, const nrg_spike_io*
                             io->invariant_matrix_spectrum, io->fullSubspaceInfo, io->mapFullSubspaceInfo,
                             io->reducedDensityMatrix, io->binnedSpikePositive, io->binnedSpikeNegative,
                             io->total_sum}));
+    EntryClock clk(ctx);
     const Model& M = ctx->model;
     if (M.nMat == 0) { nrg_set_error_message("model has no spectrum tables"); return NRG_ERR_STATE; }
     const int nVar = M.nVar, rs = nVar + 3, rsf = nVar + 6;
@@ -922,6 +965,7 @@ static int spike_common(nrg_context* ctx, int32_t iteration, const nrg_spike_io*
     double* tot = tt.as<double>();
     if (rc == NRG_OK) rc = run_fill(ctx, tPos, (long long)(2 * nw), 0.0);
     if (rc == NRG_OK) rc = run_fill(ctx, tot, 4LL * M.nMat, 0.0);
+    clk.mark(0);
     if (rc == NRG_OK) {
         OpView old;
         old.dense = dIMS;
@@ -929,6 +973,7 @@ static int spike_common(nrg_context* ctx, int32_t iteration, const nrg_spike_io*
         if (cfs) rc = spike_cfs_device(ctx, iteration, it, old, dR, tPos, tNeg, tot);
         else rc = spike_t0_device(ctx, iteration, it, gs, old, tPos, tNeg);
     }
+    clk.mark(1);
     // add into the caller's bins (weight column = second column)
     std::vector<double> hp(nw), hn(nw);
     if (rc == NRG_OK && cudaMemcpyAsync(hp.data(), tPos, sizeof(double) * nw, cudaMemcpyDeviceToHost, ctx->stream) != cudaSuccess) rc = NRG_ERR_CUDA;
@@ -972,6 +1017,7 @@ static int spike_common(nrg_context* ctx, int32_t iteration, const nrg_spike_io*
         }
     }
     S.d_bi.release(); S.d_lst.release(); S.d_lstOff.release();
+    clk.mark(2);
     return rc;
 }
 

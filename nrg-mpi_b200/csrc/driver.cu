@@ -12,6 +12,7 @@
 //   live in host memory and cross to the device and back at every call.
 #include "internal.hpp"
 
+#include <chrono>
 #include <algorithm>
 #include <atomic>
 #include <cmath>
@@ -756,12 +757,12 @@ struct HostRestore {
 // host slots of the host-array driver: the module arrays a Fortran caller keeps
 // allocated (invariant matrices ping-pong, one eigenvector and one spectrum-matrix array
 // per iteration for the restore stock, the full stock of eigenvectors)
-constexpr size_t kHostIM = 0, kHostFV = 2, kHostV = 16, kHostIMS = 16 + 4096;
+constexpr size_t kHostIM = 0, kHostFV = 2, kHostRDM = 3, kHostV = 16, kHostIMS = 16 + 4096;
 
 // one step of the CFS loop (cfsSpectrumCalculation, module.F90:1683-1706) through the
 // drop-in spike entry points, from the restore stock of iteration N and N-1
 int cfs_step_drop_in(nrg_context* ctx, int N, const std::vector<RestoreView>& its, int nb0, const double* ims0,
-                     const std::vector<int>& fsi, const std::vector<int>& map, const std::vector<double>& rdm,
+                     const std::vector<int>& fsi, const std::vector<int>& map, const double* rdm, long long nrdm,
                      double* binPos, double* binNeg, double* tot) {
     const Model& M = ctx->model;
     const RestoreView& R = its[N - M.first];
@@ -774,8 +775,8 @@ int cfs_step_drop_in(nrg_context* ctx, int N, const std::vector<RestoreView>& it
     sio.numberOfBasis_old = has_prev ? its[N - 1 - M.first].nb : nb0;
     sio.invariant_matrix_spectrum = has_prev ? its[N - 1 - M.first].ims : ims0;
     sio.fullSubspaceInfo = fsi.data(); sio.mapFullSubspaceInfo = map.data();
-    sio.elementNumFullSubspace = (int32_t)(fsi.size() / (M.nVar + 6)); sio.reducedDensityMatrix = rdm.data();
-    sio.sizeOfReducedDensity = (int64_t)rdm.size(); sio.numberOfBin = M.numberOfBin();
+    sio.elementNumFullSubspace = (int32_t)(fsi.size() / (M.nVar + 6)); sio.reducedDensityMatrix = rdm;
+    sio.sizeOfReducedDensity = (int64_t)nrdm; sio.numberOfBin = M.numberOfBin();
     sio.binnedSpikePositive = binPos; sio.binnedSpikeNegative = binNeg;
     sio.total_sum = tot;
     if (N == M.nIter) return nrg_spike_zero_temperature(ctx, N, &sio);
@@ -816,8 +817,8 @@ int resume_drop_in(nrg_context* ctx, nrg_run_output* out, cudaEvent_t* ev, const
             NRG_TRY(restart_save(path, M, N, hami, D.its, D.nb0, D.ims0.data(), D.rdm.data(), (long long)D.rdm.size(),
                                  D.fsi.data(), nfsi, D.map.data(), D.binPos.data(), D.binNeg.data(), nbin));
         }
-        NRG_TRY(cfs_step_drop_in(ctx, N, D.its, D.nb0, D.ims0.data(), D.fsi, D.map, D.rdm, D.binPos.data(),
-                                 D.binNeg.data(), tot.data()));
+        NRG_TRY(cfs_step_drop_in(ctx, N, D.its, D.nb0, D.ims0.data(), D.fsi, D.map, D.rdm.data(),
+                                 (long long)D.rdm.size(), D.binPos.data(), D.binNeg.data(), tot.data()));
     }
     NRG_CUDA_TRY(cudaEventRecord(ev[3], ctx->stream));
     NRG_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
@@ -855,6 +856,9 @@ int run_drop_in(nrg_context* ctx, const nrg_run_input* in, nrg_run_output* out, 
     }
     ctx->host_pageable = in->host_arrays_pageable != 0;
     if (load) return resume_drop_in(ctx, out, ev, rpath, save);
+    // profiling: the replay's own host work = its wall clock less the entry calls' parts
+    const auto wall0 = std::chrono::steady_clock::now();
+    const double entries0 = ctx->entry_s[0] + ctx->entry_s[1] + ctx->entry_s[2];
     if (out && out->thermo)   // thermodynamics are the caller's part of postprocess here
         for (int k = 0; k < 3 * (M.nIter - M.first + 1); ++k) out->thermo[k] = std::nan("");
     const int nVar = M.nVar, rs = nVar + 3, rsf = nVar + 6, first = M.first, nIter = M.nIter;
@@ -890,6 +894,14 @@ int run_drop_in(nrg_context* ctx, const nrg_run_input* in, nrg_run_output* out, 
     std::vector<double> fE;
     HostBuf& hFV = ctx->hslot(kHostFV);
     long long nFV = 0;
+    // postprocess.F90's copy of the kept eigenvector columns into the full stock runs on a
+    // host thread beside the next routine calls; it is joined before the stock grows and
+    // before the density matrices read it (and on every way out of this function)
+    struct Joiner {
+        std::thread t;
+        void join() { if (t.joinable()) t.join(); }
+        ~Joiner() { join(); }
+    } stock_copy;
     long long pointFBI = 1, pointFBO = 1, pointFS = 1, pointFV = 1, sizeRDM = 0;
     for (int it = first; it <= nIter; ++it) {
         const int idx = it - first;
@@ -960,6 +972,12 @@ int run_drop_in(nrg_context* ctx, const nrg_run_input* in, nrg_run_output* out, 
                 fbi.insert(fbi.end(), bi.begin(), bi.end());
                 std::vector<int> kcount, kfirst;
                 kept_in_sectors(si, nsub, bo_re, nbk, nVar, &kcount, &kfirst);
+                long long add = 0;
+                for (int s = 0; s < nsub; ++s) add += (long long)si[(size_t)s * rs + nVar] * kcount[s];
+                stock_copy.join();
+                NRG_TRY(hFV.ensure(sizeof(double) * (size_t)std::max(nFV + add, 1LL), true));
+                struct Run { double* dst; const double* src; size_t n; };
+                std::vector<Run> runs;
                 for (int s = 0; s < nsub; ++s) {
                     const int k = kcount[s], first_out = kfirst[s];
                     if (k == 0) continue;
@@ -973,12 +991,14 @@ int run_drop_in(nrg_context* ctx, const nrg_run_input* in, nrg_run_output* out, 
                     fsi.push_back(0);
                     sizeRDM += (long long)k * k;
                     const long long c0 = (long long)si[(size_t)s * rs + nVar + 1] - 1;
-                    NRG_TRY(hFV.ensure(sizeof(double) * (size_t)(nFV + (long long)d * k), true));
-                    std::memcpy(hFV.as<double>() + nFV, Vnew + c0, sizeof(double) * (size_t)d * k);
+                    runs.push_back({hFV.as<double>() + nFV, Vnew + c0, (size_t)d * k});
                     nFV += (long long)d * k;
                     pointFV += (long long)d * k;
                     ++pointFS;
                 }
+                stock_copy.t = std::thread([runs = std::move(runs)]() {
+                    for (const Run& r : runs) std::memcpy(r.dst, r.src, sizeof(double) * r.n);
+                });
                 pointFBI += nb;
                 pointFBO += nbk;
             }
@@ -994,14 +1014,20 @@ int run_drop_in(nrg_context* ctx, const nrg_run_input* in, nrg_run_output* out, 
     const size_t nw = (size_t)nbin * std::max(M.nMat, 1);
     std::vector<double> binPos, binNeg;
     bin_energies(M, nbin, binPos, binNeg);
-    std::vector<double> rdm;
+    stock_copy.join();
+    double* rdm = nullptr;   // reducedDensityMatrix, a module array like the others
+    long long nrdm = 0;
     const int elementNum = (int)(pointFS - 1);
     if (spectrum && flag_truncation) {
         // initializeReducedDensity.F90:32-78
         int deg = 0;
         for (int i = 0; i < nb_old; ++i) deg += E[i] < 1.0e-8;
         const double pf = (double)deg;
-        rdm.assign((size_t)sizeRDM, 0.0);
+        HostBuf& hR = ctx->hslot(kHostRDM);
+        NRG_TRY(hR.ensure(sizeof(double) * (size_t)std::max(sizeRDM, 1LL)));
+        rdm = hR.as<double>();
+        nrdm = sizeRDM;
+        std::memset(rdm, 0, sizeof(double) * (size_t)nrdm);
         const int r0 = map[nIter + 1] - 1;
         int point = 1;
         for (int j = r0; j < elementNum; ++j) {
@@ -1018,7 +1044,7 @@ int run_drop_in(nrg_context* ctx, const nrg_run_input* in, nrg_run_output* out, 
         rio.fullBasisInput = fbi.data(); rio.numFullBasisInput = (int64_t)(fbi.size() / rs);
         rio.fullBasisOutput = fbo.data(); rio.numFullBasisOutput = (int64_t)(fbo.size() / rs);
         rio.fullEigenvector = hFV.as<double>(); rio.numFullEigenvector = (int64_t)nFV;
-        rio.reducedDensityMatrix = rdm.data(); rio.sizeOfReducedDensity = (int64_t)rdm.size();
+        rio.reducedDensityMatrix = rdm; rio.sizeOfReducedDensity = (int64_t)nrdm;
         rio.pointReducedDensity = &point;
         std::vector<double> tr(std::max(nIter - startTrancation, 1));
         rio.trace = tr.data();
@@ -1042,16 +1068,19 @@ int run_drop_in(nrg_context* ctx, const nrg_run_input* in, nrg_run_output* out, 
                 int32_t hami[20];
                 const int nbh = N == startTrancation ? rest[nIt - 1].nb : rest[N - 1 - first].nb;
                 restart_hami(M, nbh, startTrancation, flag_truncation, hami);
-                NRG_TRY(restart_save(rpath, M, N, hami, views, nb0, ims0, rdm.data(), (long long)rdm.size(),
+                NRG_TRY(restart_save(rpath, M, N, hami, views, nb0, ims0, rdm, nrdm,
                                      fsi.data(), (long long)elementNum, map.data(), binPos.data(), binNeg.data(),
                                      nbin));
             }
-            NRG_TRY(cfs_step_drop_in(ctx, N, views, nb0, ims0, fsi, map, rdm, binPos.data(), binNeg.data(),
+            NRG_TRY(cfs_step_drop_in(ctx, N, views, nb0, ims0, fsi, map, rdm, nrdm, binPos.data(), binNeg.data(),
                                      tot.data()));
         }
     }
     NRG_CUDA_TRY(cudaEventRecord(ev[3], ctx->stream));
     NRG_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+    if (ctx->profiling)
+        ctx->replay_host_s += std::chrono::duration<double>(std::chrono::steady_clock::now() - wall0).count() -
+                              (ctx->entry_s[0] + ctx->entry_s[1] + ctx->entry_s[2] - entries0);
     if (out) {
         out->numberOfBin = nbin;
         out->startTrancation = startTrancation;

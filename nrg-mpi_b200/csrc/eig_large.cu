@@ -353,13 +353,6 @@ __global__ void __launch_bounds__(TT, 1) k_tri_cluster(const LSec* __restrict__ 
             const int mB = first_own(k + 1);
             const int nq = (cnt - mB + 3) / 4, nrb = (n - k - 1 + 255) / 256, nitems = nq * nrb;
             const double* vj = VO + j * MM;
-            for (int o = warp; o < 2 * j; o += NW) {
-                const double* colp = (o < j) ? WO + o * MM : VO + (o - j) * MM;
-                double s = 0.0;
-                for (int mm = mB + lane; mm < cnt; mm += 32) s = fma(colp[mm], vj[mm], s);
-                s = warp_sum(s);
-                if (lane < CL) cluster.map_shared_rank(P2, lane)[rank * P2W + (o < j ? o : NB + (o - j))] = s;
-            }
             const bool pivot_owner = (rank == (k + 1) % CL);
             if (pivot_owner && k + 1 <= last) {
                 for (int e = tid; e < 2 * j * CL; e += TT) {
@@ -368,9 +361,19 @@ __global__ void __launch_bounds__(TT, 1) k_tri_cluster(const LSec* __restrict__ 
                     cluster.map_shared_rank(pivn, r)[q < j ? q : NB + (q - j)] = val;
                 }
             }
+            for (int o = warp; o < 2 * j; o += NW) {
+                const double* colp = (o < j) ? WO + o * MM : VO + (o - j) * MM;
+                double s = 0.0;
+                for (int mm = mB + lane; mm < cnt; mm += 32) s = fma(colp[mm], vj[mm], s);
+                s = warp_sum(s);
+                if (lane < CL) cluster.map_shared_rank(P2, lane)[rank * P2W + (o < j ? o : NB + (o - j))] = s;
+            }
             // y = A v in work items of four own columns x 256 rows, one warp each, 32
-            // independent loads per lane; partial sums per row batch, added in a fixed order
+            // independent loads per lane; partial sums per row batch, added in a fixed order.
+            // Each warp also sums v(c) times its partial products: the block's part of y.v
+            // without a block reduction of its own.
             {
+                double yvw = 0.0;
                 for (int item = warp; item < nitems; item += NW) {
                     const int g = item % nq, rb = item / nq, m0 = mB + 4 * g;
                     const int rbase = k + 1 + rb * 256;
@@ -393,26 +396,31 @@ __global__ void __launch_bounds__(TT, 1) k_tri_cluster(const LSec* __restrict__ 
                         for (int c = 0; c < 4; ++c) sc[c] = fma(x[c][u], xv[u], sc[c]);
 #pragma unroll
                     for (int c = 0; c < 4; ++c) sc[c] = warp_sum(sc[c]);
+#pragma unroll
+                    for (int c = 0; c < 4; ++c)
+                        if (m0 + c < cnt) yvw = fma(sc[c], vj[m0 + c], yvw);
                     if (lane == 0)
 #pragma unroll
                         for (int c = 0; c < 4; ++c)
                             if (m0 + c < cnt) ysp[rb * MM + m0 + c] = sc[c];
                 }
+                if (lane == 0) red[warp] = yvw;
                 __syncthreads();
             }
             const int mc = mB + tid;
             const bool own_c = mc < cnt;
-            double yvp = 0.0;
             if (own_c) {
                 double sy = 0.0;
                 for (int rb = 0; rb < nrb; ++rb) sy += ysp[rb * MM + mc];
                 ys[mc] = sy;
-                yvp = sy * vj[mc];
                 if (tid == 0 && pivot_owner && k + 1 <= last)
                     for (int r = 0; r < CL; ++r) cluster.map_shared_rank(Y1, r)[0] = sy;
             }
-            yvp = block_sum(yvp, red);
-            if (tid < CL) cluster.map_shared_rank(P2, tid)[rank * P2W + 2 * NB] = yvp;
+            if (tid < CL) {
+                double yvp = 0.0;
+                for (int w = 0; w < NW; ++w) yvp += red[w];   // the same order in every block
+                cluster.map_shared_rank(P2, tid)[rank * P2W + 2 * NB] = yvp;
+            }
             cluster.sync();
             // ---- C: totals, w of the own rows and of the next pivot row ----
             if (tid < 2 * j) {
@@ -1130,6 +1138,15 @@ __global__ void __launch_bounds__(256) k_bt_prep(const LSec* __restrict__ secs, 
     for (int e = tid; e < NBB * NBB; e += 256) Tq[e] = Ts[e];
 }
 
+// 8-byte asynchronous global-to-shared copies (zero-filled when bytes is 0)
+__device__ __forceinline__ void cp_async8(double* dst, const double* src, int bytes) {
+    const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(d), "l"(src), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
+
 // Z(:, c0 .. c0+CBK-1) <- H_0 ... H_{n-2} Z(:, ...) panel by panel (last panel first), the
 // column block resident in shared memory; the result goes to the output
 template <int CBK>
@@ -1138,8 +1155,12 @@ __global__ void __launch_bounds__(256, 1) k_bt_apply(const LSec* __restrict__ se
     // The three small products of each panel, W = V^T Z, W2 = T W and Z -= V W2, on the
     // FP64 tensor pipe (mma.sync m8n8k4): the eight warps split the panel's 64 reflectors
     // (W, W2) or the chunk's 64 rows (the update) in slices of 8, and each warp covers the
-    // CBK columns in tiles of 8.
+    // CBK columns in tiles of 8.  What the products read streams through two shared
+    // buffers of 64 x 65 doubles with asynchronous copies one step ahead: per panel the
+    // chunks of 64 rows of V for W, then T, then the chunks again for the update, then the
+    // next panel's first chunk.
     constexpr int NTJ = CBK / 8;
+    constexpr int BUF = NBB * 65;
     extern __shared__ double asm_[];
     int bid = blockIdx.x, s = 0;
     for (; s < nsec; ++s) {
@@ -1150,12 +1171,11 @@ __global__ void __launch_bounds__(256, 1) k_bt_apply(const LSec* __restrict__ se
     if (s >= nsec) return;
     const LSec sec = secs[s];
     LView L = lview(sec, eigbuf, wsd, wsi);
-    const int n = L.n, nr = n - 1, c0 = bid * CBK, nc = min(CBK, n - c0);
+    const int n = L.n, c0 = bid * CBK, nc = min(CBK, n - c0);
     double* Zs = asm_;                      // Zs[j * n + row]
-    double* Vs = Zs + (size_t)n * CBK;      // Vs[c * 65 + r]
-    double* Ws = Vs + NBB * 65;             // Ws[c * CBK + j]
+    double* Vb = Zs + (size_t)n * CBK;      // two buffers: Vs[c * 65 + r] (a chunk) or T (column-major)
+    double* Ws = Vb + 2 * BUF;              // Ws[c * CBK + j]
     double* W2 = Ws + NBB * CBK;
-    double* Ts = W2 + NBB * CBK;            // T column-major
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int g = lane >> 2, q4 = lane & 3;
     const int wr = 8 * warp;                // this warp's slice of reflectors / rows
@@ -1163,84 +1183,102 @@ __global__ void __launch_bounds__(256, 1) k_bt_apply(const LSec* __restrict__ se
         for (int row = tid; row < n; row += 256)
             Zs[(size_t)j * n + row] = j < nc ? L.Z[(size_t)row + (size_t)(c0 + j) * n] : 0.0;
     const int qmax = (n - 2) / NBB;
+    // the load sequence: step t of panel q is a V chunk (t < C: for W; t > C: for the
+    // update, chunk t - C - 1) or T (t == C), with C = ceil(mr / 64) chunks per pass
+    auto chunks = [&](int q) { return (n - 1 - q * NBB + 63) / 64; };
+    auto issue = [&](int q, int t, double* dst) {
+        const int mr = n - 1 - q * NBB, C = chunks(q);
+        if (t == C) {
+            const double* Tq = L.R + (size_t)q * NBB * NBB;
+            for (int e = tid; e < NBB * NBB; e += 256) cp_async8(dst + e, Tq + e, 8);
+        } else {
+            const int i0 = 64 * (t < C ? t : t - C - 1), rows = min(64, mr - i0);
+            const double* Rp = L.R + bt_panel_off(n, q);
+            for (int e = tid; e < 64 * NBB; e += 256) {
+                const int r = e & 63, c = e >> 6;
+                const int rr = r < rows ? r : rows - 1;   // in bounds; nothing is read when zero-filled
+                cp_async8(dst + c * 65 + r, Rp + (size_t)(i0 + rr) + (size_t)c * mr, r < rows ? 8 : 0);
+            }
+        }
+        cp_async_commit();
+    };
+    int buf = 0;
+    issue(qmax, 0, Vb);
     for (int q = qmax; q >= 0; --q) {
-        const int jb = q * NBB, r0 = jb + 1, mr = n - r0;
-        (void)nr;
-        const double* Rp = L.R + bt_panel_off(n, q);
-        const double* Tq = L.R + (size_t)q * NBB * NBB;
-        for (int e = tid; e < NBB * NBB; e += 256) Ts[e] = Tq[e];
-        // W = V^T Z(r0:, :): W(i, j) for the warp's reflectors i
+        const int jb = q * NBB, r0 = jb + 1, mr = n - r0, C = chunks(q);
         double acc[NTJ][2];
 #pragma unroll
         for (int t = 0; t < NTJ; ++t) acc[t][0] = acc[t][1] = 0.0;
-        for (int i0 = 0; i0 < mr; i0 += 64) {
-            const int rows = min(64, mr - i0);
+        for (int t = 0; t <= 2 * C; ++t) {
+            // the next step's load (the next panel's first chunk after the last step) into
+            // the buffer the previous step has finished with
+            double* nxt = Vb + (buf ^ 1) * BUF;
+            if (t < 2 * C) issue(q, t + 1, nxt);
+            else if (q > 0) issue(q - 1, 0, nxt);
+            if (t < 2 * C || q > 0) cp_async_wait<1>();
+            else cp_async_wait<0>();
             __syncthreads();
-            for (int e = tid; e < 64 * NBB; e += 256) {
-                const int r = e & 63, c = e >> 6;
-                Vs[c * 65 + r] = r < rows ? Rp[(size_t)(i0 + r) + (size_t)c * mr] : 0.0;
-            }
-            __syncthreads();
-            const double* zr = Zs + r0 + i0;
+            const double* Vs = Vb + buf * BUF;
+            if (t < C) {
+                // W = V^T Z(r0:, :): W(i, j) for the warp's reflectors i
+                const int i0 = 64 * t, rows = min(64, mr - i0);
+                const double* zr = Zs + r0 + i0;
 #pragma unroll 4
-            for (int k0 = 0; k0 < 64; k0 += 4) {
-                const int kk = k0 + q4;
-                const double a = Vs[(wr + g) * 65 + kk];
+                for (int k0 = 0; k0 < 64; k0 += 4) {
+                    const int kk = k0 + q4;
+                    const double a = Vs[(wr + g) * 65 + kk];
 #pragma unroll
-                for (int t = 0; t < NTJ; ++t) {
-                    const double b = kk < rows ? zr[(size_t)(t * 8 + g) * n + kk] : 0.0;
-                    nrg::cta_dmma(acc[t][0], acc[t][1], a, b);
+                    for (int u = 0; u < NTJ; ++u) {
+                        const double b = kk < rows ? zr[(size_t)(u * 8 + g) * n + kk] : 0.0;
+                        nrg::cta_dmma(acc[u][0], acc[u][1], a, b);
+                    }
+                }
+                if (t == C - 1) {
+#pragma unroll
+                    for (int u = 0; u < NTJ; ++u) {
+                        Ws[(wr + g) * CBK + u * 8 + 2 * q4] = acc[u][0];
+                        Ws[(wr + g) * CBK + u * 8 + 2 * q4 + 1] = acc[u][1];
+                    }
+                }
+            } else if (t == C) {
+                // W2 = T W (T upper triangular, zero below the diagonal)
+#pragma unroll
+                for (int u = 0; u < NTJ; ++u) acc[u][0] = acc[u][1] = 0.0;
+#pragma unroll 4
+                for (int k0 = 0; k0 < NBB; k0 += 4) {
+                    const double a = Vs[(wr + g) + (k0 + q4) * NBB];
+#pragma unroll
+                    for (int u = 0; u < NTJ; ++u) nrg::cta_dmma(acc[u][0], acc[u][1], a, Ws[(k0 + q4) * CBK + u * 8 + g]);
+                }
+#pragma unroll
+                for (int u = 0; u < NTJ; ++u) {
+                    W2[(wr + g) * CBK + u * 8 + 2 * q4] = acc[u][0];
+                    W2[(wr + g) * CBK + u * 8 + 2 * q4 + 1] = acc[u][1];
+                }
+            } else {
+                // Z(r0:, :) -= V W2 on the chunk's 64 rows
+                const int i0 = 64 * (t - C - 1), rows = min(64, mr - i0);
+#pragma unroll
+                for (int u = 0; u < NTJ; ++u) acc[u][0] = acc[u][1] = 0.0;
+#pragma unroll 4
+                for (int k0 = 0; k0 < NBB; k0 += 4) {
+                    const double a = Vs[(k0 + q4) * 65 + wr + g];
+#pragma unroll
+                    for (int u = 0; u < NTJ; ++u) nrg::cta_dmma(acc[u][0], acc[u][1], a, W2[(k0 + q4) * CBK + u * 8 + g]);
+                }
+                const int row = wr + g;
+                if (row < rows) {
+                    double* zr = Zs + r0 + i0 + row;
+#pragma unroll
+                    for (int u = 0; u < NTJ; ++u) {
+                        zr[(size_t)(u * 8 + 2 * q4) * n] -= acc[u][0];
+                        zr[(size_t)(u * 8 + 2 * q4 + 1) * n] -= acc[u][1];
+                    }
                 }
             }
-        }
-#pragma unroll
-        for (int t = 0; t < NTJ; ++t) {
-            Ws[(wr + g) * CBK + t * 8 + 2 * q4] = acc[t][0];
-            Ws[(wr + g) * CBK + t * 8 + 2 * q4 + 1] = acc[t][1];
-        }
-        __syncthreads();
-        // W2 = T W (T upper triangular, zero below the diagonal)
-#pragma unroll
-        for (int t = 0; t < NTJ; ++t) acc[t][0] = acc[t][1] = 0.0;
-#pragma unroll 4
-        for (int k0 = 0; k0 < NBB; k0 += 4) {
-            const double a = Ts[(wr + g) + (k0 + q4) * NBB];
-#pragma unroll
-            for (int t = 0; t < NTJ; ++t) nrg::cta_dmma(acc[t][0], acc[t][1], a, Ws[(k0 + q4) * CBK + t * 8 + g]);
-        }
-#pragma unroll
-        for (int t = 0; t < NTJ; ++t) {
-            W2[(wr + g) * CBK + t * 8 + 2 * q4] = acc[t][0];
-            W2[(wr + g) * CBK + t * 8 + 2 * q4 + 1] = acc[t][1];
-        }
-        // Z(r0:, :) -= V W2, one chunk of 64 rows at a time
-        for (int i0 = 0; i0 < mr; i0 += 64) {
-            const int rows = min(64, mr - i0);
             __syncthreads();
-            for (int e = tid; e < 64 * NBB; e += 256) {
-                const int r = e & 63, c = e >> 6;
-                Vs[c * 65 + r] = r < rows ? Rp[(size_t)(i0 + r) + (size_t)c * mr] : 0.0;
-            }
-            __syncthreads();
-#pragma unroll
-            for (int t = 0; t < NTJ; ++t) acc[t][0] = acc[t][1] = 0.0;
-#pragma unroll 4
-            for (int k0 = 0; k0 < NBB; k0 += 4) {
-                const double a = Vs[(k0 + q4) * 65 + wr + g];
-#pragma unroll
-                for (int t = 0; t < NTJ; ++t) nrg::cta_dmma(acc[t][0], acc[t][1], a, W2[(k0 + q4) * CBK + t * 8 + g]);
-            }
-            const int row = wr + g;
-            if (row < rows) {
-                double* zr = Zs + r0 + i0 + row;
-#pragma unroll
-                for (int t = 0; t < NTJ; ++t) {
-                    zr[(size_t)(t * 8 + 2 * q4) * n] -= acc[t][0];
-                    zr[(size_t)(t * 8 + 2 * q4 + 1) * n] -= acc[t][1];
-                }
-            }
+            buf ^= 1;
         }
-        __syncthreads();
     }
     for (int j = 0; j < nc; ++j)
         for (int row = tid; row < n; row += 256)
@@ -1595,8 +1633,8 @@ int syev_large(nrg_context* ctx, const std::vector<SyevSector>& in, double* d_V,
         int dev = 0, optin = 0;
         NRG_CUDA_TRY(cudaGetDevice(&dev));
         NRG_CUDA_TRY(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
-        auto apply_smem = [&](int c) {
-            return sizeof(double) * ((size_t)maxn * c + NBB * 65 + 2 * NBB * c + NBB * NBB);
+        auto apply_smem = [&](int c) {   // Z block, two staging buffers, W and W2
+            return sizeof(double) * ((size_t)maxn * c + 2 * NBB * 65 + 2 * NBB * c);
         };
         const size_t prep_smem = sizeof(double) * (NBB * 65 + 2 * NBB * NBB);
         const int cbk = apply_smem(16) <= (size_t)optin ? 16 : (apply_smem(8) <= (size_t)optin ? 8 : 0);

@@ -138,6 +138,9 @@ struct nrg_context {
     long long h2d = 0, d2h = 0;
     long long tri_launches = 0;
     double tri_ms = 0.0, tri_flops = 0.0, tri_bytes = 0.0;
+    double entry_s[3] = {0.0, 0.0, 0.0};   // drop-in entries: staging in, device, out
+    long long entry_calls = 0;
+    double replay_host_s = 0.0;
     // driver-owned persistent storage, reused across runs
     std::deque<nrg::DevBuf> store;
     std::vector<nrg::Sectors> iter_sectors;

@@ -145,7 +145,8 @@ class Stats(ctypes.Structure):
     _fields_ = [("launches", c_int64), ("syev_launches", c_int64), ("syev_ms", c_double),
                 ("syev_flops", c_double), ("h2d_bytes", c_int64), ("d2h_bytes", c_int64),
                 ("tri_launches", c_int64), ("tri_ms", c_double), ("tri_flops", c_double),
-                ("tri_bytes", c_double)]
+                ("tri_bytes", c_double), ("entry_in_s", c_double), ("entry_compute_s", c_double),
+                ("entry_out_s", c_double), ("entry_calls", c_int64), ("replay_host_s", c_double)]
 
 
 _lib = None

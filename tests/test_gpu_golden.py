@@ -8,7 +8,11 @@ density-matrix trace of every backward step, and the nonzero spectral bins:
 * the N_keep = 2048 SIAM workload, all 60 iterations with density matrices and the T = 0
   CFS spectrum (the second bench object);
 * the N_keep = 4096 SIAM workload (the bench headline's model), its first 14 iterations
-  (-1..12), the model cut there.
+  (-1..12), the model cut there;
+* the two-orbital Hund model at N_keep = 8192 (16 local states), its first 5 iterations
+  (-1..3), forward sweep only: 131,104 states at iteration 3 in sectors of order up to
+  ~8,800, past the cluster tridiagonalisation's and the shared-memory back-transformation's
+  size limits, with tied sort keys in prepareBasis.
 
 Both the device-resident run and the drop-in replay (every routine through its entry point
 with host arrays, page-locked, and for the N_keep = 4096 case also pageable) are compared.  Tolerances: kept counts and state counts equal (the
@@ -54,6 +58,20 @@ def _bins(g, key, n):
     return w
 
 
+def _compare_forward(res, g, device_resident):
+    assert np.array_equal(np.asarray(res["kept"], dtype=np.int32), g["kept"])
+    assert np.array_equal(np.asarray(res["numberOfBasisFull"], dtype=np.int32), g["numberOfBasisFull"])
+    gse = g["groundStateEnergy"]
+    assert np.max(np.abs(res["groundStateEnergy"] - gse) / np.maximum(1.0, np.abs(gse))) <= E_TOL
+    flow = g["flow"]
+    ok = ~np.isnan(flow)
+    got = res["flow"][:, :flow.shape[1]]
+    assert np.max(np.abs(got[ok] - flow[ok]) / np.maximum(1.0, np.abs(flow[ok]))) <= E_TOL
+    if device_resident:
+        th = g["thermo"]
+        assert np.max(np.abs(res["thermo"] - th) / np.maximum(1.0, np.abs(th))) <= THERMO_TOL
+
+
 def _compare(res, g, device_resident):
     assert int(res["startTrancation"]) == int(g["startTrancation"])
     assert np.array_equal(np.asarray(res["kept"], dtype=np.int32), g["kept"])
@@ -92,6 +110,22 @@ def test_whole_run_matches_golden(ctx_factory, name):
         # gather the runs they read on the host instead of reading pinned memory directly
         res3 = ctx.run(spectrum=True, flow_stride=64, host_drop_in=True, host_pageable=True)
         _compare(res3, g, device_resident=False)
+    ctx.release_storage()
+
+
+def _two_orbital_window():
+    inp = model.config(4, n_iterations=5)
+    inp.flag_spectrum = False
+    return inp
+
+
+def test_two_orbital_window_matches_golden(ctx_factory):
+    g = _golden("two_orbital_nkeep8192_n5")
+    ctx = ctx_factory(_two_orbital_window())
+    res = ctx.run(spectrum=False, flow_stride=64)
+    _compare_forward(res, g, device_resident=True)
+    res2 = ctx.run(spectrum=False, flow_stride=64, host_drop_in=True)
+    _compare_forward(res2, g, device_resident=False)
     ctx.release_storage()
 
 
