@@ -232,14 +232,30 @@ constexpr int TRW = 128;    // rows per staged chunk of the trailing update
 constexpr int P2W = 2 * NB + 2;   // partials per block: W^T v | V^T v | y.v
 
 struct TriLayout {
-    int MM, PN, NRB;   // own indices per block, rows (even), row batches of 256
+    int MM, PN, NRB;   // own indices per block, rows (even), row batches of 512 (rounded up)
     __host__ __device__ long long doubles(int CL) const {
-        // the panel rows AR share their space with the staging of the trailing update
+        // the panel rows AR share their space with the staging of the trailing update; v
+        // for the product (PN + 2, 16-byte aligned) last
         const long long stage = (long long)NB * MM > 2LL * NB * TRW ? (long long)NB * MM : 2LL * NB * TRW;
         return 2LL * NB * MM + PN + MM + (long long)CL * P2W + CL + 2 + 2LL * NB + 2LL * NB + P2W + 32 +
-               stage + (long long)NRB * MM + 3LL * NB;
+               stage + (long long)NRB * MM + 3LL * NB + PN + 4;
     }
 };
+
+// the sums over the warp of four values: lane l ends with the total of value (l >> 3) & 3
+// (every lane of a group of eight with the same bits), by halving exchanges
+__device__ __forceinline__ double warp_sum4(double a0, double a1, double a2, double a3, int lane) {
+    const bool h16 = lane & 16, h8 = lane & 8;
+    double k0 = h16 ? a2 : a0, k1 = h16 ? a3 : a1;
+    k0 += __shfl_xor_sync(0xffffffffu, h16 ? a0 : a2, 16);
+    k1 += __shfl_xor_sync(0xffffffffu, h16 ? a1 : a3, 16);
+    double kk = h8 ? k1 : k0;
+    kk += __shfl_xor_sync(0xffffffffu, h8 ? k0 : k1, 8);
+    kk += __shfl_xor_sync(0xffffffffu, kk, 4);
+    kk += __shfl_xor_sync(0xffffffffu, kk, 2);
+    kk += __shfl_xor_sync(0xffffffffu, kk, 1);
+    return kk;
+}
 
 __device__ __forceinline__ double warp_sum(double v) {
     for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
@@ -286,11 +302,16 @@ __global__ void __launch_bounds__(TT, 1) k_tri_cluster(const LSec* __restrict__ 
     double* stW = stV + NB * TRW;          // trailing update; NB x TRW
     double* ysp = AR + ((size_t)NB * MM > 2 * NB * TRW ? (size_t)NB * MM : 2 * NB * TRW);   // NRB x MM
     double* pan = ysp + (size_t)lay.NRB * MM;   // D | E | tau of the panel's columns
+    // v of the current column for the product, row r at vv[r + par]: with par the parity
+    // of the own columns' offsets, rows pair up on 16-byte boundaries in A and in vv
+    double* vv = sm + ((pan - sm + 3 * NB + 1) & ~(ptrdiff_t)1);
     double* Vg = L.VW;
     double* Wg = L.VW + (size_t)NB * n;
     double* A = L.A;
     const int cnt = (n - rank + CL - 1) / CL;                           // own indices rank + CL*m
     auto first_own = [&](int i0) { return (i0 - rank + CL - 1) / CL; };  // i0 >= 0
+    // CL is even, so every own column's offset (rank + CL m) n has the parity of rank n
+    const int par = (int)(((reinterpret_cast<uintptr_t>(A) >> 3) + (uintptr_t)rank * n) & 1);
 
     for (int p = 0; p < n - 1; p += NB) {
         const int last = min(p + NB - 1, n - 2);
@@ -343,15 +364,20 @@ __global__ void __launch_bounds__(TT, 1) k_tri_cluster(const LSec* __restrict__ 
                 tau = (beta - alpha) / beta;
                 scal = 1.0 / (alpha - beta);
             }
-            // v(k+1) = 1 is implied: cv(k+1) keeps alpha, which every thread reads above
-            for (int r = k + 2 + tid; r < n; r += TT) cv[r] = xn2 == 0.0 ? 0.0 : cv[r] * scal;
+            // v into vv (cv(k+1) keeps alpha, which every thread reads above): v(k+1) = 1, and
+            // the row before it 0 for a product that starts one row early to pair the rows
+            for (int r = k + 2 + tid; r < n; r += TT) vv[r + par] = xn2 == 0.0 ? 0.0 : cv[r] * scal;
+            if (tid == 0) { vv[k + par] = 0.0; vv[k + 1 + par] = 1.0; }
             if (act && i >= k + 1) VO[j * MM + m] = (i == k + 1) ? 1.0 : (xn2 == 0.0 ? 0.0 : c * scal);
             if (tid == 0) { pan[NB + j] = beta; pan[2 * NB + j] = tau; }
             __syncthreads();
             // ---- B: partial W^T v, V^T v over the own rows, the next pivot row, then y of
             // the own columns and partial y.v ----
             const int mB = first_own(k + 1);
-            const int nq = (cnt - mB + 3) / 4, nrb = (n - k - 1 + 255) / 256, nitems = nq * nrb;
+            // the product's rows start at rs = k + 1 or k (vv(k) = 0), so that the offsets of
+            // (rs, rs + 1) in A and in vv are even
+            const int rs = (k + 1) - ((k + 1 + par) & 1);
+            const int nq = (cnt - mB + 3) / 4, nrb = (n - rs + 511) / 512, nitems = nq * nrb;
             const double* vj = VO + j * MM;
             const bool pivot_owner = (rank == (k + 1) % CL);
             if (pivot_owner && k + 1 <= last) {
@@ -368,42 +394,72 @@ __global__ void __launch_bounds__(TT, 1) k_tri_cluster(const LSec* __restrict__ 
                 s = warp_sum(s);
                 if (lane < CL) cluster.map_shared_rank(P2, lane)[rank * P2W + (o < j ? o : NB + (o - j))] = s;
             }
-            // y = A v in work items of four own columns x 256 rows, one warp each, 32
-            // independent loads per lane; partial sums per row batch, added in a fixed order.
-            // Each warp also sums v(c) times its partial products: the block's part of y.v
-            // without a block reduction of its own.
+            // y = A v in work items of four own columns x 512 rows (256 row pairs), one warp
+            // each: 16-byte loads of row pairs, eight pairs per lane and column in two
+            // batches of 16 loads, bounds checked only in the last row batch; one exchange
+            // reduction of the four sums per item; partial sums per row batch, added in a
+            // fixed order.  Each warp also sums v(c) times its partial products: the
+            // block's part of y.v without a block reduction of its own.
             {
                 double yvw = 0.0;
                 for (int item = warp; item < nitems; item += NW) {
                     const int g = item % nq, rb = item / nq, m0 = mB + 4 * g;
-                    const int rbase = k + 1 + rb * 256;
-                    const double* col[4];
-#pragma unroll
-                    for (int c = 0; c < 4; ++c) col[c] = A + (size_t)(rank + CL * min(m0 + c, cnt - 1)) * n;
-                    double x[4][8], xv[8];
-#pragma unroll
-                    for (int u = 0; u < 8; ++u) {
-                        const int r = rbase + lane + 32 * u;
-                        const bool in = r < n;
-                        xv[u] = in ? (r == k + 1 ? 1.0 : cv[r]) : 0.0;
-#pragma unroll
-                        for (int c = 0; c < 4; ++c) x[c][u] = in ? col[c][r] : 0.0;
-                    }
-                    double sc[4] = {0.0, 0.0, 0.0, 0.0};
-#pragma unroll
-                    for (int u = 0; u < 8; ++u)
-#pragma unroll
-                        for (int c = 0; c < 4; ++c) sc[c] = fma(x[c][u], xv[u], sc[c]);
-#pragma unroll
-                    for (int c = 0; c < 4; ++c) sc[c] = warp_sum(sc[c]);
+                    const int R0 = rs + 512 * rb;
+                    const double2* col[4];
 #pragma unroll
                     for (int c = 0; c < 4; ++c)
-                        if (m0 + c < cnt) yvw = fma(sc[c], vj[m0 + c], yvw);
-                    if (lane == 0)
+                        col[c] = reinterpret_cast<const double2*>(A + (size_t)(rank + CL * min(m0 + c, cnt - 1)) * n + R0);
+                    const double2* vp = reinterpret_cast<const double2*>(vv + R0 + par);
+                    double sc[4] = {0.0, 0.0, 0.0, 0.0};
+                    const int np = (n - R0) / 2;   // whole pairs from R0 on
+                    constexpr int UB = 4;           // pairs per lane and column in one batch of loads
+                    if (np >= 256) {
 #pragma unroll
-                        for (int c = 0; c < 4; ++c)
-                            if (m0 + c < cnt) ysp[rb * MM + m0 + c] = sc[c];
+                        for (int h = 0; h < 8 / UB; ++h) {
+                            double2 x[4][UB], xv[UB];
+#pragma unroll
+                            for (int u = 0; u < UB; ++u) {
+                                const int pp = lane + 32 * (UB * h + u);
+                                xv[u] = vp[pp];
+#pragma unroll
+                                for (int c = 0; c < 4; ++c) x[c][u] = col[c][pp];
+                            }
+#pragma unroll
+                            for (int u = 0; u < UB; ++u)
+#pragma unroll
+                                for (int c = 0; c < 4; ++c) sc[c] = fma(x[c][u].y, xv[u].y, fma(x[c][u].x, xv[u].x, sc[c]));
+                        }
+                    } else {
+                        // the last row batch: whole pairs, then a last single row when n - R0 is odd
+                        for (int h = 0; h < 8 / UB; ++h) {
+                            double2 x[4][UB], xv[UB];
+#pragma unroll
+                            for (int u = 0; u < UB; ++u) {
+                                const int pp = lane + 32 * (UB * h + u);
+                                const bool in = pp < np, one = pp == np && R0 + 2 * pp == n - 1;
+                                const double* vs = vv + R0 + par + 2 * pp;
+                                xv[u] = in ? vp[pp] : make_double2(one ? vs[0] : 0.0, 0.0);
+#pragma unroll
+                                for (int c = 0; c < 4; ++c) {
+                                    const double* as = reinterpret_cast<const double*>(col[c] + pp);
+                                    x[c][u] = in ? col[c][pp] : make_double2(one ? as[0] : 0.0, 0.0);
+                                }
+                            }
+#pragma unroll
+                            for (int u = 0; u < UB; ++u)
+#pragma unroll
+                                for (int c = 0; c < 4; ++c) sc[c] = fma(x[c][u].y, xv[u].y, fma(x[c][u].x, xv[u].x, sc[c]));
+                        }
+                    }
+                    const double tot = warp_sum4(sc[0], sc[1], sc[2], sc[3], lane);
+                    const int mc4 = m0 + ((lane >> 3) & 3);
+                    if ((lane & 7) == 0 && mc4 < cnt) {
+                        ysp[rb * MM + mc4] = tot;
+                        yvw = fma(tot, vj[mc4], yvw);
+                    }
                 }
+                yvw += __shfl_xor_sync(0xffffffffu, yvw, 8);
+                yvw += __shfl_xor_sync(0xffffffffu, yvw, 16);
                 if (lane == 0) red[warp] = yvw;
                 __syncthreads();
             }
@@ -1317,7 +1373,7 @@ static int tri_cluster_cl(nrg_context* ctx, const LSec* dsec, int ns, int maxn, 
     TriLayout lay;
     lay.MM = (maxn + CL - 1) / CL;
     lay.PN = maxn + (maxn & 1);
-    lay.NRB = (maxn + 255) / 256;
+    lay.NRB = (maxn + 511) / 512;
     if (lay.MM > TT) return NRG_OK;
     const size_t smem = sizeof(double) * (size_t)lay.doubles(CL);
     int dev = 0, optin = 0;
