@@ -268,6 +268,7 @@ __device__ __forceinline__ double w_entry(double y, const double* Vr, const doub
                                           const double* t1, const double* t2, int j, double tau,
                                           double al, double v) {
     double s = y, s2 = 0.0;
+    #pragma unroll 4
     for (int q = 0; q < j; ++q) {
         s = fma(-Vr[q * stride], t1[q], s);
         s2 = fma(-Wr[q * stride], t2[q], s2);
@@ -336,6 +337,7 @@ __global__ void __launch_bounds__(TT, 1) k_tri_cluster(const LSec* __restrict__ 
             if (act) {
                 double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
                 int q = 0;
+                #pragma unroll 4
                 for (; q + 1 < j; q += 2) {
                     s0 = fma(VO[q * MM + m], piv[q], s0);
                     s1 = fma(WO[q * MM + m], piv[NB + q], s1);
@@ -387,12 +389,26 @@ __global__ void __launch_bounds__(TT, 1) k_tri_cluster(const LSec* __restrict__ 
                     cluster.map_shared_rank(pivn, r)[q < j ? q : NB + (q - j)] = val;
                 }
             }
-            for (int o = warp; o < 2 * j; o += NW) {
-                const double* colp = (o < j) ? WO + o * MM : VO + (o - j) * MM;
-                double s = 0.0;
-                for (int mm = mB + lane; mm < cnt; mm += 32) s = fma(colp[mm], vj[mm], s);
-                s = warp_sum(s);
-                if (lane < CL) cluster.map_shared_rank(P2, lane)[rank * P2W + (o < j ? o : NB + (o - j))] = s;
+            // the 2j partial dots over the own rows, four per warp (o = 4 g + c: W^T v for
+            // o < j, V^T v after), one exchange reduction for the four
+            for (int g = warp; 4 * g < 2 * j; g += NW) {
+                const double* colp[4];
+#pragma unroll
+                for (int c = 0; c < 4; ++c) {
+                    const int o = min(4 * g + c, 2 * j - 1);
+                    colp[c] = (o < j) ? WO + o * MM : VO + (o - j) * MM;
+                }
+                double s4[4] = {0.0, 0.0, 0.0, 0.0};
+                for (int mm = mB + lane; mm < cnt; mm += 32) {
+                    const double vm = vj[mm];
+#pragma unroll
+                    for (int c = 0; c < 4; ++c) s4[c] = fma(colp[c][mm], vm, s4[c]);
+                }
+                const double tot = warp_sum4(s4[0], s4[1], s4[2], s4[3], lane);
+                const int o = 4 * g + ((lane >> 3) & 3);
+                if (o < 2 * j)
+                    for (int r = lane & 7; r < CL; r += 8)
+                        cluster.map_shared_rank(P2, r)[rank * P2W + (o < j ? o : NB + (o - j))] = tot;
             }
             // y = A v in work items of four own columns x 512 rows (256 row pairs), one warp
             // each: 16-byte loads of row pairs, eight pairs per lane and column in two
@@ -491,6 +507,7 @@ __global__ void __launch_bounds__(TT, 1) k_tri_cluster(const LSec* __restrict__ 
             }
             __syncthreads();
             double t12 = 0.0, t12b = 0.0;
+            #pragma unroll 4
             for (int q = 0; q + 1 < j; q += 2) {
                 t12 = fma(tsum[q], tsum[NB + q], t12);
                 t12b = fma(tsum[q + 1], tsum[NB + q + 1], t12b);
