@@ -1233,7 +1233,10 @@ __global__ void __launch_bounds__(256, 1) k_bt_apply(const LSec* __restrict__ se
     // chunks of 64 rows of V for W, then T, then the chunks again for the update, then the
     // next panel's first chunk.
     constexpr int NTJ = CBK / 8;
-    constexpr int BUF = NBB * 65;
+    // leading dimensions 4 mod 16 doubles (the Z block, the staged chunks and T): the
+    // fragment loads and the row updates of a warp then fall on distinct bank pairs
+    constexpr int VLD = NBB + 4;
+    constexpr int BUF = NBB * VLD;
     extern __shared__ double asm_[];
     int bid = blockIdx.x, s = 0;
     for (; s < nsec; ++s) {
@@ -1245,8 +1248,9 @@ __global__ void __launch_bounds__(256, 1) k_bt_apply(const LSec* __restrict__ se
     const LSec sec = secs[s];
     LView L = lview(sec, eigbuf, wsd, wsi);
     const int n = L.n, c0 = bid * CBK, nc = min(CBK, n - c0);
-    double* Zs = asm_;                      // Zs[j * n + row]
-    double* Vb = Zs + (size_t)n * CBK;      // two buffers: Vs[c * 65 + r] (a chunk) or T (column-major)
+    const int ldz = n + ((4 - n) & 15);
+    double* Zs = asm_;                      // Zs[j * ldz + row]
+    double* Vb = Zs + (size_t)ldz * CBK;    // two buffers: Vs[c * VLD + r] (a chunk) or T (ld VLD)
     double* Ws = Vb + 2 * BUF;              // Ws[c * CBK + j]
     double* W2 = Ws + NBB * CBK;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -1254,7 +1258,7 @@ __global__ void __launch_bounds__(256, 1) k_bt_apply(const LSec* __restrict__ se
     const int wr = 8 * warp;                // this warp's slice of reflectors / rows
     for (int j = 0; j < CBK; ++j)
         for (int row = tid; row < n; row += 256)
-            Zs[(size_t)j * n + row] = j < nc ? L.Z[(size_t)row + (size_t)(c0 + j) * n] : 0.0;
+            Zs[(size_t)j * ldz + row] = j < nc ? L.Z[(size_t)row + (size_t)(c0 + j) * n] : 0.0;
     const int qmax = (n - 2) / NBB;
     // the load sequence: step t of panel q is a V chunk (t < C: for W; t > C: for the
     // update, chunk t - C - 1) or T (t == C), with C = ceil(mr / 64) chunks per pass
@@ -1263,14 +1267,14 @@ __global__ void __launch_bounds__(256, 1) k_bt_apply(const LSec* __restrict__ se
         const int mr = n - 1 - q * NBB, C = chunks(q);
         if (t == C) {
             const double* Tq = L.R + (size_t)q * NBB * NBB;
-            for (int e = tid; e < NBB * NBB; e += 256) cp_async8(dst + e, Tq + e, 8);
+            for (int e = tid; e < NBB * NBB; e += 256) cp_async8(dst + (e % NBB) + (e / NBB) * VLD, Tq + e, 8);
         } else {
             const int i0 = 64 * (t < C ? t : t - C - 1), rows = min(64, mr - i0);
             const double* Rp = L.R + bt_panel_off(n, q);
             for (int e = tid; e < 64 * NBB; e += 256) {
                 const int r = e & 63, c = e >> 6;
                 const int rr = r < rows ? r : rows - 1;   // in bounds; nothing is read when zero-filled
-                cp_async8(dst + c * 65 + r, Rp + (size_t)(i0 + rr) + (size_t)c * mr, r < rows ? 8 : 0);
+                cp_async8(dst + c * VLD + r, Rp + (size_t)(i0 + rr) + (size_t)c * mr, r < rows ? 8 : 0);
             }
         }
         cp_async_commit();
@@ -1299,10 +1303,10 @@ __global__ void __launch_bounds__(256, 1) k_bt_apply(const LSec* __restrict__ se
 #pragma unroll 4
                 for (int k0 = 0; k0 < 64; k0 += 4) {
                     const int kk = k0 + q4;
-                    const double a = Vs[(wr + g) * 65 + kk];
+                    const double a = Vs[(wr + g) * VLD + kk];
 #pragma unroll
                     for (int u = 0; u < NTJ; ++u) {
-                        const double b = kk < rows ? zr[(size_t)(u * 8 + g) * n + kk] : 0.0;
+                        const double b = kk < rows ? zr[(size_t)(u * 8 + g) * ldz + kk] : 0.0;
                         nrg::cta_dmma(acc[u][0], acc[u][1], a, b);
                     }
                 }
@@ -1319,7 +1323,7 @@ __global__ void __launch_bounds__(256, 1) k_bt_apply(const LSec* __restrict__ se
                 for (int u = 0; u < NTJ; ++u) acc[u][0] = acc[u][1] = 0.0;
 #pragma unroll 4
                 for (int k0 = 0; k0 < NBB; k0 += 4) {
-                    const double a = Vs[(wr + g) + (k0 + q4) * NBB];
+                    const double a = Vs[(wr + g) + (k0 + q4) * VLD];
 #pragma unroll
                     for (int u = 0; u < NTJ; ++u) nrg::cta_dmma(acc[u][0], acc[u][1], a, Ws[(k0 + q4) * CBK + u * 8 + g]);
                 }
@@ -1335,7 +1339,7 @@ __global__ void __launch_bounds__(256, 1) k_bt_apply(const LSec* __restrict__ se
                 for (int u = 0; u < NTJ; ++u) acc[u][0] = acc[u][1] = 0.0;
 #pragma unroll 4
                 for (int k0 = 0; k0 < NBB; k0 += 4) {
-                    const double a = Vs[(k0 + q4) * 65 + wr + g];
+                    const double a = Vs[(k0 + q4) * VLD + wr + g];
 #pragma unroll
                     for (int u = 0; u < NTJ; ++u) nrg::cta_dmma(acc[u][0], acc[u][1], a, W2[(k0 + q4) * CBK + u * 8 + g]);
                 }
@@ -1344,8 +1348,8 @@ __global__ void __launch_bounds__(256, 1) k_bt_apply(const LSec* __restrict__ se
                     double* zr = Zs + r0 + i0 + row;
 #pragma unroll
                     for (int u = 0; u < NTJ; ++u) {
-                        zr[(size_t)(u * 8 + 2 * q4) * n] -= acc[u][0];
-                        zr[(size_t)(u * 8 + 2 * q4 + 1) * n] -= acc[u][1];
+                        zr[(size_t)(u * 8 + 2 * q4) * ldz] -= acc[u][0];
+                        zr[(size_t)(u * 8 + 2 * q4 + 1) * ldz] -= acc[u][1];
                     }
                 }
             }
@@ -1355,7 +1359,7 @@ __global__ void __launch_bounds__(256, 1) k_bt_apply(const LSec* __restrict__ se
     }
     for (int j = 0; j < nc; ++j)
         for (int row = tid; row < n; row += 256)
-            L.A[(size_t)row + (size_t)(c0 + j) * n] = Zs[(size_t)j * n + row];
+            L.A[(size_t)row + (size_t)(c0 + j) * n] = Zs[(size_t)j * ldz + row];
 }
 
 __global__ void k_large_out(const LSec* __restrict__ secs, double* eigbuf, double* wsd, int* wsi) {
@@ -1706,8 +1710,8 @@ int syev_large(nrg_context* ctx, const std::vector<SyevSector>& in, double* d_V,
         int dev = 0, optin = 0;
         NRG_CUDA_TRY(cudaGetDevice(&dev));
         NRG_CUDA_TRY(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
-        auto apply_smem = [&](int c) {   // Z block, two staging buffers, W and W2
-            return sizeof(double) * ((size_t)maxn * c + 2 * NBB * 65 + 2 * NBB * c);
+        auto apply_smem = [&](int c) {   // Z block (ld up to maxn + 15), two staging buffers, W and W2
+            return sizeof(double) * ((size_t)(maxn + 15) * c + 2 * NBB * (NBB + 4) + 2 * NBB * c);
         };
         const size_t prep_smem = sizeof(double) * (NBB * 65 + 2 * NBB * NBB);
         const int cbk = apply_smem(16) <= (size_t)optin ? 16 : (apply_smem(8) <= (size_t)optin ? 8 : 0);
