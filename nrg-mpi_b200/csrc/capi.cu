@@ -68,6 +68,7 @@ nrg_context::~nrg_context() {
     for (auto& b : host_store) b.release();
     for (auto& b : scratch.b) b.release();
     for (auto& s : iter_sectors) { s.d_bi.release(); s.d_lst.release(); s.d_lstOff.release(); }
+    for (auto& t : table_pool) { t.bi.release(); t.lst.release(); t.off.release(); }
     d_status.release();
     nrg::Model& M = model;
     for (nrg::DevBuf* b : {&M.d_operation, &M.d_dflag, &M.d_dtype, &M.d_dch, &M.d_dswp, &M.d_bflag,
@@ -153,6 +154,16 @@ struct EntryClock {
         t = n;
     }
 };
+
+// A drop-in call's Sectors takes the device table buffers of pool slot k before its upload
+// and gives them back (grown, if they grew) when the call ends; the swap leaves the other
+// side empty
+void swap_tables(nrg_context* ctx, Sectors& S, size_t k) {
+    nrg_context::TableBufs& t = ctx->table_slot(k);
+    std::swap(S.d_bi, t.bi);
+    std::swap(S.d_lst, t.lst);
+    std::swap(S.d_lstOff, t.off);
+}
 
 template <class T>
 int stage_in(nrg_context* ctx, const T* p, size_t n, size_t slot, const T** out) {
@@ -406,6 +417,8 @@ int nrg_context_release_storage(nrg_context* ctx) {
     for (auto& b : ctx->scratch.b) b.release();
     for (auto& s : ctx->iter_sectors) { s.d_bi.release(); s.d_lst.release(); s.d_lstOff.release(); }
     ctx->iter_sectors.clear();
+    for (auto& t : ctx->table_pool) { t.bi.release(); t.lst.release(); t.off.release(); }
+    ctx->table_pool.clear();
     return NRG_OK;
 }
 
@@ -534,9 +547,10 @@ int nrg_diagonalization(nrg_context* ctx, int32_t iteration, const nrg_diagonali
     auto bi = to_host(ctx, io->basis_input, (size_t)io->numberOfBasis * rs, &st);
     NRG_TRY(st);
     Sectors S;
+    swap_tables(ctx, S, 0);
     int rc = S.build(io->numberOfSubspace, si.data(), io->numberOfBasis, bi.data(), M.nVar, M.nOps);
     if (rc == NRG_OK) rc = S.upload(ctx);
-    if (rc != NRG_OK) { S.d_bi.release(); S.d_lst.release(); S.d_lstOff.release(); return rc; }
+    if (rc != NRG_OK) { swap_tables(ctx, S, 0); return rc; }
     const int nbo = io->numberOfBasis_old;
     if (io->sizeOfEigenvector < S.sizeV || nbo < 1) {
         nrg_set_error_message("eigenvector capacity %lld < %lld", (long long)io->sizeOfEigenvector, S.sizeV);
@@ -598,7 +612,7 @@ int nrg_diagonalization(nrg_context* ctx, int32_t iteration, const nrg_diagonali
     if (rc == NRG_OK && io->groundStateEnergy) *io->groundStateEnergy = out.groundStateEnergy;
     if (cudaStreamSynchronize(ctx->stream) != cudaSuccess && rc == NRG_OK) rc = NRG_ERR_CUDA;
     clk.mark(2);
-    S.d_bi.release(); S.d_lst.release(); S.d_lstOff.release();
+    swap_tables(ctx, S, 0);
     return rc;
 }
 
@@ -622,6 +636,7 @@ static int invmat_common(nrg_context* ctx, int32_t iteration, const nrg_invarian
     auto bo = to_host(ctx, io->basis_output, (size_t)io->numberOfBasis * rs, &st);
     NRG_TRY(st);
     Sectors S;
+    swap_tables(ctx, S, 0);
     int rc = S.build(io->numberOfSubspace, si.data(), io->numberOfBasisFull, bi.data(), M.nVar, M.nOps);
     if (rc == NRG_OK) rc = S.upload(ctx);
     std::vector<int> kept;
@@ -695,7 +710,7 @@ static int invmat_common(nrg_context* ctx, int32_t iteration, const nrg_invarian
     if (cudaStreamSynchronize(ctx->stream) != cudaSuccess && rc == NRG_OK) rc = NRG_ERR_CUDA;
     clk.mark(2);
     if (rc == NRG_OK) rc = check_device_status(ctx);
-    S.d_bi.release(); S.d_lst.release(); S.d_lstOff.release();
+    swap_tables(ctx, S, 0);
     return rc;
 }
 
@@ -721,11 +736,11 @@ struct FullIter {
     std::vector<int> rows;      // fullSubspaceInfo row index per sector
 };
 
-void release(FullIter& f) { f.S.d_bi.release(); f.S.d_lst.release(); f.S.d_lstOff.release(); }
-
-// builds the sectors of one iteration from rows [r0, r1) of fullSubspaceInfo
+// builds the sectors of one iteration from rows [r0, r1) of fullSubspaceInfo, its device
+// tables in pool slot k (given back by swap_tables(ctx, out->S, k))
 int build_full_iter(nrg_context* ctx, const int* fsi, int r0, int r1, const int* fbi, long long nfbi,
-                    FullIter* out) {
+                    FullIter* out, size_t k) {
+    swap_tables(ctx, out->S, k);
     const Model& M = ctx->model;
     const int nVar = M.nVar, rsf = nVar + 6, rs = nVar + 3;
     const int nsub = r1 - r0;
@@ -809,11 +824,16 @@ int nrg_reduced_density_matrix(nrg_context* ctx, const nrg_reduced_density_io* i
     DevBuf& tr = ctx->scratch.b[21];
     NRG_TRY(tr.ensure(sizeof(double) * (size_t)(nIter - start + 1)));
     FullIter child, present;
+    size_t sc = 0;   // the table pool slot of child's tables; present's is 1 - sc
+    bool has_child = false, has_present = false;
     int rc = NRG_OK;
     int r0, r1;
     clk.mark(0);
     rc = full_range(map.data(), nIter, M.first, io->elementNumFullSubspace, nIter, &r0, &r1);
-    if (rc == NRG_OK) rc = build_full_iter(ctx, fsi.data(), r0, r1, fbi.data(), io->numFullBasisInput, &child);
+    if (rc == NRG_OK) {
+        rc = build_full_iter(ctx, fsi.data(), r0, r1, fbi.data(), io->numFullBasisInput, &child, sc);
+        has_child = true;
+    }
     for (int i = 1; rc == NRG_OK && i <= nIter - start; ++i) {
         const int N = nIter - i;
         rc = full_range(map.data(), nIter, M.first, io->elementNumFullSubspace, N, &r0, &r1);
@@ -824,18 +844,23 @@ int nrg_reduced_density_matrix(nrg_context* ctx, const nrg_reduced_density_io* i
             point += fsi[(size_t)j * rsf + nVar + 1] * fsi[(size_t)j * rsf + nVar + 1];
         }
         if (point - 1 > io->sizeOfReducedDensity) { rc = NRG_ERR_INVALID; nrg_set_error_message("reducedDensityMatrix too small"); break; }
-        rc = build_full_iter(ctx, fsi.data(), r0, r1, fbi.data(), io->numFullBasisInput, &present);
+        rc = build_full_iter(ctx, fsi.data(), r0, r1, fbi.data(), io->numFullBasisInput, &present, 1 - sc);
+        has_present = true;
         if (rc != NRG_OK) break;
         IterView P, C;
         P.S = &present.S; P.kept = present.kept; P.d_V = dV; P.d_rdm = dR; P.rdm_off = present.rdm_off;
         C.S = &child.S; C.kept = child.kept; C.d_V = dV; C.d_rdm = dR; C.rdm_off = child.rdm_off;
         rc = rdm_step_device(ctx, P, C, dR, tr.as<double>() + (i - 1));
-        release(child);
+        // child's tables back to the pool (the launches that read them precede, on the
+        // stream, the uploads of the next borrower); present becomes the child
+        swap_tables(ctx, child.S, sc);
         child = present;
         present = FullIter();
+        has_present = false;
+        sc = 1 - sc;
     }
-    release(child);
-    release(present);
+    if (has_child) swap_tables(ctx, child.S, sc);
+    if (has_present) swap_tables(ctx, present.S, 1 - sc);
     clk.mark(1);
     if (rc == NRG_OK) rc = finish_out(ctx, io->reducedDensityMatrix, dR, (size_t)io->sizeOfReducedDensity);
     if (rc == NRG_OK && io->trace) {
@@ -882,9 +907,10 @@ static int spike_common(nrg_context* ctx, int32_t iteration, const nrg_spike_io*
     auto bo = to_host(ctx, io->basis_output, (size_t)nbf * rs, &st); NRG_TRY(st);
     auto E = to_host(ctx, io->eigenvalue, (size_t)nbf, &st); NRG_TRY(st);
     Sectors S;
+    swap_tables(ctx, S, 0);
     int rc = S.build(io->numberOfSubspace, si.data(), nbf, bi.data(), nVar, M.nOps);
     if (rc == NRG_OK) rc = S.upload(ctx);
-    if (rc != NRG_OK) { S.d_bi.release(); S.d_lst.release(); S.d_lstOff.release(); return rc; }
+    if (rc != NRG_OK) { swap_tables(ctx, S, 0); return rc; }
     // eigenvalues back in sector order (the caller's array is in the truncation order)
     std::vector<double> Esec(nbf, 0.0);
     for (int i = 0; i < nbf; ++i) {
@@ -1016,7 +1042,7 @@ static int spike_common(nrg_context* ctx, int32_t iteration, const nrg_spike_io*
             }
         }
     }
-    S.d_bi.release(); S.d_lst.release(); S.d_lstOff.release();
+    swap_tables(ctx, S, 0);
     clk.mark(2);
     return rc;
 }

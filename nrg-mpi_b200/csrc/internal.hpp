@@ -180,6 +180,15 @@ struct nrg_context {
         if (store.size() <= i) store.resize(i + 1);
         return store[i];
     }
+    // device copies of the drop-in entries' sector tables (basis, index lists), kept
+    // between calls: an entry borrows a set and gives it back, so once the buffers have
+    // grown its calls allocate and free nothing (a free would also wait for the device)
+    struct TableBufs { nrg::DevBuf bi, lst, off; };
+    std::deque<TableBufs> table_pool;
+    TableBufs& table_slot(size_t i) {
+        if (table_pool.size() <= i) table_pool.resize(i + 1);
+        return table_pool[i];
+    }
     // host module arrays of the host-array driver, reused across runs: page-locked, or
     // pageable like a Fortran allocatable when host_pageable is set
     std::deque<nrg::HostBuf> host_store;
