@@ -12,6 +12,10 @@ second (60 per step), whole job.
   stream the library launches on, barrier + synchronize on both sides, max over ranks.
 * forward_only: the same sweep without the density matrices and the spectrum (the scope
   of the reference arm's steps).
+* bookkeeping: one forward sweep with the per-state bookkeeping between iterations
+  (truncation, the next basis records and row lists, the kept energies) on the device,
+  the default, and one with it on the host (NRG_HOST_TABLES=1): iterations/s, kernel
+  launches and host<->device bytes per iteration.
 * e2e: the same metric through the drop-in entry points with host arrays (every routine
   copies its module arrays host->device and back, as a Fortran caller would), with the
   caller's arrays page-locked; e2e.pageable: the same with pageable arrays (a Fortran
@@ -461,6 +465,34 @@ def main():
     forward_only = {"value": n_it * 1e3 / sf.elapsed_time(ef), "unit": "iterations/s",
                     "timing": "one sweep without density matrices and spectrum, CUDA events"}
 
+    def forward_sweep(host_tables):
+        # one event-timed forward sweep with the per-state bookkeeping on the device (the
+        # default) or on the host (NRG_HOST_TABLES=1), no energy-flow output
+        if host_tables:
+            os.environ["NRG_HOST_TABLES"] = "1"
+        try:
+            ctx.run(spectrum=False, flow_stride=0)
+            torch.cuda.synchronize(dev)
+            ctx.reset_stats()
+            l0 = ctx.launch_count
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            ctx.run(spectrum=False, flow_stride=0)
+            b.record(stream)
+            torch.cuda.synchronize(dev)
+            st = ctx.stats()
+            return {"iterations_per_s": n_it * 1e3 / a.elapsed_time(b),
+                    "launches_per_iteration": (ctx.launch_count - l0) / n_it,
+                    "h2d_bytes_per_iteration": int(st["h2d_bytes"]) // n_it,
+                    "d2h_bytes_per_iteration": int(st["d2h_bytes"]) // n_it}
+        finally:
+            os.environ.pop("NRG_HOST_TABLES", None)
+
+    bookkeeping = {"what": "forward sweep of the headline workload with the per-state bookkeeping "
+                           "(truncation, basis records, row lists, kept energies) on the device and on "
+                           "the host; CUDA events, one sweep each",
+                   "device": forward_sweep(False), "host": forward_sweep(True)}
+
     def drop_in(pageable, steps):
         # one untimed run allocates the emulated caller's module arrays, then K timed runs
         r = ctx.run(spectrum=True, host_drop_in=True, host_pageable=pageable)
@@ -548,6 +580,7 @@ def main():
             "phase_seconds": {"nrg_sweep": float(ph[0]), "rdm": float(ph[1]), "cfs_spectrum": float(ph[2])},
             "spectrum_seconds": float(ph[2]),
             "forward_only": forward_only,
+            "bookkeeping": bookkeeping,
             "device_memory_gb": device_gb,
             "sum_rule": sums,
             "gpu_launches": int(launches),

@@ -145,7 +145,8 @@ NRG_API int nrg_version(void);
  * by quantum numbers, then reference, with that exchange sort's order among equal keys),
  * then the sector table subspaceInfo = (basis, dimension, count_eigenvector, start_input)
  * (:63-114).  Integer bookkeeping on the host, as in the reference; it needs no context
- * and no device (the device-resident sweep calls the same code).  operation is the
+ * and no device (the device-resident sweep calls the same code where it builds the
+ * records on the host).  operation is the
  * Fortran (nOps, nVar+nChain) table; basis_input receives nb_old*nOps records;
  * numberOfSubspace receives the sector count, also when subspaceCapacity is too small
  * (NRG_ERR_INVALID). */
@@ -305,7 +306,16 @@ NRG_API int nrg_host_free(void* p);
 
 /* ---- whole run: main.F90:142-252 with everything device resident ---------------------
  * Replays the reference's driver (forward NRG sweep, backward reduced density matrices,
- * CFS spectrum at T = 0) on one device.  Initial state as read from initial.dat. */
+ * CFS spectrum at T = 0) on one device.  Initial state as read from initial.dat.  In the
+ * device-resident run (host_drop_in = 0) the per-state bookkeeping between iterations
+ * also runs on the device: the truncation of postprocess (postprocess.F90:69-140) and,
+ * after the first iteration, the basis records and row lists of prepareBasis
+ * (prepareBasis.F90:31-114); the host keeps a few integers per sector.  Models whose
+ * operations change the quantum numbers alike (ties in sortBasisArray's exchange sort)
+ * build the records on the host, where that exchange sequence is replayed.  Setting the
+ * environment variable NRG_HOST_TABLES=1 keeps all the bookkeeping on the host;
+ * NRG_CHECK_TABLES=1 compares the device's tables with the host's at every iteration and
+ * fails the run (NRG_ERR_STATE) on any difference. */
 typedef struct nrg_run_input {
     int32_t numberOfBasis;                /* impurity basis size                        */
     const int32_t* basis_output;          /* [nb*(nVar+3)]                              */

@@ -7,7 +7,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 SRC = os.path.join(HERE, "csrc")
 OUT = os.path.join(HERE, "nrg_b200", "libnrgb200.so")
 SOURCES = ["capi.cu", "driver.cu", "routines.cu", "kernels.cu", "ggemm.cu", "eig.cu", "eig_large.cu",
-           "noalloc.cu", "restart.cu"]
+           "noalloc.cu", "restart.cu", "tables.cu"]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo", "-O3", "-std=c++17",
          "--extended-lambda", "-Xcompiler", "-fPIC", "-Xcompiler", "-fvisibility=hidden", "-Xcompiler", "-g"]

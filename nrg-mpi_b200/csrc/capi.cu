@@ -89,6 +89,7 @@ nrg_context::~nrg_context() {
         if (e) cudaEventDestroy(e);
     h_small.release();
     h_evals.release();
+    h_kept.release();
     if (aux_hi) cudaStreamDestroy(aux_hi);
     for (auto* pl : {&pending_tri, &pending_syev})
         for (auto& t : *pl) {

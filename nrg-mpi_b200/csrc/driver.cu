@@ -4,9 +4,12 @@
 //
 // Two data flows:
 // * device resident (nrg_run_input.host_drop_in = 0): eigenvector blocks, invariant
-//   matrices, density matrices and bins stay in device memory; the host keeps the
-//   integer bookkeeping (basis records, sector tables, the truncation decision), which
-//   needs the eigenvalues of each iteration (one small device-to-host copy per step);
+//   matrices, density matrices and bins stay in device memory, and so does the per-state
+//   bookkeeping (the truncation, the next iteration's basis records and row lists, the
+//   kept energies: tables.cu); the host keeps the sector-level tables it sizes the
+//   launches with (a few integers per sector and operation cross per iteration).  Models
+//   whose operations change the quantum numbers alike (ties in sortBasisArray) build the
+//   records on the host, with the exchange sort replayed;
 // * host drop-in (host_drop_in = 1): every routine goes through its public entry point
 //   with host arrays, exactly as the Fortran caller would call the drop-in: module arrays
 //   live in host memory and cross to the device and back at every call.
@@ -16,6 +19,7 @@
 #include <algorithm>
 #include <atomic>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 #include <mutex>
 #include <numeric>
@@ -381,6 +385,64 @@ void kept_in_sectors(const std::vector<int>& si, int nsub, const std::vector<int
         }
 }
 
+// basis_output of the kept states after the first iteration: (qn of the sector, column)
+// for columns 1..kept of every sector, in sector order (postprocess.F90:140-160 on the
+// record diagonalization.F90:394-407 writes)
+std::vector<int> kept_records(const Sectors& S, const std::vector<int>& kept) {
+    const int rs = S.nVar + 3;
+    std::vector<int> bo;
+    for (int s = 0; s < S.nsub; ++s)
+        for (int t = 0; t < kept[s]; ++t) {
+            const size_t o = bo.size();
+            bo.resize(o + rs, 0);
+            for (int v = 0; v < S.nVar; ++v) bo[o + v] = S.qn[(size_t)s * S.nVar + v];
+            bo[o + S.nVar] = t + 1;
+        }
+    return bo;
+}
+
+bool env_flag(const char* name) {
+    const char* v = std::getenv(name);
+    return v && std::atoi(v) != 0;
+}
+
+// NRG_CHECK_TABLES=1 (a test aid): the tables the device built for one iteration against
+// the host's prepareBasis on the same kept states, every sector-level field and every
+// downloaded record and row list compared exactly
+int check_device_rows(nrg_context* ctx, const Model& M, int it, const Sectors& prev, const std::vector<int>& kept_prev,
+                      const Sectors& S) {
+    const int rs = M.nVar + 3;
+    const std::vector<int> bo = kept_records(prev, kept_prev);
+    const int nb_old = (int)(bo.size() / rs);
+    std::vector<int> rec, si;
+    prepare_basis_host(M, bo, nb_old, &rec, &si);
+    Sectors H;
+    NRG_TRY(H.build((int)(si.size() / rs), si.data(), nb_old * M.nOps, rec.data(), M.nVar, M.nOps));
+    const char* what = nullptr;
+    if (H.nsub != S.nsub || H.nb != S.nb) what = "sector or state count";
+    else if (H.qn != S.qn || H.dim != S.dim || H.start != S.start || H.ce != S.ce || H.sizeV != S.sizeV)
+        what = "sector table";
+    else if (H.lstOff != S.lstOff || H.refBase != S.refBase) what = "row-list offsets";
+    if (!what) {
+        std::vector<int> bi((size_t)S.nb * rs), lst(H.lst.size());
+        NRG_CUDA_TRY(cudaMemcpyAsync(bi.data(), S.d_bi.p, sizeof(int) * bi.size(), cudaMemcpyDeviceToHost, ctx->stream));
+        if (!lst.empty())
+            NRG_CUDA_TRY(cudaMemcpyAsync(lst.data(), S.d_lst.p, sizeof(int) * lst.size(), cudaMemcpyDeviceToHost,
+                                         ctx->stream));
+        NRG_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+        if (lst != H.lst) what = "row lists";
+        for (int i = 0; i < S.nb && !what; ++i)
+            if (bi[(size_t)i * rs + M.nVar] != H.rowRef[i] + 1 || bi[(size_t)i * rs + M.nVar + 1] != H.rowVar[i] ||
+                bi[(size_t)i * rs + M.nVar + 2] != H.rowOp[i] + 1)
+                what = "basis_input records";
+    }
+    if (what) {
+        nrg_set_error_message("iteration %d: the device-built %s differ from the host's prepareBasis", it, what);
+        return NRG_ERR_STATE;
+    }
+    return NRG_OK;
+}
+
 struct IterRec {
     int nb_full = 0, nb_kept = 0;
     double emin = 0.0;   // the minimum the shift subtracted (full-density-matrix energies)
@@ -471,55 +533,118 @@ int run_device(nrg_context* ctx, const nrg_run_input* in, nrg_run_output* out, c
         NRG_TRY(ctx->h_evals.ensure(sizeof(double) * (size_t)std::min(keep * M.nOps, 1LL << 22)));
     }
     // ---- forward sweep ----
+    // per-state bookkeeping on the device unless the operations change the quantum numbers
+    // alike (NRG_HOST_TABLES=1 keeps all of it on the host; NRG_CHECK_TABLES=1 compares the
+    // device's tables with the host's at every iteration)
+    const bool dev_tables = ctx->device_tables && !env_flag("NRG_HOST_TABLES") && ops_change_qn_distinctly(M);
+    const bool check_tables = dev_tables && env_flag("NRG_CHECK_TABLES");
+    const bool flow_out = out && out->flow && out->flowStride > 0;
+    const bool fdm_req = spectrum && in->temperature > 0.0;
+    TruncTables TT;
     for (int it = first; it <= nIter; ++it) {
         const int idx = it - first;
         IterRec& R = recs[idx];
-        std::vector<int> rec, si;
-        prepare_basis_host(M, bo, nb_old, &rec, &si);
-        const int nb = nb_old * M.nOps;
-        const int nsub = (int)(si.size() / rs);
         Sectors& S = ctx->iter_sectors[idx];
-        NRG_TRY(S.build(nsub, si.data(), nb, rec.data(), nVar, M.nOps));
-        NRG_TRY(S.upload(ctx));
-        ctx->h2d += (long long)sizeof(int) * ((long long)nb * rs + (long long)S.lst.size() + (long long)S.lstOff.size());
+        if (dev_tables && idx > 0) {   // from the previous iteration's sectors and kept counts
+            std::vector<RowRun> runs;
+            NRG_TRY(S.plan(M, ctx->iter_sectors[idx - 1], recs[idx - 1].kept, &runs));
+            NRG_TRY(rows_device(ctx, S, runs));
+            if (check_tables) NRG_TRY(check_device_rows(ctx, M, it, ctx->iter_sectors[idx - 1], recs[idx - 1].kept, S));
+        } else {
+            std::vector<int> rec, si;
+            prepare_basis_host(M, bo, nb_old, &rec, &si);
+            NRG_TRY(S.build((int)(si.size() / rs), si.data(), nb_old * M.nOps, rec.data(), nVar, M.nOps));
+            NRG_TRY(S.upload(ctx));   // counted in ctx->h2d by the upload
+        }
+        const int nb = S.nb;
+        const int nsub = S.nsub;
+        const bool truncate = it != M.first && it != M.nIter && nb > M.truncation;   // postprocess.F90:79-81
+        if (dev_tables) {
+            TT.P = TruncParams();
+            TT.P.nb = nb;
+            TT.P.nsub = nsub;
+            TT.P.truncate = truncate ? 1 : 0;
+            TT.P.ntrunc = M.truncation;
+            TT.P.limit = (int)(M.truncation * 1.2);
+            NRG_TRY(TT.prepare(ctx, S));
+        }
+        // the host needs the energies themselves for the last iteration (ground states,
+        // density-matrix seed), the full-density-matrix weights and the energy flow
+        const bool need_E = !dev_tables || it == nIter || fdm_req || flow_out || check_tables;
         DevBuf& bV = slotV(idx);
         DevBuf& bE = slotE(idx);
         NRG_TRY(bV.ensure(sizeof(double) * (size_t)S.sizeV));
         NRG_TRY(bE.ensure(sizeof(double) * (size_t)nb));
-        // the call returns with the shifted eigenvalues on the host while the eigenvectors
-        // are still being formed: the truncation and the next iteration's tables are built
-        // meanwhile, and every later launch on the stream is ordered after them
+        // the call returns with the shifted eigenvalues (or the device truncation's kept
+        // counts) on the host while the eigenvectors are still being formed: the next
+        // iteration's tables are built meanwhile, and every later launch on the stream is
+        // ordered after them
         DiagOut dout;
-        if (ctx->early_evals) {
+        DiagPost post;
+        post.early = ctx->early_evals;
+        post.trunc = dev_tables ? &TT : nullptr;
+        if (ctx->early_evals && need_E) {
             NRG_TRY(ctx->h_evals.ensure(sizeof(double) * (size_t)nb));
-            NRG_TRY(diag_device(ctx, it, S, dEold, nb_old, dIMold, bV.as<double>(), bE.as<double>(), &dout,
-                                ctx->h_evals.as<double>()));
-            R.Esec.assign(ctx->h_evals.as<double>(), ctx->h_evals.as<double>() + nb);
-        } else {
-            NRG_TRY(diag_device(ctx, it, S, dEold, nb_old, dIMold, bV.as<double>(), bE.as<double>(), &dout));
-            R.Esec.resize(nb);
-            NRG_CUDA_TRY(cudaMemcpyAsync(R.Esec.data(), bE.p, sizeof(double) * nb, cudaMemcpyDeviceToHost, st));
-            NRG_CUDA_TRY(cudaStreamSynchronize(st));
-            ctx->d2h += (long long)sizeof(double) * nb;
+            post.h_E = ctx->h_evals.as<double>();
+        }
+        NRG_TRY(diag_device(ctx, it, S, dEold, nb_old, dIMold, bV.as<double>(), bE.as<double>(), &dout, &post));
+        if (need_E) {
+            if (ctx->early_evals) {
+                R.Esec.assign(ctx->h_evals.as<double>(), ctx->h_evals.as<double>() + nb);
+            } else {
+                R.Esec.resize(nb);
+                NRG_CUDA_TRY(cudaMemcpyAsync(R.Esec.data(), bE.p, sizeof(double) * nb, cudaMemcpyDeviceToHost, st));
+                NRG_CUDA_TRY(cudaStreamSynchronize(st));
+                ctx->d2h += (long long)sizeof(double) * nb;
+            }
         }
         if (out && out->thermo) NRG_TRY(run_thermo(ctx, S, bE.as<double>(), dThermo + 3 * (size_t)idx));
         if (out && out->groundStateEnergy) out->groundStateEnergy[idx] = dout.groundStateEnergy;
         R.emin = dout.emin;
-        std::vector<int> order;
-        const int nbk = truncate_host(M, it, R.Esec, &order, &startTrancation, &flag_truncation);
-        record_flow(out, idx, R.Esec, order, nbk);
-        std::vector<int> rowSec(nb);
-        for (int s = 0; s < nsub; ++s)
-            for (int j = 0; j < S.dim[s]; ++j) rowSec[S.start[s] + j] = s;
-        std::vector<int> bo_new((size_t)nb * rs, 0);
-        std::vector<double> Eold_next(nbk);
-        R.kept.assign(nsub, 0);
-        for (int q = 0; q < nb; ++q) {
-            const int row = order[q], s = rowSec[row];
-            int* r = &bo_new[(size_t)q * rs];
-            for (int v = 0; v < nVar; ++v) r[v] = S.qn[(size_t)s * nVar + v];
-            r[nVar] = row - S.start[s] + 1;
-            if (q < nbk) { Eold_next[q] = R.Esec[row]; R.kept[s]++; }
+        int nbk = 0;
+        std::vector<int> bo_new;
+        std::vector<double> Eold_next;
+        if (dev_tables) {
+            NRG_TRY(TT.result(&R.kept, &nbk));
+            if (truncate && startTrancation > it) {   // postprocess.F90:83-86
+                startTrancation = it;
+                flag_truncation = true;
+            }
+            std::vector<int> order;   // the kept rows in index order (flow, check)
+            if (flow_out || check_tables) {
+                for (int s = 0; s < nsub; ++s)
+                    for (int t = 0; t < R.kept[s]; ++t) order.push_back(S.start[s] + t);
+            }
+            if (check_tables) {
+                std::vector<int> ho;
+                int st2 = nIter + 1;
+                bool fl2 = false;
+                const int nbk_h = truncate_host(M, it, R.Esec, &ho, &st2, &fl2);
+                ho.resize(nbk_h);
+                if (nbk_h != nbk || ho != order) {
+                    nrg_set_error_message("iteration %d: the device truncation kept %d states, the host's %d", it, nbk,
+                                          nbk_h);
+                    return NRG_ERR_STATE;
+                }
+            }
+            record_flow(out, idx, R.Esec, order, nbk);
+        } else {
+            std::vector<int> order;
+            nbk = truncate_host(M, it, R.Esec, &order, &startTrancation, &flag_truncation);
+            record_flow(out, idx, R.Esec, order, nbk);
+            std::vector<int> rowSec(nb);
+            for (int s = 0; s < nsub; ++s)
+                for (int j = 0; j < S.dim[s]; ++j) rowSec[S.start[s] + j] = s;
+            bo_new.assign((size_t)nb * rs, 0);
+            Eold_next.resize(nbk);
+            R.kept.assign(nsub, 0);
+            for (int q = 0; q < nb; ++q) {
+                const int row = order[q], s = rowSec[row];
+                int* r = &bo_new[(size_t)q * rs];
+                for (int v = 0; v < nVar; ++v) r[v] = S.qn[(size_t)s * nVar + v];
+                r[nVar] = row - S.start[s] + 1;
+                if (q < nbk) { Eold_next[q] = R.Esec[row]; R.kept[s]++; }
+            }
         }
         R.nb_full = nb;
         R.nb_kept = nbk;
@@ -540,13 +665,16 @@ int run_device(nrg_context* ctx, const nrg_run_input* in, nrg_run_output* out, c
             }
         }
         DevBuf& bEo = ctx->slot(3 + ((idx + 1) & 1));
-        NRG_TRY(bEo.ensure(sizeof(double) * nbk));
-        NRG_TRY(h2d_async(ctx, bEo.p, Eold_next.data(), sizeof(double) * nbk));
-        ctx->h2d += (long long)sizeof(double) * nbk;
+        NRG_TRY(bEo.ensure(sizeof(double) * std::max(nbk, 1)));
+        if (dev_tables) {
+            NRG_TRY(TT.gather(ctx, bE.as<double>(), bEo.as<double>()));
+        } else {
+            NRG_TRY(h2d_async(ctx, bEo.p, Eold_next.data(), sizeof(double) * nbk));
+            bo.swap(bo_new);
+        }
         dEold = bEo.as<double>();
         dIMold = dIMnew;
         imsOld = imsNew;
-        bo.swap(bo_new);
         nb_old = nbk;
     }
     NRG_CUDA_TRY(cudaEventRecord(ev[1], st));

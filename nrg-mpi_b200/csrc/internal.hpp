@@ -70,6 +70,18 @@ struct Model {
 // ------------------------------------------------------------------------------------
 // per-iteration sector tables built from subspaceInfo + basis_input
 // ------------------------------------------------------------------------------------
+// one run of rows of the next iteration's basis: the kept states of one old sector
+// combined with one operation (tables.cu)
+struct RowRun {
+    int row0;       // first row (0-based) of basis_input
+    int len;        // rows: the old sector's kept states
+    int ref0;       // 0-based reference of the first row (kept states before the old sector)
+    int op;         // 0-based operation
+    int sec;        // new sector
+    int sec_start;  // its first row
+    int lst0;       // offset of the (sector, operation) row list
+};
+
 struct Sectors {
     int nsub = 0, nb = 0, nVar = 0, nOps = 0;
     std::vector<int> qn;        // nsub*nVar
@@ -84,6 +96,12 @@ struct Sectors {
     DevBuf d_bi, d_lst, d_lstOff;
     int build(int nsub, const int* si, int nb, const int* bi, int nVar, int nOps);
     int upload(nrg_context* ctx);
+    // The table prepareBasis builds for the next iteration, from this iteration's sectors
+    // and kept counts alone (tables.cu; models whose operations change the quantum numbers
+    // in pairwise different ways).  Fills the sector-level fields; the per-row records and
+    // row lists are written on the device by rows_device from the returned runs.
+    int plan(const Model& M, const Sectors& prev, const std::vector<int>& kept_prev, std::vector<RowRun>* runs);
+    void index_qn();                    // rebuilds qnHash from qn
     int find(const int* q) const;       // findSubspace: first sector with these qn, or -1
     std::vector<int> qnHash;            // open-addressing index of the sectors by qn (find)
     static unsigned long long hash_qn(const int* q, int nVar);
@@ -176,6 +194,8 @@ struct nrg_context {
     bool early_evals = true;
     nrg::HostBuf h_small;   // pinned: the shift's minimum and E(1), the status word
     nrg::HostBuf h_evals;   // pinned: the shifted eigenvalues of the current iteration
+    nrg::HostBuf h_kept;    // pinned: the device truncation's kept counts
+    bool device_tables = true;   // per-state bookkeeping of nrg_run on the device (tables.cu)
     nrg::DevBuf& slot(size_t i) {
         if (store.size() <= i) store.resize(i + 1);
         return store[i];
@@ -318,8 +338,45 @@ struct DiagOut {
 // With h_E (pinned host, nb doubles) the call returns as soon as the shifted eigenvalues
 // are in h_E: the eigenvectors are still being formed on the device, ordered before
 // any later work on ctx->stream.
+// Work diag_device does for the device-resident run right after the eigenvalue shift, on
+// the caller's stream.  early: return once the shifted eigenvalues' minimum, the status
+// word, h_E and the truncation's counts have reached the host, before the eigenvectors are
+// complete (later launches on the stream still follow them); h_E (early only): pinned copy
+// of the shifted eigenvalues, or null.  Without early the call returns with the stream
+// drained.
+struct DiagPost {
+    bool early = false;
+    double* h_E = nullptr;
+    struct TruncTables* trunc = nullptr;   // device truncation launched after the shift
+};
 int diag_device(nrg_context* ctx, int iteration, Sectors& S, const double* d_Eold, int nb_old,
-                const double* d_IMold, double* d_V, double* d_E, DiagOut* out, double* h_E = nullptr);
+                const double* d_IMold, double* d_V, double* d_E, DiagOut* out, const DiagPost* post = nullptr);
+
+// ---- device bookkeeping of the device-resident run (tables.cu) ----
+struct TruncParams {
+    int nb = 0, nsub = 0;
+    int truncate = 0;              // the rule of postprocess.F90:79-126 applies
+    int ntrunc = 0;                // param%truncation (N_keep)
+    int limit = 0;                 // int(N_keep * truncationLimitScale)
+    double thr = 0.000001;         // truncationThreshold (module.F90:629)
+    double step = 0.001;           // the cut-back step (postprocess.F90:109)
+    long long max_steps = 1LL << 24;   // bound of the cut-back loop (the reference has none)
+};
+struct TruncTables {
+    TruncParams P;
+    int nsub = 0;
+    int* d_secTab = nullptr;       // start, dimension per sector
+    int* d_out = nullptr;          // kept total, status, kept per sector
+    int* d_koff = nullptr;         // kept states before each sector
+    double* d_ecut = nullptr;
+    int* h_out = nullptr;          // pinned copy of d_out
+    int prepare(nrg_context* ctx, const Sectors& S);
+    int launch(nrg_context* ctx, const double* d_E);    // kernel + copy of the counts to h_out
+    int result(std::vector<int>* kept, int* nb_kept) const;   // after h_out has arrived
+    int gather(nrg_context* ctx, const double* d_E, double* d_Enext) const;
+};
+int rows_device(nrg_context* ctx, Sectors& S, const std::vector<RowRun>& runs);
+bool ops_change_qn_distinctly(const Model& M);
 // reads the profiling timers of completed eigensolver windows into the counters
 int flush_profile_timers(nrg_context* ctx);
 

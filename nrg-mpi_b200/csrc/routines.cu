@@ -121,23 +121,7 @@ int Sectors::build(int nsub_, const int* si, int nb_, const int* bi, int nVar_, 
         acc += (long long)dim[s] * dim[s];
     }
     sizeV = acc;
-    // index by quantum numbers: the first sector of each qn (findSubspace semantics)
-    {
-        size_t cap = 16;
-        while (cap < 4 * (size_t)nsub) cap <<= 1;
-        qnHash.assign(cap, -1);
-        for (int s = 0; s < nsub; ++s) {
-            const int* q = &qn[(size_t)s * nVar];
-            for (size_t x = hash_qn(q, nVar) & (cap - 1);; x = (x + 1) & (cap - 1)) {
-                const int o = qnHash[x];
-                if (o < 0) { qnHash[x] = s; break; }
-                bool eq = true;
-                for (int v = 0; v < nVar; ++v)
-                    if (qn[(size_t)o * nVar + v] != q[v]) { eq = false; break; }
-                if (eq) break;   // an earlier sector has these qn: it stays the one found
-            }
-        }
-    }
+    index_qn();
     rowOp.resize(nb); rowRef.resize(nb); rowVar.resize(nb);
     for (int i = 0; i < nb; ++i) {
         rowRef[i] = bi[(size_t)i * rs + nVar] - 1;
@@ -254,6 +238,24 @@ int h2d_async(nrg_context* ctx, void* dst, const void* src, size_t bytes) {
     return NRG_OK;
 }
 
+// index by quantum numbers: the first sector of each qn (findSubspace semantics)
+void Sectors::index_qn() {
+    size_t cap = 16;
+    while (cap < 4 * (size_t)nsub) cap <<= 1;
+    qnHash.assign(cap, -1);
+    for (int s = 0; s < nsub; ++s) {
+        const int* q = &qn[(size_t)s * nVar];
+        for (size_t x = hash_qn(q, nVar) & (cap - 1);; x = (x + 1) & (cap - 1)) {
+            const int o = qnHash[x];
+            if (o < 0) { qnHash[x] = s; break; }
+            bool eq = true;
+            for (int v = 0; v < nVar; ++v)
+                if (qn[(size_t)o * nVar + v] != q[v]) { eq = false; break; }
+            if (eq) break;   // an earlier sector has these qn: it stays the one found
+        }
+    }
+}
+
 unsigned long long Sectors::hash_qn(const int* q, int nVar) {
     unsigned long long h = 1469598103934665603ULL;   // FNV-1a over the quantum numbers
     for (int v = 0; v < nVar; ++v) {
@@ -301,8 +303,10 @@ int check_device_status(nrg_context* ctx) {
 // diagonalization (diagonalization.F90:1-410)
 // ------------------------------------------------------------------------------------
 int diag_device(nrg_context* ctx, int iteration, Sectors& S, const double* d_Eold, int nb_old,
-                const double* d_IMold, double* d_V, double* d_E, DiagOut* out, double* h_E) {
-    const bool early = h_E != nullptr;
+                const double* d_IMold, double* d_V, double* d_E, DiagOut* out, const DiagPost* post) {
+    const bool early = post && post->early;
+    double* h_E = post ? post->h_E : nullptr;
+    TruncTables* trunc = post ? post->trunc : nullptr;
     const int nsec = S.nsub;
     std::vector<int> order(nsec);
     std::iota(order.begin(), order.end(), 0);
@@ -423,10 +427,14 @@ int diag_device(nrg_context* ctx, int iteration, Sectors& S, const double* d_Eol
         if (has_g2) NRG_CUDA_TRY(cudaStreamWaitEvent(ctx->stream, ctx->ev_evals2, 0));
         if (fork_small) NRG_CUDA_TRY(cudaStreamWaitEvent(ctx->stream, ctx->ev_join, 0));
         NRG_TRY(run_eig_shift(ctx, d_E, S.nb, bmin.as<double>()));
-        NRG_CUDA_TRY(cudaMemcpyAsync(h_E, d_E, sizeof(double) * S.nb, cudaMemcpyDeviceToHost, ctx->stream));
+        if (trunc) NRG_TRY(trunc->launch(ctx, d_E));
+        if (h_E) {
+            NRG_CUDA_TRY(cudaMemcpyAsync(h_E, d_E, sizeof(double) * S.nb, cudaMemcpyDeviceToHost, ctx->stream));
+            ctx->d2h += (long long)sizeof(double) * S.nb;
+        }
         NRG_CUDA_TRY(cudaMemcpyAsync(hs, bmin.p, sizeof(double) * 2, cudaMemcpyDeviceToHost, ctx->stream));
         NRG_CUDA_TRY(cudaMemcpyAsync(hs + 2, ctx->d_status.p, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
-        ctx->d2h += (long long)sizeof(double) * (S.nb + 2) + (long long)sizeof(int);
+        ctx->d2h += (long long)sizeof(double) * 2 + (long long)sizeof(int);
         NRG_CUDA_TRY(cudaEventRecord(ctx->ev_evals_host, ctx->stream));
     }
     if (fork_large) NRG_CUDA_TRY(cudaStreamWaitEvent(ctx->stream, ctx->ev_join_hi, 0));
@@ -452,6 +460,7 @@ int diag_device(nrg_context* ctx, int iteration, Sectors& S, const double* d_Eol
         return NRG_OK;
     }
     NRG_TRY(run_eig_shift(ctx, d_E, S.nb, bmin.as<double>()));
+    if (trunc) NRG_TRY(trunc->launch(ctx, d_E));
     NRG_TRY(run_eig_chop(ctx, S.sizeV, d_V));
     double mg[2];
     NRG_CUDA_TRY(cudaMemcpyAsync(mg, bmin.p, sizeof(double) * 2, cudaMemcpyDeviceToHost, ctx->stream));
