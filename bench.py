@@ -10,8 +10,7 @@ second (60 per step), whole job.
 
 * value: device-resident run (nrg_run), inputs resident, timed with CUDA events on the
   stream the library launches on, barrier + synchronize on both sides, max over ranks.
-* forward_only: the same sweep without the density matrices and the spectrum (the scope
-  of the reference arm's steps).
+* forward_only: the same sweep without the density matrices and the spectrum.
 * bookkeeping: one forward sweep with the per-state bookkeeping between iterations
   (truncation, the next basis records and row lists, the kept energies) on the device,
   the default, and one with it on the host (NRG_HOST_TABLES=1): iterations/s, kernel
@@ -28,10 +27,13 @@ second (60 per step), whole job.
   it).  "eigensolver" gives the same for the whole eigensolver of an iteration
   (sum_s (4/3+2) d_s^3 over the event-timed window).
 * cpu_baseline: the oracle (numpy/scipy port of the reference path, OpenBLAS on all host
-  threads) on full-size forward iterations of the same sweep (a bounded sample).
-* --impl reference: the oracle port timed per full-size forward NRG iteration of the same
-  sweep (prepareBasis, dsyev per sector, truncation, both invariant-matrix routines),
-  rank 0 only: the reference cannot be built here (Fortran, MPI, MKL).
+  threads) on two full-size iterations of the same chain with their backward density
+  matrices and CFS spectrum (a bounded sample of the metric's scope).
+* --impl reference: the oracle port on the same scope, rank 0 only: K steps = K full-size
+  NRG iterations (prepareBasis, dsyev per sector, truncation, both invariant-matrix
+  routines) with their density-matrix and CFS steps, on a window of the headline chain
+  whose last iteration is the window's last; warm-up: min(W, 2) untimed full-size
+  forward iterations.  The reference itself cannot be built here (Fortran, MPI, MKL).
 * n_keep_2048: the N_keep = 2048 SIAM workload (Lambda=2, U=0.2, Gamma=0.02,
   eps_d=-0.1, 60 iterations), one warm-up and two event-timed sweeps.
 * fdm: that workload with the full-density-matrix spectrum and density matrices at
@@ -320,24 +322,53 @@ def two_orbital_window(torch, dev, local, stream):
         c.close()
 
 
-def cpu_sample(n_timed=2):
-    """Oracle port on full-size forward iterations of the same sweep."""
+def oracle_window(n_full, warmup=0):
+    """The oracle port over the scope of the headline's metric: forward NRG iterations, the
+    backward reduced density matrices and the CFS spectrum, on a window of the same chain
+    (the headline chain cut so that its last n_full iterations are the full-size ones:
+    every iteration from the first truncated one to the last, whose sizes and per-iteration
+    work are those of the 60-iteration sweep).  The iterations before full size (five,
+    cheap) run untimed; `warmup` full-size forward iterations of another window run first,
+    untimed.  Returns (iterations/s, seconds, first and last timed iteration, states per
+    iteration)."""
     from nrg_b200 import model
     from oracle import nrg_oracle as O
-    inp = model.siam(**WORKLOAD)
-    d = tempfile.mkdtemp(prefix="nrg_cpu_")
-    model.write_inputs(inp, d)
-    st = O.State(d)
-    it = st.first
-    while st.numberOfBasis_old < st.truncation and it <= st.nIter:
-        O.nrg_iteration(st, it)    # grow to full size (untimed)
-        it += 1
+
+    def window(n):
+        # the first full-size iteration: before it no truncation happens, so the basis grows
+        # by nOps per iteration from the initial one
+        probe = model.siam(**WORKLOAD)
+        k, nb = 0, probe.numberOfBasis
+        while nb < WORKLOAD["n_keep"]:
+            nb *= probe.numberOfOperation
+            k += 1
+        last = probe.indexOfFirstIteration + k + n - 1
+        inp = model.siam(**dict(WORKLOAD, n_iterations=last + 2))   # numberOfIteration = n_iterations - 2
+        d = tempfile.mkdtemp(prefix="nrg_cpu_")
+        model.write_inputs(inp, d)
+        st = O.State(d)
+        it = st.first
+        while st.numberOfBasis_old < st.truncation and it <= st.nIter:
+            O.nrg_iteration(st, it)    # grow to full size (untimed)
+            it += 1
+        return st, it
+
+    if warmup > 0:
+        st, it = window(warmup)
+        for N in range(it, st.nIter + 1):
+            O.nrg_iteration(st, N)
+    st, it0 = window(n_full)
     t0 = time.perf_counter()
-    for _ in range(n_timed):
-        O.nrg_iteration(st, it)
-        it += 1
+    for N in range(it0, st.nIter + 1):                # main.F90:175-177
+        O.nrg_iteration(st, N)
+    if st.flag_truncation:                            # main.F90:188-201
+        O.initialize_reduced_density(st)
+        O.reduced_density_matrix_calculation(st)
+    for N in range(st.startTrancation, st.nIter + 1):   # main.F90:204-224
+        O.cfs_spectrum_calculation(st, N)
     dt = time.perf_counter() - t0
-    return n_timed / dt, dt, it - n_timed, it - 1, int(st.numberOfBasis_full)
+    n = st.nIter - it0 + 1
+    return n / dt, dt, it0, st.nIter, int(st.numberOfBasis_full)
 
 
 def roofline_traffic():
@@ -350,6 +381,13 @@ def roofline_traffic():
         return None, None
 
 
+def headline_config(world):
+    """The `config` object of both arms' JSON lines."""
+    return {"workload": WORKLOAD_NAME, "n_keep": WORKLOAD["n_keep"],
+            "iterations": WORKLOAD["n_iterations"], "parallelism": f"replicas x{world}",
+            "l2": "working set > L2: each step writes ~20 GB of eigenvector blocks and spectral matrices"}
+
+
 def reference_arm(args):
     rank, _, world = dist_env()
     if world > 1:
@@ -359,39 +397,26 @@ def reference_arm(args):
             dist.barrier()
             dist.destroy_process_group()
             return
-    from nrg_b200 import model
-    from oracle import nrg_oracle as O
-    inp = model.siam(**WORKLOAD)
-    d = tempfile.mkdtemp(prefix="nrg_ref_")
-    model.write_inputs(inp, d)
-    st = O.State(d)
-    it = st.first
-    while st.numberOfBasis_old < st.truncation and it <= st.nIter:
-        O.nrg_iteration(st, it)
-        it += 1
-    for _ in range(args.warmup):
-        O.nrg_iteration(st, it)
-        it += 1
-    t0 = time.perf_counter()
-    for _ in range(args.steps):
-        O.nrg_iteration(st, it)
-        it += 1
-    dt = time.perf_counter() - t0
-    v = args.steps / dt
+    # K timed steps = K full-size NRG iterations with their backward density matrices and
+    # CFS spectrum; warm-up: min(W, 2) untimed full-size forward iterations (~10 s each on
+    # 16 host threads, so K = 20 ends in about four minutes)
+    warm = min(args.warmup, 2)
+    v, dt, i0, i1, nbf = oracle_window(max(1, args.steps), warmup=warm)
+    n = i1 - i0 + 1
     cores = os.cpu_count()
+    sample = (f"full-size NRG iterations {i0}..{i1} of the headline chain (nb ~ {nbf} each) with their "
+              f"backward density matrices and CFS spectrum, the window's last iteration as the last; "
+              f"{dt:.1f} s, numpy/scipy-OpenBLAS oracle on {cores} host threads")
     line = {
         "impl": "reference", "metric": METRIC, "value": v, "unit": "iterations/s",
-        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
-        "ms_per_step": dt / args.steps * 1e3, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": WORKLOAD_NAME, "n_keep": WORKLOAD["n_keep"], "iterations": 60,
-                   "parallelism": "replicas",
-                   "step": f"one full-size forward NRG iteration (nb ~ {int(st.numberOfBasis_full)})",
-                   "scope": "forward iterations only (prepareBasis, dsyev per sector, truncation, both "
-                            "invariant-matrix routines): compare with the b200 arm's forward_only"},
-        "cpu_baseline": {"value": v, "unit": "iterations/s", "cores": cores, "kind": "port",
-                         "sample": f"forward NRG iterations {it - args.steps}..{it - 1} of the sweep "
-                                   "(prepareBasis, dsyev per sector, truncation, invariant matrices)"},
+        "n_gpus": args.gpus, "steps": n, "warmup": warm,
+        "ms_per_step": dt / n * 1e3, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic (generated Wilson chain and impurity tables)",
+        "config": headline_config(world),
+        "scope": ("one step = one full-size NRG iteration (prepareBasis, dsyev per sector, truncation, both "
+                  "invariant-matrix routines) plus its step of the backward density matrices and of the CFS "
+                  "spectrum; the b200 arm's value also counts the five cheap iterations before full size"),
+        "cpu_baseline": {"value": v, "unit": "iterations/s", "cores": cores, "kind": "port", "sample": sample},
         "e2e": {"value": v, "unit": "iterations/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -563,20 +588,18 @@ def main():
         traffic, traffic_src = roofline_traffic()
         cpu = None
         if not args.no_cpu:
-            v, dt, i0, i1, nbf = cpu_sample()
+            v, dt, i0, i1, nbf = oracle_window(2)
             cpu = {"value": v, "unit": "iterations/s", "cores": os.cpu_count(), "kind": "port",
-                   "sample": f"forward NRG iterations {i0}..{i1} of the same sweep (nb ~ {nbf} each), "
-                             f"{dt:.1f} s, numpy/scipy-OpenBLAS oracle; forward path only (compare with "
-                             "forward_only)"}
+                   "sample": f"full-size NRG iterations {i0}..{i1} of the same chain (nb ~ {nbf} each) with "
+                             f"their backward density matrices and CFS spectrum (the window's last "
+                             f"iteration as the last), {dt:.1f} s, numpy/scipy-OpenBLAS oracle on all host "
+                             "threads"}
         line = {
             "metric": METRIC, "value": value, "unit": "iterations/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": t_max / args.steps * 1e3,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic (generated Wilson chain and impurity tables)",
-            "config": {"workload": WORKLOAD_NAME, "n_keep": WORKLOAD["n_keep"], "iterations": n_it,
-                       "parallelism": f"replicas x{world}",
-                       "l2": "working set > L2: each step writes ~20 GB of eigenvector blocks and "
-                             "spectral matrices"},
+            "config": headline_config(world),
             "phase_seconds": {"nrg_sweep": float(ph[0]), "rdm": float(ph[1]), "cfs_spectrum": float(ph[2])},
             "spectrum_seconds": float(ph[2]),
             "forward_only": forward_only,
