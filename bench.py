@@ -46,6 +46,9 @@ second (60 per step), whole job.
   at a time and then 8 in flight; wall clock around each batch with the device
   synchronised; with N ranks the instances are dealt to the ranks by the greedy cost
   rule and the slowest rank's time counts.
+* many_instance_full: the many-instance workload itself: all 64 draws (N_keep from
+  {512, 1024, 2048, 4096}) with the full-density-matrix spectrum at T = 1e-5, 8 in
+  flight, each instance's storage released when it ends; wall clock around the batch.
 Multi-GPU: one NRG instance does not shard (one GPU per instance), so N ranks run N
 replicas of the headline workload; the many-instance sample is partitioned instead.
 """
@@ -88,7 +91,7 @@ def parse():
     p.add_argument("--no-nk2048", action="store_true")
     p.add_argument("--no-pageable", action="store_true")
     p.add_argument("--no-two-orbital", action="store_true")
-    p.add_argument("--many-full", action="store_true", help="also time all 64 instances of the sweep")
+    p.add_argument("--no-many-full", action="store_true", help="skip the 64-instance FDM sweep")
     p.add_argument("--e2e-steps", type=int, default=3)
     # profiling helpers: a shorter sweep of the same model (not the headline workload)
     p.add_argument("--iterations", type=int, default=None)
@@ -256,10 +259,12 @@ def second_workload(torch, dev, local, stream, fdm_temperature=None):
         c.close()
 
 
-def many_instance_full(torch, dev, rank, world, dist, concurrency=8):
-    """All 64 draws of the seeded sweep (N_keep from {512, 1024, 2048, 4096}, 50 iterations,
-    T=0 CFS), largest first, `concurrency` in flight with each context's storage released
-    when its instance ends; one untimed pass first (module load, tuner), then one timed."""
+def many_instance_full(torch, dev, rank, world, dist, concurrency=8, temperature=1e-5):
+    """The many-instance workload: all 64 draws of the seeded sweep (N_keep from {512,
+    1024, 2048, 4096}, 50 iterations) with the full-density-matrix spectrum at
+    T = `temperature`, largest first, `concurrency` in flight, each context's storage
+    released when its instance ends.  Untimed first: one instance of each N_keep (module
+    load, the GEMM tuner's first launches); then all 64 timed."""
     from nrg_b200 import Context, run_batch, sweep
     inst = sorted(sweep.sweep_instances(), key=lambda x: -x.cost())
     share = sweep.rank_share(inst, rank, world)
@@ -269,12 +274,17 @@ def many_instance_full(torch, dev, rank, world, dist, concurrency=8):
             c = Context(dev.index)
             c.set_model(x.build())
             ctxs.append(c)
-        run_batch(ctxs, spectrum=True, concurrency=concurrency, release=True)
+        warm, seen = [], set()
+        for c, x in zip(ctxs, share):
+            if x.n_keep not in seen:
+                seen.add(x.n_keep)
+                warm.append(c)
+        run_batch(warm, spectrum=True, concurrency=concurrency, release=True, temperature=temperature)
         if dist is not None:
             dist.barrier()
         torch.cuda.synchronize(dev)
         t0 = time.perf_counter()
-        run_batch(ctxs, spectrum=True, concurrency=concurrency, release=True)
+        res, _ = run_batch(ctxs, spectrum=True, concurrency=concurrency, release=True, temperature=temperature)
         torch.cuda.synchronize(dev)
         dt = time.perf_counter() - t0
         if dist is not None:
@@ -284,12 +294,19 @@ def many_instance_full(torch, dev, rank, world, dist, concurrency=8):
     finally:
         for c in ctxs:
             c.close()
+    sums = []
+    for r in res:
+        nbin = r["numberOfBin"]
+        sums += [abs(float(r["binPos"][m * nbin:(m + 1) * nbin, 1].sum()
+                           + r["binNeg"][m * nbin:(m + 1) * nbin, 1].sum()) - 1.0) for m in range(2)]
     its = sum(x.n_iterations for x in inst)
     return {"workload": f"all {len(inst)} SIAMs of the seeded draw (seed {sweep.SWEEP_SEED}), N_keep from "
-                        "{512, 1024, 2048, 4096}, Lambda=2, 50 NRG iterations each + RDM + T=0 CFS spectrum",
+                        "{512, 1024, 2048, 4096}, Lambda=2, 50 NRG iterations each + density matrices + FDM "
+                        f"spectrum at T={temperature}",
             "instances": len(inst), "iterations": its, "seconds": dt, "iterations_per_s": its / dt,
-            "concurrency": concurrency, "ranks": world,
-            "timing": "wall clock around the batch, device synchronised, max over ranks; storage released per instance"}
+            "concurrency": concurrency, "ranks": world, "sum_rule_max_dev": max(sums) if sums else None,
+            "timing": "wall clock around the batch, device synchronised, max over ranks; storage released per "
+                      "instance; one instance of each N_keep run untimed first"}
 
 
 def two_orbital_window(torch, dev, local, stream):
@@ -572,7 +589,7 @@ def main():
     fdm = None if args.no_fdm else second_workload(torch, dev, local, stream, fdm_temperature=1e-6)
     many = None if args.no_many else many_instance(torch, dev, rank, world, dist)
     two = None if args.no_two_orbital else two_orbital_window(torch, dev, local, stream)
-    many_full = many_instance_full(torch, dev, rank, world, dist) if args.many_full else None
+    many_full = None if args.no_many_full else many_instance_full(torch, dev, rank, world, dist)
     if rank == 0:
         clocks = clk.summary()
         nbin = res["numberOfBin"]
@@ -631,8 +648,7 @@ def main():
             "many_instance": many,
             "two_orbital_window": two,
         }
-        if many_full is not None:
-            line["many_instance_full"] = many_full
+        line["many_instance_full"] = many_full
         print(json.dumps(line), flush=True)
     ctx.close()
     if dist is not None:

@@ -569,9 +569,11 @@ class Context:
 
 
 def run_batch(contexts, spectrum: bool = True, concurrency: int = 0, flow_stride: int = 8,
-              release: bool = False):
+              release: bool = False, temperature: float = 0.0):
     """nrg_run_batch: independent instances (distinct contexts on one device) side by side.
     ``release=True`` frees each context's run storage when its instance ends.
+    ``temperature > 0`` gives every instance the full-density-matrix spectrum at that
+    temperature (as ``Context.run``) instead of the T = 0 CFS spectrum.
 
     Returns (results, statuses): one result dict per context and the per-instance
     statuses; raises NrgError when any instance failed (every instance still ran).
@@ -579,7 +581,7 @@ def run_batch(contexts, spectrum: bool = True, concurrency: int = 0, flow_stride
     if not contexts:
         return [], []
     lib = contexts[0].lib
-    args = [c._run_args(spectrum, flow_stride, 0, False) for c in contexts]
+    args = [c._run_args(spectrum, flow_stride, 0, False, temperature) for c in contexts]
     n = len(contexts)
     hs = (c_void_p * n)(*[c._h for c in contexts])
     ris = (RunInput * n)(*[a["ri"] for a in args])

@@ -50,6 +50,35 @@ def test_batch_matches_oracle_per_instance():
             c.close()
 
 
+def test_batch_fdm_matches_the_instances_run_alone():
+    """The full-density-matrix spectrum (the many-instance workload's T > 0) side by side:
+    each instance's bins and shell traces equal its run alone (the same kernels on the
+    same data; FP64 atomics in the binning allow last-bit differences)."""
+    xs = _small_sweep()[:3]
+    T = 1e-4
+    ctxs = []
+    try:
+        for x in xs:
+            c = Context(0)
+            c.set_model(x.build())
+            ctxs.append(c)
+        alone = [c.run(spectrum=True, temperature=T) for c in ctxs]
+        results, statuses = run_batch(ctxs, spectrum=True, concurrency=3, temperature=T)
+        assert statuses == [0] * len(xs)
+        for a, r in zip(alone, results):
+            assert [int(k) for k in r["kept"]] == [int(k) for k in a["kept"]]
+            assert np.max(np.abs(r["binPos"][:, 1] - a["binPos"][:, 1])) <= 1e-12
+            assert np.max(np.abs(r["binNeg"][:, 1] - a["binNeg"][:, 1])) <= 1e-12
+            assert np.nanmax(np.abs(r["rdmTrace"] - a["rdmTrace"])) <= 1e-12
+            nbin = r["numberOfBin"]
+            for m in range(2):
+                tot = (r["binPos"][m * nbin:(m + 1) * nbin, 1].sum() + r["binNeg"][m * nbin:(m + 1) * nbin, 1].sum())
+                assert abs(tot - 1.0) <= SUM_TOL
+    finally:
+        for c in ctxs:
+            c.close()
+
+
 def test_batch_rejects_a_repeated_context():
     inp = _small_sweep()[0].build()
     c = Context(0)
