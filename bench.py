@@ -29,9 +29,10 @@ second (60 per step), whole job.
 * cpu_baseline: the oracle (numpy/scipy port of the reference path, OpenBLAS on all host
   threads) on two full-size iterations of the same chain with their backward density
   matrices and CFS spectrum (a bounded sample of the metric's scope).
-* --impl reference: the oracle port on the same scope, rank 0 only: K steps = K full-size
-  NRG iterations (prepareBasis, dsyev per sector, truncation, both invariant-matrix
-  routines) with their density-matrix and CFS steps, on a window of the headline chain
+* --impl reference: the oracle port on the same scope, rank 0 only: min(K, 10) steps, one
+  full-size NRG iteration each (prepareBasis, dsyev per sector, truncation, both
+  invariant-matrix routines) with its density-matrix and CFS steps, on a window of the
+  headline chain
   whose last iteration is the window's last; warm-up: min(W, 2) untimed full-size
   forward iterations.  The reference itself cannot be built here (Fortran, MPI, MKL).
 * n_keep_2048: the N_keep = 2048 SIAM workload (Lambda=2, U=0.2, Gamma=0.02,
@@ -414,11 +415,11 @@ def reference_arm(args):
             dist.barrier()
             dist.destroy_process_group()
             return
-    # K timed steps = K full-size NRG iterations with their backward density matrices and
-    # CFS spectrum; warm-up: min(W, 2) untimed full-size forward iterations (~10 s each on
-    # 16 host threads, so K = 20 ends in about four minutes)
+    # timed steps = min(K, 10) full-size NRG iterations with their backward density matrices
+    # and CFS spectrum (~10 s each on 16 host threads); warm-up: min(W, 2) untimed full-size
+    # forward iterations: the whole run ends within about two and a half minutes
     warm = min(args.warmup, 2)
-    v, dt, i0, i1, nbf = oracle_window(max(1, args.steps), warmup=warm)
+    v, dt, i0, i1, nbf = oracle_window(min(max(1, args.steps), 10), warmup=warm)
     n = i1 - i0 + 1
     cores = os.cpu_count()
     sample = (f"full-size NRG iterations {i0}..{i1} of the headline chain (nb ~ {nbf} each) with their "
