@@ -91,6 +91,8 @@ nrg_context::~nrg_context() {
     h_evals.release();
     h_kept.release();
     if (aux_hi) cudaStreamDestroy(aux_hi);
+    if (aux_copy) cudaStreamDestroy(aux_copy);
+    if (ev_copied) cudaEventDestroy(ev_copied);
     for (auto* pl : {&pending_tri, &pending_syev})
         for (auto& t : *pl) {
             cudaEventDestroy(t.a);
@@ -592,10 +594,18 @@ int nrg_diagonalization(nrg_context* ctx, int32_t iteration, const nrg_diagonali
     if (rc == NRG_OK) rc = stage_out(ctx, io->eigenvector, (size_t)S.sizeV, kSlotIO + 2, &dV);
     if (rc == NRG_OK) rc = stage_out(ctx, io->eigenvalue, (size_t)S.nb, kSlotIO + 3, &dE);
     DiagOut out;
+    // a page-locked eigenvector array takes each group's blocks as soon as they are final
+    DiagPost post;
+    if (rc == NRG_OK && dV != io->eigenvector) {
+        cudaPointerAttributes a;
+        if (cudaPointerGetAttributes(&a, io->eigenvector) == cudaSuccess && a.type == cudaMemoryTypeHost)
+            post.h_V = io->eigenvector;
+        cudaGetLastError();
+    }
     clk.mark(0);
-    if (rc == NRG_OK) rc = diag_device(ctx, iteration, S, dEo, nbo, dIM, dV, dE, &out);
+    if (rc == NRG_OK) rc = diag_device(ctx, iteration, S, dEo, nbo, dIM, dV, dE, &out, &post);
     clk.mark(1);
-    if (rc == NRG_OK) rc = finish_out(ctx, io->eigenvector, dV, (size_t)S.sizeV);
+    if (rc == NRG_OK && !post.copied_V) rc = finish_out(ctx, io->eigenvector, dV, (size_t)S.sizeV);
     if (rc == NRG_OK) rc = finish_out(ctx, io->eigenvalue, dE, (size_t)S.nb);
     if (rc == NRG_OK && io->basis_output) {
         std::vector<int> bo((size_t)S.nb * rs, 0);

@@ -188,6 +188,8 @@ struct nrg_context {
     // for the back-transformations, so the host bookkeeping of the next iteration runs
     // while they finish
     cudaEvent_t ev_evals_hi = nullptr, ev_evals2 = nullptr, ev_evals_host = nullptr;
+    cudaStream_t aux_copy = nullptr;        // eigenvector blocks to the host as their groups end
+    cudaEvent_t ev_copied = nullptr;
     // measured policy: the early path gains ~6 % for an instance that has the device to
     // itself and loses ~10 % with eight instances in flight (their work already fills
     // the host gap), so nrg_run_batch turns it off when it runs instances side by side
@@ -284,7 +286,7 @@ int run_assemble(nrg_context* ctx, int iteration, const Sectors& S, const SyevSe
 // the shift of the eigenvalues (E -= min E, E <= 1e-12 -> 0; min and E(1) to
 // d_min_and_gs) and the chop of the eigenvectors (|V| < 1e-14 -> 0), on ctx->stream
 int run_eig_shift(nrg_context* ctx, double* d_E, int nb, double* d_min_and_gs);
-int run_eig_chop(nrg_context* ctx, long long sizeV, double* d_V);
+int run_eig_chop(nrg_context* ctx, long long sizeV, double* d_V, cudaStream_t st = nullptr);   // null: ctx->stream
 
 struct ImGatherProb {
     long long t_off;    // T (dL x kR) col-major
@@ -348,9 +350,16 @@ struct DiagPost {
     bool early = false;
     double* h_E = nullptr;
     struct TruncTables* trunc = nullptr;   // device truncation launched after the shift
+    // Without early: the caller's page-locked eigenvector array (the drop-in's module
+    // array), or null.  When the largest sectors run on their own stream, the blocks of the
+    // other sectors are chopped and copied there as soon as their groups end, on a copy
+    // stream, while the largest sectors are still being reduced; theirs follow.  The call
+    // returns with every block in h_V (the caller then copies nothing).
+    double* h_V = nullptr;
+    bool copied_V = false;                 // out: h_V holds the eigenvectors
 };
 int diag_device(nrg_context* ctx, int iteration, Sectors& S, const double* d_Eold, int nb_old,
-                const double* d_IMold, double* d_V, double* d_E, DiagOut* out, const DiagPost* post = nullptr);
+                const double* d_IMold, double* d_V, double* d_E, DiagOut* out, DiagPost* post = nullptr);
 
 // ---- device bookkeeping of the device-resident run (tables.cu) ----
 struct TruncParams {

@@ -484,8 +484,9 @@ int run_eig_shift(nrg_context* ctx, double* d_E, int nb, double* d_min_and_gs) {
     return NRG_OK;
 }
 
-int run_eig_chop(nrg_context* ctx, long long sizeV, double* d_V) {
-    k_chop<<<grid_for(sizeV, 256), 256, 0, ctx->stream>>>(d_V, sizeV);
+int run_eig_chop(nrg_context* ctx, long long sizeV, double* d_V, cudaStream_t st) {
+    if (sizeV <= 0) return NRG_OK;
+    k_chop<<<grid_for(sizeV, 256), 256, 0, st ? st : ctx->stream>>>(d_V, sizeV);
     ctx->launches++;
     NRG_CUDA_TRY(cudaGetLastError());
     return NRG_OK;

@@ -303,7 +303,7 @@ int check_device_status(nrg_context* ctx) {
 // diagonalization (diagonalization.F90:1-410)
 // ------------------------------------------------------------------------------------
 int diag_device(nrg_context* ctx, int iteration, Sectors& S, const double* d_Eold, int nb_old,
-                const double* d_IMold, double* d_V, double* d_E, DiagOut* out, const DiagPost* post) {
+                const double* d_IMold, double* d_V, double* d_E, DiagOut* out, DiagPost* post) {
     const bool early = post && post->early;
     double* h_E = post ? post->h_E : nullptr;
     TruncTables* trunc = post ? post->trunc : nullptr;
@@ -418,6 +418,45 @@ int diag_device(nrg_context* ctx, int iteration, Sectors& S, const double* d_Eol
         NRG_CUDA_TRY(cudaEventRecord(ctx->ev_join2, ctx->aux2));
     }
     NRG_TRY(rl);
+    // The drop-in's eigenvectors to the caller's page-locked array as their groups end: the
+    // blocks outside the largest class once the small sectors and the second large group are
+    // done (while the largest sectors are still being reduced), the largest class's after
+    // it; each part chopped (diagonalization.F90:273-280) just before its copy.
+    const bool copy_early = !early && post && post->h_V && !g1.empty() && (fork_small || has_g2);
+    if (copy_early) {
+        if (!ctx->aux_copy) {
+            NRG_CUDA_TRY(cudaStreamCreateWithFlags(&ctx->aux_copy, cudaStreamNonBlocking));
+            NRG_CUDA_TRY(cudaEventCreateWithFlags(&ctx->ev_copied, cudaEventDisableTiming));
+        }
+        cudaStream_t cs = ctx->aux_copy;
+        if (!fork_large) NRG_CUDA_TRY(cudaEventRecord(ctx->ev_join_hi, ctx->stream));   // g1 ran there
+        std::vector<std::pair<long long, long long>> hi, rest;   // (offset, length) in doubles
+        for (const auto& q : g1) hi.push_back({q.a_off, (long long)q.n * q.n});
+        std::sort(hi.begin(), hi.end());
+        long long pos = 0;
+        for (const auto& r : hi) {
+            if (r.first > pos) rest.push_back({pos, r.first - pos});
+            pos = r.first + r.second;
+        }
+        if (pos < S.sizeV) rest.push_back({pos, S.sizeV - pos});
+        auto chop_copy = [&](const std::vector<std::pair<long long, long long>>& parts) -> int {
+            for (const auto& r : parts) {
+                NRG_TRY(run_eig_chop(ctx, r.second, d_V + r.first, cs));
+                NRG_CUDA_TRY(cudaMemcpyAsync(post->h_V + r.first, d_V + r.first, sizeof(double) * r.second,
+                                             cudaMemcpyDeviceToHost, cs));
+                ctx->d2h += (long long)sizeof(double) * r.second;
+            }
+            return NRG_OK;
+        };
+        if (fork_small) NRG_CUDA_TRY(cudaStreamWaitEvent(cs, ctx->ev_join, 0));
+        if (has_g2) NRG_CUDA_TRY(cudaStreamWaitEvent(cs, ctx->ev_join2, 0));
+        NRG_TRY(chop_copy(rest));
+        NRG_CUDA_TRY(cudaStreamWaitEvent(cs, ctx->ev_join_hi, 0));
+        NRG_TRY(chop_copy(hi));
+        NRG_CUDA_TRY(cudaEventRecord(ctx->ev_copied, cs));
+        NRG_CUDA_TRY(cudaStreamWaitEvent(ctx->stream, ctx->ev_copied, 0));
+        post->copied_V = true;
+    }
     double* hs = nullptr;
     if (early) {
         // eigenvalues of every group -> shift -> host, then the eigenvectors' join
@@ -461,7 +500,7 @@ int diag_device(nrg_context* ctx, int iteration, Sectors& S, const double* d_Eol
     }
     NRG_TRY(run_eig_shift(ctx, d_E, S.nb, bmin.as<double>()));
     if (trunc) NRG_TRY(trunc->launch(ctx, d_E));
-    NRG_TRY(run_eig_chop(ctx, S.sizeV, d_V));
+    if (!copy_early) NRG_TRY(run_eig_chop(ctx, S.sizeV, d_V));
     double mg[2];
     NRG_CUDA_TRY(cudaMemcpyAsync(mg, bmin.p, sizeof(double) * 2, cudaMemcpyDeviceToHost, ctx->stream));
     ctx->d2h += sizeof(mg);

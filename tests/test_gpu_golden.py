@@ -7,8 +7,8 @@ density-matrix trace of every backward step, and the nonzero spectral bins:
 
 * the N_keep = 2048 SIAM workload, all 60 iterations with density matrices and the T = 0
   CFS spectrum (the second bench object);
-* the N_keep = 4096 SIAM workload (the bench headline's model), its first 14 iterations
-  (-1..12), the model cut there;
+* the N_keep = 4096 SIAM workload (the bench headline), all 60 iterations with density
+  matrices and the T = 0 CFS spectrum;
 * the two-orbital Hund model at N_keep = 8192 (16 local states), its first 5 iterations
   (-1..3), forward sweep only: 131,104 states at iteration 3 in sectors of order up to
   ~8,800, past the cluster tridiagonalisation's and the shared-memory back-transformation's
@@ -44,7 +44,7 @@ MAT_TOL = 1e-12
 
 CASES = {
     "siam_nkeep2048": lambda: model.config(2),
-    "siam_nkeep4096_n14": lambda: model.config(3, n_iterations=14),
+    "siam_nkeep4096": lambda: model.config(3),
 }
 
 
@@ -105,7 +105,7 @@ def test_whole_run_matches_golden(ctx_factory, name):
     _compare(res, g, device_resident=True)
     res2 = ctx.run(spectrum=True, flow_stride=64, host_drop_in=True)
     _compare(res2, g, device_resident=False)
-    if name == "siam_nkeep4096_n14":
+    if name == "siam_nkeep4096":
         # the caller's module arrays in pageable memory (a Fortran allocatable): the routines
         # gather the runs they read on the host instead of reading pinned memory directly
         res3 = ctx.run(spectrum=True, flow_stride=64, host_drop_in=True, host_pageable=True)
