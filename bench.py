@@ -29,7 +29,7 @@ second (60 per step), whole job.
 * cpu_baseline: the oracle (numpy/scipy port of the reference path, OpenBLAS on all host
   threads) on two full-size iterations of the same chain with their backward density
   matrices and CFS spectrum (a bounded sample of the metric's scope).
-* --impl reference: the oracle port on the same scope, rank 0 only: min(K, 10) steps, one
+* --impl reference: the oracle port on the same scope, rank 0 only: K steps, one
   full-size NRG iteration each (prepareBasis, dsyev per sector, truncation, both
   invariant-matrix routines) with its density-matrix and CFS steps, on a window of the
   headline chain
@@ -415,11 +415,11 @@ def reference_arm(args):
             dist.barrier()
             dist.destroy_process_group()
             return
-    # timed steps = min(K, 10) full-size NRG iterations with their backward density matrices
-    # and CFS spectrum (~10 s each on 16 host threads); warm-up: min(W, 2) untimed full-size
-    # forward iterations: the whole run ends within about two and a half minutes
+    # K timed steps = K full-size NRG iterations with their backward density matrices and
+    # CFS spectrum (~10 s each on 16 host threads); warm-up: min(W, 2) untimed full-size
+    # forward iterations (K = 20: about four minutes in all)
     warm = min(args.warmup, 2)
-    v, dt, i0, i1, nbf = oracle_window(min(max(1, args.steps), 10), warmup=warm)
+    v, dt, i0, i1, nbf = oracle_window(max(1, args.steps), warmup=warm)
     n = i1 - i0 + 1
     cores = os.cpu_count()
     sample = (f"full-size NRG iterations {i0}..{i1} of the headline chain (nb ~ {nbf} each) with their "
