@@ -33,7 +33,7 @@ second (60 per step), whole job.
   full-size NRG iteration each (prepareBasis, dsyev per sector, truncation, both
   invariant-matrix routines) with its density-matrix and CFS steps, on a window of the
   headline chain
-  whose last iteration is the window's last; warm-up: min(W, 2) untimed full-size
+  whose last iteration is the window's last; W warm-up steps = W untimed full-size
   forward iterations.  The reference itself cannot be built here (Fortran, MPI, MKL).
 * n_keep_2048: the N_keep = 2048 SIAM workload (Lambda=2, U=0.2, Gamma=0.02,
   eps_d=-0.1, 60 iterations), one warm-up and two event-timed sweeps.
@@ -416,9 +416,9 @@ def reference_arm(args):
             dist.destroy_process_group()
             return
     # K timed steps = K full-size NRG iterations with their backward density matrices and
-    # CFS spectrum (~10 s each on 16 host threads); warm-up: min(W, 2) untimed full-size
-    # forward iterations (K = 20: about four minutes in all)
-    warm = min(args.warmup, 2)
+    # CFS spectrum (~10 s each on 16 host threads); W warm-up steps = W untimed full-size
+    # forward iterations (K = 20, W = 5: about four and a half minutes in all)
+    warm = max(0, args.warmup)
     v, dt, i0, i1, nbf = oracle_window(max(1, args.steps), warmup=warm)
     n = i1 - i0 + 1
     cores = os.cpu_count()
